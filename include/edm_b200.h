@@ -1,0 +1,311 @@
+/*
+ * edm_b200.h — C ABI of the B200-native ED-MRDT per-timestep hot path.
+ *
+ * The reference (Edel-datsci/FLIM-Microscopy-Simulator-with-Causal-Inference,
+ * "ED-MRDT v1.1") is pure Python + Numba and has no FFI layer; its drop-in
+ * boundary is the Python object API.  Each entry point below replaces one call
+ * of that API (cited per function), with plain pointers, sizes and a CUDA
+ * stream handle passed as `void*` (cudaStream_t), so a ctypes / cgo / JNI
+ * binding needs no CUDA or torch headers.
+ *
+ * Conventions (mirroring the reference's numba kernels, ed_mrdt/dynamics.py):
+ *   - particles are indexed per replica 0..N_r-1 ("particle index"), exactly
+ *     as ParticleState orders them (ed_mrdt/particles.py:80-187);
+ *   - positions are float64 [N][2] in µm, species int32, flags uint8;
+ *   - every entry point returns 0 on success and a negative EDM_E* code on
+ *     failure; edm_last_error() describes the last failure of this thread;
+ *   - runtime overflow (photon buffer, Hill-table range, pair caps) never
+ *     truncates silently: it sets a bit in the engine's status word
+ *     (EDM_STATUS_*), readable with edm_get_status().
+ */
+#ifndef EDM_B200_H
+#define EDM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EDM_ABI_VERSION 1
+
+/* ---- fixed capacities of the parameter blocks --------------------------- */
+#define EDM_MAX_SPECIES 16
+#define EDM_MAX_BIND 4
+#define EDM_MAX_CAT 8
+#define EDM_MAX_EXCH 8
+#define EDM_MAX_CONV 8
+#define EDM_MAX_GRIDS 8
+#define EDM_MAX_RULES 24
+#define EDM_MAX_REGIONS 8
+#define EDM_MAX_FLUO 4
+#define EDM_MAX_FRET 4
+#define EDM_MAX_FCLASS 8
+
+/* ---- error codes -------------------------------------------------------- */
+#define EDM_OK 0
+#define EDM_EINVAL -1   /* bad argument / inconsistent parameters           */
+#define EDM_ECUDA -2    /* a CUDA runtime call failed                       */
+#define EDM_ENOMEM -3   /* device allocation failed                         */
+#define EDM_EUNSUP -4   /* feature not supported by this build              */
+
+/* ---- status bits (sticky, per engine) ------------------------------------ */
+#define EDM_STATUS_PHOTON_CAP 0x1u     /* photon stream reached max_photons (reference truncates too) */
+#define EDM_STATUS_HILL_RANGE 0x2u     /* density count beyond the exact Hill table: device pow used   */
+#define EDM_STATUS_FORCE_TERMS 0x4u    /* >EDM_MAX_FORCE_TERMS force terms on one particle             */
+#define EDM_STATUS_NONFINITE 0x8u      /* a non-finite position was produced                            */
+#define EDM_STATUS_BIND_CAP 0x10u      /* binding candidate buffer overflow                             */
+#define EDM_STATUS_RECRUIT_CAP 0x20u   /* recruitment candidate buffer overflow                         */
+#define EDM_STATUS_POISSON_NORMAL 0x40u /* a Poisson mean >= 30 used the normal approximation            */
+
+/* ---- noise streams (Philox key = seed; counter = (a, b, step, stream)) --- */
+enum EdmStream {
+  EDM_S_BD_NORMAL = 1,        /* standard_normal((N,2))          dynamics.py:2194 */
+  EDM_S_BIND = 16,            /* + 2r: random(M) per binding r   dynamics.py:2207 */
+  EDM_S_DISSOC = 17,          /* + 2r: random(N)                 dynamics.py:2219 */
+  EDM_S_CAT = 32,             /* + c : random(M) per catalytic   dynamics.py:2246 */
+  EDM_S_EX_ACCEPT = 48,       /* + 4e: random(N)                 dynamics.py:2301 */
+  EDM_S_EX_POS = 49,          /* + 4e: random((N,2))             dynamics.py:2302 */
+  EDM_S_EX_LOC = 50,          /* + 4e: random(N) (local recruit) dynamics.py:2372 */
+  EDM_S_EX_DETACH = 51,       /* + 4e: random(N)                 dynamics.py:2407 */
+  EDM_S_EX_OFFSET = 96,       /* + e : standard_normal((N,2))    dynamics.py:2373 */
+  EDM_S_CONV = 80,            /* + v : random(N)                 dynamics.py:2438 */
+  EDM_S_PH_POISSON = 112,     /* random(N)            photophysics.py:1136 */
+  EDM_S_PH_TRANS = 113,       /* random(N)            photophysics.py:1137 */
+  EDM_S_PH_ARRIVAL = 114,     /* random(est_photons)  photophysics.py:1145 */
+  EDM_S_SC_QE = 120,          /* random(n_ph)         microscope.py:848 */
+  EDM_S_SC_ASSIGN = 121,      /* random(n_surv)       microscope.py:378 */
+  EDM_S_SC_JITTER = 122,      /* normal(0,σ,n)        microscope.py:743 */
+  EDM_S_SC_DARK = 123,        /* poisson per pixel    microscope.py:871 */
+  EDM_S_SC_DARK_BIN = 124,    /* integers per count   microscope.py:874 */
+  EDM_S_SC_AP = 125,          /* binomial per pixel   microscope.py:915 */
+  EDM_S_SC_AP_BIN = 126       /* integers per count   microscope.py:917 */
+};
+
+/* ---- dynamics parameter block (one per replica) -------------------------- */
+typedef struct {
+  int32_t sensor;        /* species counted                                   */
+  int32_t nx, ny;        /* grid dims, max(3, int(L/res)) (dynamics.py:1958)  */
+  int32_t pad;
+  double sx, sy;         /* cell sizes L/n                                    */
+  int64_t offset;        /* start of this grid in the global count array      */
+} EdmGrid;
+
+typedef struct {
+  int32_t grid;          /* index into EdmDynParams.grid                      */
+  int32_t inhibition;    /* 1: 1/(1+r^n); 0: a+(1-a) r^n/(1+r^n)              */
+  int32_t table_len;     /* exact Hill factors for counts 0..table_len-1      */
+  int32_t pad;
+  int64_t table_offset;  /* into the engine's hill table (float64)            */
+  double K_half, n_hill, basal, inv_area;
+} EdmRule;
+
+typedef struct {
+  int32_t ra, rb, product, pad;
+  double contact_sq;     /* sigma_eff^2 (dynamics.py:1900-1951)               */
+  double prob_bind, prob_dissoc;
+} EdmBind;
+
+typedef struct {
+  int32_t enzyme, substrate, product, rule;  /* rule -1: no feedback          */
+  double contact_sq, prob;
+} EdmCat;
+
+typedef struct {
+  int32_t species, max_recruits;
+  int32_t rule_on, rule_on2, rule_off, pad; /* -1 when absent                 */
+  double prob_on, prob_off;
+} EdmExch;
+
+typedef struct {
+  int32_t from, to, rule, pad;
+  double prob;
+} EdmConv;
+
+enum EdmDField { EDM_DFIELD_NONE = 0, EDM_DFIELD_REGIONS = 1, EDM_DFIELD_SINE_X = 2 };
+
+typedef struct {
+  /* domain / time */
+  double Lx, Ly, dt;
+  int32_t periodic_x, periodic_y;
+  /* cell list (dynamics.py:89-114, 1738-1788) */
+  int32_t nx, ny;
+  double cell_sx, cell_sy, cutoff_sq;
+  /* replica slices of the engine's global arrays */
+  int64_t particle_offset, n_particles;
+  int64_t cell_offset;
+  int64_t grid_cells;    /* total density-grid cells of this replica          */
+  /* BD (dynamics.py:323-406, 1837-1864) */
+  double max_disp, max_disp_sq;
+  int32_t use_wca, use_harmonic, n_species, dfield;
+  double D_base[EDM_MAX_SPECIES];
+  double sigma[EDM_MAX_SPECIES * EDM_MAX_SPECIES];
+  double eps[EDM_MAX_SPECIES * EDM_MAX_SPECIES];
+  double kharm[EDM_MAX_SPECIES * EDM_MAX_SPECIES];
+  /* D(x) field */
+  int32_t n_regions, pad0;
+  double reg_cx[EDM_MAX_REGIONS], reg_cy[EDM_MAX_REGIONS];
+  double reg_r[EDM_MAX_REGIONS], reg_f[EDM_MAX_REGIONS];
+  double smooth_w;
+  double sine_amp, sine_wavelength;  /* D = D0 (1 + amp sin(2 pi x / wl))   */
+  /* reactions, in the reference's pass order */
+  int32_t n_bind, n_cat, n_exch, n_conv, n_grids, n_rules;
+  EdmBind bind[EDM_MAX_BIND];
+  EdmCat cat[EDM_MAX_CAT];
+  EdmExch exch[EDM_MAX_EXCH];
+  EdmConv conv[EDM_MAX_CONV];
+  EdmGrid grid[EDM_MAX_GRIDS];
+  EdmRule rule[EDM_MAX_RULES];
+  /* noise key */
+  uint64_t seed;
+} EdmDynParams;
+
+/* ---- photophysics parameter block (photophysics.py:690-887) ------------- */
+typedef struct {
+  int32_t mode;          /* 0 bond, 1 proximity                               */
+  int32_t donor_fid, acceptor_fid, intramolecular;
+  int32_t cls_bound;     /* FRET class of a bonded donor (bond mode)          */
+  int32_t cls_high, cls_low;  /* proximity mode classes                       */
+  int32_t target_species;
+  double prox_radius_sq;
+} EdmFret;
+
+typedef struct {
+  int32_t n_fluoro, n_fret;
+  int32_t ground[EDM_MAX_FLUO], excited[EDM_MAX_FLUO], t1[EDM_MAX_FLUO], bl[EDM_MAX_FLUO];
+  /* per (fluorophore, pss state 0/1, FRET class): class 0 = no FRET */
+  double mean_d[EDM_MAX_FLUO][2][EDM_MAX_FCLASS];
+  double mean_f[EDM_MAX_FLUO][2][EDM_MAX_FCLASS];
+  double exp_neg_d[EDM_MAX_FLUO][2][EDM_MAX_FCLASS];  /* exp(-mean), host libm */
+  double exp_neg_f[EDM_MAX_FLUO][2][EDM_MAX_FCLASS];
+  double T00[EDM_MAX_FLUO][2][EDM_MAX_FCLASS];
+  double T0001[EDM_MAX_FLUO][2][EDM_MAX_FCLASS];      /* T00 + T01          */
+  double tau[EDM_MAX_FLUO][EDM_MAX_FCLASS];           /* tau_DA per class   */
+  double tau_all[EDM_MAX_FLUO];
+  int32_t has_fret_cls[EDM_MAX_FCLASS];               /* k_fret > 0         */
+  EdmFret fret[EDM_MAX_FRET];
+  int64_t max_photons, est_photons;
+  int64_t photon_offset; /* start of this replica's slice of the photon buffer */
+  int64_t emitter_offset, n_emitters;
+} EdmPhotParams;
+
+/* ---- microscope parameter block (microscope.py:73-1233) ------------------ */
+typedef struct {
+  int32_t nx, ny, n_bins, n_channels;   /* n_channels = max(2, n_fluoro)      */
+  int32_t psf_range_px, n_sigma;
+  double pixel_size, offset_x, offset_y;
+  double bin_width, sigma_irf, qe;
+  double sigma_ch[EDM_MAX_FLUO];        /* with the reference's fallbacks     */
+  double inv_2sig2_ch[EDM_MAX_FLUO];    /* 0.5/(sigma*sigma)                  */
+  double dark_lambda, dark_exp_neg;     /* dark_rate*dwell, exp(-lambda)      */
+  double ap_prob;
+  int64_t flim_offset;   /* start of this replica's stack (uint32 elements)   */
+} EdmScopeParams;
+
+/* ---- host-side particle state (id order, replicas concatenated) --------- */
+typedef struct {
+  int64_t n;             /* total particles over all replicas                 */
+  double* positions;     /* [n][2]                                            */
+  int32_t* species_id;
+  uint8_t* is_alive;
+  int32_t* bond_partner; /* replica-local particle index, -1 = free           */
+  uint8_t* has_dye;
+  int32_t* dye_type_id;
+  int8_t* ctmc_state;
+  uint8_t* is_bleached;
+} EdmHostState;
+
+/* per-replica counters, EDM_NCOUNTERS int64 each */
+enum EdmCounter {
+  EDM_C_BINDINGS = 0, EDM_C_DISSOC, EDM_C_CATALYTIC, EDM_C_RECRUITED,
+  EDM_C_DETACHED, EDM_C_CONVERTED,
+  EDM_C_PHOTONS, EDM_C_DONOR_PH, EDM_C_ACCEPTOR_PH, EDM_C_FRET_PH,
+  EDM_C_DETECTED, EDM_C_DARK, EDM_C_AFTERPULSE, EDM_C_RECEIVED,
+  EDM_NCOUNTERS
+};
+
+typedef struct EdmEngine EdmEngine;
+
+/* ---- versioning / layout checks ----------------------------------------- */
+int edm_abi_version(void);
+/* sizeof of the ABI structs: which = 0 EdmDynParams, 1 EdmPhotParams,
+ * 2 EdmScopeParams, 3 EdmHostState; lets a binding verify its mirror. */
+int64_t edm_abi_sizeof(int which);
+const char* edm_last_error(void);
+
+/* ---- engine lifetime ------------------------------------------------------
+ * Replaces DynamicsEngine.__init__ + PhotonSimulator.__init__ +
+ * VirtualMicroscope.__init__ (dynamics.py:1724, photophysics.py:693,
+ * microscope.py:1045): the host derives every float64 constant exactly as
+ * the reference does and hands the blocks over; the engine allocates device
+ * memory for all replicas.  precision: 64 = plain float64 path (absolute
+ * positions), 32 = float32 cell-relative path.  hill: exact Hill factors,
+ * indexed by EdmRule.table_offset.  phot/scope may be NULL (dynamics only). */
+int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot,
+               const EdmScopeParams* scope, int32_t n_replicas,
+               const double* hill, int64_t n_hill, int32_t precision,
+               int32_t device, EdmEngine** out);
+int edm_destroy(EdmEngine* eng);
+
+/* Host <-> device particle state, id order (ParticleState arrays). */
+int edm_set_state(EdmEngine* eng, const EdmHostState* st, void* stream);
+int edm_get_state(EdmEngine* eng, EdmHostState* st, void* stream);
+int edm_set_step(EdmEngine* eng, int64_t step_index);
+int64_t edm_get_step(EdmEngine* eng);
+
+/* DynamicsEngine.step() x n_steps (dynamics.py:2150-2465). */
+int edm_dynamics_step(EdmEngine* eng, int32_t n_steps, void* stream);
+
+/* PhotonSimulator.evolve_one_bd_step() (photophysics.py:1116-1197) for the
+ * current state; the batch stays on the device until edm_get_photons(). */
+int edm_photon_step(EdmEngine* eng, void* stream);
+/* Number of photons of the last batch per replica (host array [n_replicas]). */
+int edm_get_photon_counts(EdmEngine* eng, int64_t* counts, void* stream);
+/* Copy the last batch of one replica to host arrays (PhotonBatch fields). */
+int edm_get_photons(EdmEngine* eng, int32_t replica, int32_t* particle_idx,
+                    double* arrival_time, int8_t* channel, uint8_t* is_fret,
+                    int64_t capacity, void* stream);
+
+/* VirtualMicroscope.process_photons(batch) (microscope.py:1069-1157) on the
+ * last device batch. */
+int edm_scope_process(EdmEngine* eng, void* stream);
+
+/* One fused BD step of the whole pipeline loop body (pipeline.py:554-564):
+ * dynamics step, photophysics, photon processing; n_steps times, with the
+ * launch sequence captured into CUDA graphs of graph_chunk steps. */
+int edm_pipeline_steps(EdmEngine* eng, int32_t n_steps, int32_t with_photons,
+                       int32_t graph_chunk, void* stream);
+
+/* VirtualMicroscope.finalize_frame() (microscope.py:1159-1203): dark counts
+ * and afterpulsing into the stacks, keyed by frame_index.  Stacks stay on
+ * the device; read them with edm_get_flim and clear with edm_reset_flim. */
+int edm_scope_finalize(EdmEngine* eng, int64_t frame_index, void* stream);
+int edm_get_flim(EdmEngine* eng, int32_t replica, uint32_t* host_out,
+                 int64_t n_elems, void* stream);
+int edm_reset_flim(EdmEngine* eng, void* stream);
+
+/* Counters [n_replicas][EDM_NCOUNTERS] and the sticky status word. */
+int edm_get_counters(EdmEngine* eng, int64_t* out, void* stream);
+int edm_get_status(EdmEngine* eng, uint32_t* status, void* stream);
+
+/* Device pointer to the cell-list arrays of the last dynamics step
+ * (CellList.head/next equivalent, dynamics.py:109-138): per replica cell c
+ * holds particle indices sorted[start[c] .. start[c+1]) (global indices).  */
+int edm_get_cells(EdmEngine* eng, int32_t replica, int32_t* cell_start,
+                  int32_t* members, int64_t cap_cells, int64_t cap_members,
+                  void* stream);
+
+/* Noise of the engine's generator, for injection into the reference:
+ * writes n keyed standard normals pairs (2n doubles) / uniforms.  The
+ * arrays are device pointers; keys a[i] (particle / photon index). */
+int edm_noise_normal_pairs(uint64_t seed, int64_t step, int32_t stream_id,
+                           const int64_t* keys_dev, int64_t n, double* out_dev,
+                           void* stream);
+int edm_noise_uniforms(uint64_t seed, int64_t step, int32_t stream_id,
+                       const int64_t* keys_a_dev, const int64_t* keys_b_dev,
+                       int64_t n, double* out2_dev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EDM_B200_H */
