@@ -1,0 +1,174 @@
+// edm_common.cuh — device helpers shared by every kernel of the engine.
+//
+// Keyed noise: Philox4x32-10 (Salmon et al., SC'11) with counter
+// (a, b, step_lo, stream<<16 | step_hi) and key = seed; 64-bit words map to
+// uniforms (x >> 11) * 2^-53.  Standard normals come from the Marsaglia polar
+// method with a fixed-order atanh-series logarithm, every float64 operation
+// an explicit round-to-nearest intrinsic (no contraction), so a host
+// implementation that evaluates the same sequence gets the same bits.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/edm_b200.h"
+
+namespace edm {
+
+constexpr uint32_t kM0 = 0xD2511F53u, kM1 = 0xCD9E8D57u;
+constexpr uint32_t kW0 = 0x9E3779B9u, kW1 = 0xBB67AE85u;
+
+struct U2 {
+  double u0, u1;
+};
+
+__device__ __forceinline__ void philox10(uint32_t& c0, uint32_t& c1, uint32_t& c2, uint32_t& c3,
+                                         uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t hi0 = __umulhi(kM0, c0), lo0 = kM0 * c0;
+    const uint32_t hi1 = __umulhi(kM1, c2), lo1 = kM1 * c2;
+    const uint32_t n0 = hi1 ^ c1 ^ k0;
+    const uint32_t n2 = hi0 ^ c3 ^ k1;
+    c0 = n0;
+    c1 = lo1;
+    c2 = n2;
+    c3 = lo0;
+    k0 += kW0;
+    k1 += kW1;
+  }
+}
+
+__device__ __forceinline__ U2 uniform2(uint64_t seed, int64_t step, int stream, uint64_t a, uint64_t b) {
+  uint32_t c0 = (uint32_t)a, c1 = (uint32_t)b, c2 = (uint32_t)((uint64_t)step);
+  uint32_t c3 = ((uint32_t)stream << 16) | (uint32_t)(((uint64_t)step >> 32) & 0xFFFFu);
+  philox10(c0, c1, c2, c3, (uint32_t)seed, (uint32_t)(seed >> 32));
+  const uint64_t x0 = ((uint64_t)c1 << 32) | c0;
+  const uint64_t x1 = ((uint64_t)c3 << 32) | c2;
+  U2 r;
+  r.u0 = __dmul_rn(__ull2double_rn(x0 >> 11), 0x1p-53);
+  r.u1 = __dmul_rn(__ull2double_rn(x1 >> 11), 0x1p-53);
+  return r;
+}
+
+__device__ __forceinline__ double uniform1(uint64_t seed, int64_t step, int stream, uint64_t a, uint64_t b) {
+  return uniform2(seed, step, stream, a, b).u0;
+}
+
+// ln q by the atanh series (Abramowitz & Stegun 4.1.27), q = m 2^e with
+// m in [sqrt(1/2), sqrt(2)), s = (m-1)/(m+1), 12 odd terms, Horner in s^2.
+__device__ __forceinline__ double ln_series(double q) {
+  const uint64_t bits = (uint64_t)__double_as_longlong(q);
+  int e = (int)((bits >> 52) & 0x7FF) - 1023;
+  double m = __longlong_as_double((long long)((bits & 0x000FFFFFFFFFFFFFull) | 0x3FF0000000000000ull));
+  if (m > 0x1.6a09e667f3bcdp+0) {
+    m = __dmul_rn(m, 0.5);
+    e += 1;
+  }
+  const double s = __ddiv_rn(__dadd_rn(m, -1.0), __dadd_rn(m, 1.0));
+  const double s2 = __dmul_rn(s, s);
+  double p = 0x1.642c8590b2164p-5;                   // 1/23
+  p = __dadd_rn(__dmul_rn(p, s2), 0x1.8618618618618p-5);  // 1/21
+  p = __dadd_rn(__dmul_rn(p, s2), 0x1.af286bca1af28p-5);  // 1/19
+  p = __dadd_rn(__dmul_rn(p, s2), 0x1.e1e1e1e1e1e1ep-5);  // 1/17
+  p = __dadd_rn(__dmul_rn(p, s2), 0x1.1111111111111p-4);  // 1/15
+  p = __dadd_rn(__dmul_rn(p, s2), 0x1.3b13b13b13b14p-4);  // 1/13
+  p = __dadd_rn(__dmul_rn(p, s2), 0x1.745d1745d1746p-4);  // 1/11
+  p = __dadd_rn(__dmul_rn(p, s2), 0x1.c71c71c71c71cp-4);  // 1/9
+  p = __dadd_rn(__dmul_rn(p, s2), 0x1.2492492492492p-3);  // 1/7
+  p = __dadd_rn(__dmul_rn(p, s2), 0x1.999999999999ap-3);  // 1/5
+  p = __dadd_rn(__dmul_rn(p, s2), 0x1.5555555555555p-2);  // 1/3
+  p = __dadd_rn(__dmul_rn(p, s2), 1.0);
+  const double lnm = __dmul_rn(__dmul_rn(2.0, s), p);
+  const double de = (double)e;
+  return __dadd_rn(__dmul_rn(de, 0x1.62e42fee00000p-1),
+                   __dadd_rn(__dmul_rn(de, 0x1.a39ef35793c76p-33), lnm));
+}
+
+// Standard normal pair, Marsaglia polar method; attempt t uses counter b = t.
+__device__ __forceinline__ U2 normal2(uint64_t seed, int64_t step, int stream, uint64_t a) {
+  U2 z;
+  for (uint32_t t = 0; t < 64; ++t) {
+    const U2 u = uniform2(seed, step, stream, a, t);
+    const double x = __dadd_rn(__dmul_rn(2.0, u.u0), -1.0);
+    const double y = __dadd_rn(__dmul_rn(2.0, u.u1), -1.0);
+    const double q = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
+    if (q > 0.0 && q < 1.0) {
+      const double f = __dsqrt_rn(__ddiv_rn(__dmul_rn(-2.0, ln_series(q)), q));
+      z.u0 = __dmul_rn(x, f);
+      z.u1 = __dmul_rn(y, f);
+      return z;
+    }
+  }
+  z.u0 = 0.0;
+  z.u1 = 0.0;
+  return z;
+}
+
+// ---- particle flags: bits 0-6 species, bit 7 alive -------------------------
+__device__ __forceinline__ int fl_species(uint8_t f) { return f & 0x7F; }
+__device__ __forceinline__ bool fl_alive(uint8_t f) { return (f & 0x80) != 0; }
+__device__ __forceinline__ uint8_t fl_make(int sp, bool alive) { return (uint8_t)((sp & 0x7F) | (alive ? 0x80 : 0)); }
+
+// byte compare-and-swap on the containing 32-bit word
+__device__ __forceinline__ bool cas_u8(uint8_t* addr, uint8_t expect, uint8_t desired) {
+  unsigned int* w = (unsigned int*)((uintptr_t)addr & ~(uintptr_t)3);
+  const unsigned int sh = ((uintptr_t)addr & 3u) * 8u;
+  unsigned int old = *((volatile unsigned int*)w);
+  for (int it = 0; it < 1 << 20; ++it) {
+    const uint8_t cur = (uint8_t)((old >> sh) & 0xFFu);
+    if (cur != expect) return false;
+    const unsigned int nw = (old & ~(0xFFu << sh)) | ((unsigned int)desired << sh);
+    const unsigned int prev = atomicCAS(w, old, nw);
+    if (prev == old) return true;
+    old = prev;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void atomic_add_i64(int64_t* p, long long v) {
+  atomicAdd((unsigned long long*)p, (unsigned long long)v);
+}
+
+__device__ __forceinline__ void set_status(uint32_t* st, uint32_t bit) { atomicOr(st, bit); }
+
+__device__ __forceinline__ int clampi(int v, int n) {
+  v = v >= n ? n - 1 : v;
+  return v < 0 ? 0 : v;
+}
+
+// Python float `%` (floor-mod), as Numba evaluates positions % L.
+__device__ __forceinline__ double py_fmod(double x, double L) {
+  double r = fmod(x, L);
+  if (r != 0.0) {
+    if ((r < 0.0) != (L < 0.0)) r = __dadd_rn(r, L);
+  } else {
+    r = copysign(0.0, L);
+  }
+  return r;
+}
+
+// Reference cell index of an absolute coordinate: int(x / s) clamped.
+__device__ __forceinline__ int cell_index(double x, double s, int n) {
+  return clampi((int)__ddiv_rn(x, s), n);
+}
+
+// Hill factor of rule R at grid count k: exact table, or (beyond the table)
+// the reference expression evaluated on the device with the exact density.
+__device__ __forceinline__ double hill_of(const EdmRule& R, const double* __restrict__ hill, int k,
+                                          uint32_t* status) {
+  if (k < R.table_len) return hill[R.table_offset + k];
+  set_status(status, EDM_STATUS_HILL_RANGE);
+  double rho = 0.0;
+  for (int i = 0; i < k; ++i) rho = __dadd_rn(rho, R.inv_area);
+  if (R.K_half > 0) {
+    const double ratio = __ddiv_rn(rho, R.K_half);
+    const double rn = pow(ratio, R.n_hill);
+    if (R.inhibition) return __ddiv_rn(1.0, __dadd_rn(1.0, rn));
+    const double h = __ddiv_rn(rn, __dadd_rn(1.0, rn));
+    return __dadd_rn(R.basal, __dmul_rn(__dadd_rn(1.0, -R.basal), h));
+  }
+  return 1.0;
+}
+
+}  // namespace edm

@@ -1,0 +1,949 @@
+// edm_dyn.cuh — dynamics kernels (one BD step of DynamicsEngine.step,
+// ed_mrdt/dynamics.py:2150-2465) for all replicas of an engine.
+//
+// Layout.  Per step the particles of every replica are counting-sorted by
+// their reference cell (dynamics.py:176-196: cx = int(x/cell_sx) clamped,
+// key cx*ny + cy) into "slots"; replica r owns slots
+// [particle_offset, particle_offset + n_particles) and cells
+// [cell_offset, cell_offset + nx*ny).  Slot arrays: position (float64
+// absolute, or float32 offset inside the cell + the integer cell), the cell,
+// one flag byte (species | alive<<7) and the particle id.  Id-indexed arrays
+// (bond partner, dye, photophysical state) do not move.
+//
+// Order independence.  The slot order inside a cell comes from atomics and is
+// not deterministic; nothing downstream depends on it:
+//  - pair forces are summed per particle in the reference's own pair order
+//    (its (j, i) pairs by ascending j, then its (i, j) pairs by neighbour-cell
+//    ordinal and descending j; WCA terms before harmonic terms), recovered
+//    from particle ids and cells;
+//  - every random draw is keyed by particle ids, not by storage position;
+//  - reaction passes are set-valued (catalysis) or per particle; the two
+//    order-dependent rules (binding's greedy pair order, the recruitment cap
+//    in index order) are resolved on small candidate lists sorted by the
+//    reference's order key.
+#pragma once
+
+#include "edm_common.cuh"
+
+namespace edm {
+
+constexpr int kBlock = 256;
+
+struct DevState {
+  void* pos_pre;      // double2 (f64) or float2 (f32 offsets), slot order, before the move
+  void* pos_post;     // same, after the move
+  int32_t* cell_pre;  // local cell of each slot, before the move
+  int32_t* cell_post;
+  const uint8_t* flags_old;
+  uint8_t* flags;     // slot flags of the current step
+  const int32_t* ids_old;
+  int32_t* ids;       // global particle id of each slot
+  int32_t* slot_of_id;
+  int32_t* bond;      // id-indexed, global id or -1
+  int32_t* cell_start;   // [n_cells + 1]
+  int32_t* cell_cursor;
+  int32_t* cnt_next;     // cell counts of the post-move positions
+  int32_t* grid_cnt;     // density-grid counts (snapshot of the current pass)
+  int32_t* grid_delta;   // pending changes of the current pass
+  const double* hill;
+  int64_t* counters;     // [R][EDM_NCOUNTERS]
+  uint32_t* status;
+  const int64_t* d_step;
+  // candidate buffers
+  int32_t* rec_count;    // [R]
+  int32_t* rec_id;       // [R][kRecCap] local id
+  double* rec_xy;        // [R][kRecCap][2]
+  int32_t* bind_count;   // [R]
+  int64_t* bind_key;     // [R][kBindCap]
+  int32_t* bind_ab;      // [R][kBindCap][2] local ids (a = reactant A role, b = B role)
+};
+
+constexpr int kRecCap = 128;
+constexpr int kBindCap = 512;
+
+// ---- replica geometry --------------------------------------------------------
+struct Geo {
+  int nx, ny, px, py;
+  double Lx, Ly, sx, sy, cutoff_sq;
+  float sxf, syf;
+  int64_t cbase, poff;
+  __device__ __forceinline__ explicit Geo(const EdmDynParams& p)
+      : nx(p.nx), ny(p.ny), px(p.periodic_x), py(p.periodic_y), Lx(p.Lx), Ly(p.Ly),
+        sx(p.cell_sx), sy(p.cell_sy), cutoff_sq(p.cutoff_sq), sxf((float)p.cell_sx),
+        syf((float)p.cell_sy), cbase(p.cell_offset), poff(p.particle_offset) {}
+};
+
+// Absolute position of a slot (float64).
+template <bool F64>
+__device__ __forceinline__ void abs_pos(const void* pos, const int32_t* cell, int64_t s, const Geo& g,
+                                        double& x, double& y) {
+  if constexpr (F64) {
+    const double2 v = ((const double2*)pos)[s];
+    x = v.x;
+    y = v.y;
+  } else {
+    const float2 v = ((const float2*)pos)[s];
+    const int c = cell[s];
+    const int cx = c / g.ny, cy = c - (c / g.ny) * g.ny;
+    x = __dadd_rn(__dmul_rn((double)cx, g.sx), (double)v.x);
+    y = __dadd_rn(__dmul_rn((double)cy, g.sy), (double)v.y);
+  }
+}
+
+// Reference minimum-image separation (dynamics.py:199-216) of absolute points.
+__device__ __forceinline__ double min_image_sq(double x1, double y1, double x2, double y2, const Geo& g,
+                                               double& dx, double& dy) {
+  dx = x1 - x2;
+  dy = y1 - y2;
+  if (g.px) {
+    if (dx > 0.5 * g.Lx) dx -= g.Lx;
+    else if (dx < -0.5 * g.Lx) dx += g.Lx;
+  }
+  if (g.py) {
+    if (dy > 0.5 * g.Ly) dy -= g.Ly;
+    else if (dy < -0.5 * g.Ly) dy += g.Ly;
+  }
+  return dx * dx + dy * dy;
+}
+
+// float32 separation of two cell-relative points (cells ci, cj).
+__device__ __forceinline__ float rel_sq_f32(int ci, float2 oi, int cj, float2 oj, const Geo& g, float& dx,
+                                            float& dy) {
+  const int cxi = ci / g.ny, cyi = ci - cxi * g.ny;
+  const int cxj = cj / g.ny, cyj = cj - cxj * g.ny;
+  int dcx = cxi - cxj, dcy = cyi - cyj;
+  if (g.px) {
+    if (2 * dcx > g.nx) dcx -= g.nx;
+    else if (2 * dcx < -g.nx) dcx += g.nx;
+  }
+  if (g.py) {
+    if (2 * dcy > g.ny) dcy -= g.ny;
+    else if (2 * dcy < -g.ny) dcy += g.ny;
+  }
+  dx = (float)dcx * g.sxf + (oi.x - oj.x);
+  dy = (float)dcy * g.syf + (oi.y - oj.y);
+  return dx * dx + dy * dy;
+}
+
+// Squared separation of slots a and b in the given position array.
+template <bool F64>
+__device__ __forceinline__ double sep_sq(const void* pos, const int32_t* cell, int64_t a, int64_t b,
+                                         const Geo& g) {
+  if constexpr (F64) {
+    const double2 pa = ((const double2*)pos)[a], pb = ((const double2*)pos)[b];
+    double dx, dy;
+    return min_image_sq(pa.x, pa.y, pb.x, pb.y, g, dx, dy);
+  } else {
+    float dx, dy;
+    return (double)rel_sq_f32(cell[a], ((const float2*)pos)[a], cell[b], ((const float2*)pos)[b], g, dx, dy);
+  }
+}
+
+// Replica r and slot s of this thread (block table of kBlock-slot tiles).
+struct Tile {
+  int r;
+  int64_t s;
+};
+__device__ __forceinline__ Tile tile_of(const int2* blk) {
+  const int2 b = blk[blockIdx.x];
+  Tile t;
+  t.r = b.x;
+  t.s = (int64_t)(uint32_t)b.y + threadIdx.x;
+  return t;
+}
+
+// ---- density grids -----------------------------------------------------------
+__device__ __forceinline__ int64_t grid_cell_of(const EdmGrid& G, double x, double y) {
+  const int gx = clampi((int)__ddiv_rn(x, G.sx), G.nx);
+  const int gy = clampi((int)__ddiv_rn(y, G.sy), G.ny);
+  return G.offset + (int64_t)gx * G.ny + gy;
+}
+
+// Add d to every grid counting species sp, at (x, y) — into `arr`.
+__device__ __forceinline__ void grid_add(const EdmDynParams& p, int32_t* arr, int sp, double x, double y, int d) {
+  for (int g = 0; g < p.n_grids; ++g) {
+    if (p.grid[g].sensor == sp) atomicAdd(&arr[grid_cell_of(p.grid[g], x, y)], d);
+  }
+}
+
+__device__ __forceinline__ double rule_factor(const EdmDynParams& p, int rule, const DevState& st, double x,
+                                              double y) {
+  const EdmRule& R = p.rule[rule];
+  const int k = st.grid_cnt[grid_cell_of(p.grid[R.grid], x, y)];
+  return hill_of(R, st.hill, k, st.status);
+}
+
+// =============================================================================
+// Cell list: exclusive scan of the post-move cell counts, scatter into slots.
+// =============================================================================
+constexpr int kScanThreads = 512;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int& total) {
+  __shared__ int warp_sums[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sums[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+    int w = lane < nw ? warp_sums[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < nw) warp_sums[lane] = w;
+  }
+  __syncthreads();
+  const int base = wid > 0 ? warp_sums[wid - 1] : 0;
+  total = warp_sums[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return base + x - v;
+}
+
+__global__ void k_scan_reduce(const int32_t* __restrict__ cnt, int64_t n, int32_t* __restrict__ bsum) {
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  int v = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i)
+    if (base + i < n) v += cnt[base + i];
+  int total;
+  block_exclusive_scan(v, total);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+__global__ void k_scan_bsum(int32_t* __restrict__ bsum, int nb) {
+  int carry = 0;
+  for (int off = 0; off < nb; off += blockDim.x) {
+    const int i = off + threadIdx.x;
+    const int v = i < nb ? bsum[i] : 0;
+    int total;
+    const int ex = block_exclusive_scan(v, total);
+    if (i < nb) bsum[i] = carry + ex;
+    carry += total;
+  }
+}
+
+__global__ void k_scan_down(int32_t* __restrict__ cnt, int64_t n, const int32_t* __restrict__ bsum,
+                            int32_t* __restrict__ start, int32_t* __restrict__ cursor) {
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  int vals[kScanItems];
+  int v = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    vals[i] = base + i < n ? cnt[base + i] : 0;
+    v += vals[i];
+  }
+  int total;
+  int run = block_exclusive_scan(v, total) + bsum[blockIdx.x];
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    if (base + i < n) {
+      start[base + i] = run;
+      cursor[base + i] = run;
+      cnt[base + i] = 0;
+    }
+    run += vals[i];
+  }
+  // the thread holding element n-1 writes the sentinel start[n]
+  if (base < n && base + kScanItems >= n) start[n] = run;
+  if (n == 0 && blockIdx.x == 0 && threadIdx.x == 0) start[0] = 0;
+}
+
+template <bool F64>
+__global__ void __launch_bounds__(kBlock) k_scatter(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk,
+                                                    DevState st) {
+  const Tile t = tile_of(blk);
+  const EdmDynParams& p = P[t.r];
+  if (t.s >= p.particle_offset + p.n_particles) return;
+  const int c = st.cell_post[t.s];
+  const int d = atomicAdd(&st.cell_cursor[p.cell_offset + c], 1);
+  if constexpr (F64) {
+    ((double2*)st.pos_pre)[d] = ((const double2*)st.pos_post)[t.s];
+  } else {
+    ((float2*)st.pos_pre)[d] = ((const float2*)st.pos_post)[t.s];
+  }
+  st.cell_pre[d] = c;
+  st.flags[d] = st.flags_old[t.s];
+  const int id = st.ids_old[t.s];
+  st.ids[d] = id;
+  st.slot_of_id[id] = d;
+}
+
+// =============================================================================
+// Forces + Ermak–McCammon move (dynamics.py:440-519, 665-816, 323-406).
+// =============================================================================
+struct ForceTerm {
+  uint64_t key;
+  double fx, fy;
+};
+
+// Enumerate the pair-force terms of slot s; pass `emit(key, fx, fy)`.
+template <bool F64, typename Emit>
+__device__ __forceinline__ void for_each_force_term(const EdmDynParams& p, const Geo& g, const DevState& st,
+                                                    int64_t s, int sp, int id, Emit emit) {
+  const int c = st.cell_pre[s];
+  const int cx = c / g.ny, cy = c - (c / g.ny) * g.ny;
+  double xi = 0, yi = 0;
+  float2 oi = make_float2(0.f, 0.f);
+  if constexpr (F64) {
+    const double2 v = ((const double2*)st.pos_pre)[s];
+    xi = v.x;
+    yi = v.y;
+  } else {
+    oi = ((const float2*)st.pos_pre)[s];
+  }
+  for (int dcx = -1; dcx <= 1; ++dcx) {
+    int ncx = cx + dcx;
+    if (g.px) ncx = ncx < 0 ? ncx + g.nx : (ncx >= g.nx ? ncx - g.nx : ncx);
+    else if (ncx < 0 || ncx >= g.nx) continue;
+    for (int dcy = -1; dcy <= 1; ++dcy) {
+      int ncy = cy + dcy;
+      if (g.py) ncy = ncy < 0 ? ncy + g.ny : (ncy >= g.ny ? ncy - g.ny : ncy);
+      else if (ncy < 0 || ncy >= g.ny) continue;
+      const int64_t nc = g.cbase + (int64_t)ncx * g.ny + ncy;
+      const int ordinal = (dcx + 1) * 3 + (dcy + 1);
+      const int j0 = st.cell_start[nc], j1 = st.cell_start[nc + 1];
+      for (int j = j0; j < j1; ++j) {
+        if (j == s) continue;
+        const uint8_t fj = st.flags[j];
+        if (!fl_alive(fj)) continue;
+        const int spj = fl_species(fj);
+        const double sig = p.sigma[sp * EDM_MAX_SPECIES + spj];
+        if (!(sig > 0.0)) continue;
+        // separation i - j and the pair-list cutoff test (dynamics.py:262-268)
+        double dx, dy, dsq;
+        if constexpr (F64) {
+          const double2 v = ((const double2*)st.pos_pre)[j];
+          dsq = min_image_sq(xi, yi, v.x, v.y, g, dx, dy);
+          if (!(dsq < g.cutoff_sq)) continue;
+        } else {
+          const float2 oj = ((const float2*)st.pos_pre)[j];
+          const float fdx = -(float)dcx * g.sxf + (oi.x - oj.x);
+          const float fdy = -(float)dcy * g.syf + (oi.y - oj.y);
+          const float fdsq = fdx * fdx + fdy * fdy;
+          if (!((double)fdsq < g.cutoff_sq)) continue;
+          dx = fdx;
+          dy = fdy;
+          dsq = fdsq;
+        }
+        const int idj = st.ids[j] - (int)g.poff;
+        const uint64_t order = idj < id ? (uint64_t)idj
+                                        : ((1ull << 60) | ((uint64_t)ordinal << 32) | (uint64_t)(0xFFFFFFFFu - (uint32_t)idj));
+        if (p.use_wca) {
+          const double eps = p.eps[sp * EDM_MAX_SPECIES + spj];
+          if (eps > 0.0) {
+            if constexpr (F64) {
+              const double rcut2 = sig * sig * 1.2599210498948732;
+              if (dsq < rcut2 && dsq >= 1e-30) {
+                const double inv_r2 = 1.0 / dsq;
+                const double s2 = sig * sig * inv_r2;
+                const double s6 = s2 * s2 * s2;
+                const double s12 = s6 * s6;
+                double f = 24.0 * eps * (2.0 * s12 - s6) * inv_r2;
+                const double fmax = 2400.0 * eps / (sig * sig);
+                if (f > fmax) f = fmax;
+                emit(order, f * dx, f * dy);
+              }
+            } else {
+              const float sgf = (float)sig, epf = (float)eps;
+              const float fd = (float)dsq;
+              const float rcut2 = sgf * sgf * 1.2599210498948732f;
+              if (fd < rcut2 && fd >= 1e-30f) {
+                const float inv_r2 = 1.0f / fd;
+                const float s2 = sgf * sgf * inv_r2;
+                const float s6 = s2 * s2 * s2;
+                const float s12 = s6 * s6;
+                float f = 24.0f * epf * (2.0f * s12 - s6) * inv_r2;
+                const float fmax = 2400.0f * epf / (sgf * sgf);
+                if (f > fmax) f = fmax;
+                emit(order, (double)(f * (float)dx), (double)(f * (float)dy));
+              }
+            }
+          }
+        }
+        if (p.use_harmonic) {
+          const double k = p.kharm[sp * EDM_MAX_SPECIES + spj];
+          if (k > 0.0) {
+            if constexpr (F64) {
+              const double s2 = sig * sig;
+              if (dsq < s2 && dsq >= 1e-30) {
+                const double r = sqrt(dsq);
+                const double f = k * (sig - r) / r;
+                emit(order | (1ull << 62), f * dx, f * dy);
+              }
+            } else {
+              const float sgf = (float)sig, kf = (float)k, fd = (float)dsq;
+              if (fd < sgf * sgf && fd >= 1e-30f) {
+                const float r = sqrtf(fd);
+                const float f = kf * (sgf - r) / r;
+                emit(order | (1ull << 62), (double)(f * (float)dx), (double)(f * (float)dy));
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+// D(x) and grad D at an absolute position (dynamics.py:440-519; sine-x field).
+__device__ __forceinline__ void dfield(const EdmDynParams& p, int sp, double x, double y, double& D, double& gx,
+                                       double& gy) {
+  const double base = p.D_base[sp];
+  double factor = 1.0, gfx = 0.0, gfy = 0.0;
+  if (p.dfield == EDM_DFIELD_REGIONS) {
+    for (int reg = 0; reg < p.n_regions; ++reg) {
+      const double dxc = x - p.reg_cx[reg], dyc = y - p.reg_cy[reg];
+      const double dsq = dxc * dxc + dyc * dyc;
+      const double d = dsq > 1e-30 ? sqrt(dsq) : 1e-15;
+      const double arg = (d - p.reg_r[reg]) / p.smooth_w;
+      double sig, dsig;
+      if (arg > 100.0) {
+        sig = 0.0;
+        dsig = 0.0;
+      } else if (arg < -100.0) {
+        sig = 1.0;
+        dsig = 0.0;
+      } else {
+        const double ea = exp(arg);
+        const double den = 1.0 + ea;
+        sig = 1.0 / den;
+        dsig = -ea / (den * den * p.smooth_w);
+      }
+      const double local = 1.0 + (p.reg_f[reg] - 1.0) * sig;
+      if (sig > 0.01) {
+        factor = local;
+        const double inv_d = 1.0 / d;
+        gfx = (p.reg_f[reg] - 1.0) * dsig * dxc * inv_d;
+        gfy = (p.reg_f[reg] - 1.0) * dsig * dyc * inv_d;
+        break;
+      }
+    }
+    D = base * factor;
+    gx = base * gfx;
+    gy = base * gfy;
+  } else if (p.dfield == EDM_DFIELD_SINE_X) {
+    const double w = 2.0 * 3.141592653589793 / p.sine_wavelength;
+    const double ph = w * x;
+    double sn, cs;
+    sincos(ph, &sn, &cs);
+    D = base * (1.0 + p.sine_amp * sn);
+    gx = base * p.sine_amp * w * cs;
+    gy = 0.0;
+  } else {
+    D = base * factor;
+    gx = base * gfx;
+    gy = base * gfy;
+  }
+}
+
+template <bool F64>
+__global__ void __launch_bounds__(kBlock) k_move(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk,
+                                                 DevState st) {
+  const Tile t = tile_of(blk);
+  const EdmDynParams& p = P[t.r];
+  const int64_t s = t.s;
+  if (s >= p.particle_offset + p.n_particles) return;
+  const Geo g(p);
+  const uint8_t f = st.flags[s];
+  const int c = st.cell_pre[s];
+  if (!fl_alive(f)) {  // dead / dormant particles do not move (dynamics.py:360)
+    if constexpr (F64) {
+      ((double2*)st.pos_post)[s] = ((const double2*)st.pos_pre)[s];
+    } else {
+      ((float2*)st.pos_post)[s] = ((const float2*)st.pos_pre)[s];
+    }
+    st.cell_post[s] = c;
+    atomicAdd(&st.cnt_next[g.cbase + c], 1);
+    return;
+  }
+  const int sp = fl_species(f);
+  const int id = st.ids[s] - (int)g.poff;
+  const int64_t step = *st.d_step;
+
+  // pair forces, in the reference's accumulation order
+  double Fx = 0.0, Fy = 0.0;
+  int nterms = 0;
+  for_each_force_term<F64>(p, g, st, s, sp, id, [&](uint64_t, double fx, double fy) {
+    ++nterms;
+    Fx += fx;
+    Fy += fy;
+  });
+  if (nterms > 1) {
+    Fx = 0.0;
+    Fy = 0.0;
+    uint64_t last = 0;
+    bool first = true;
+    for (int k = 0; k < nterms; ++k) {
+      uint64_t best = ~0ull;
+      double bx = 0.0, by = 0.0;
+      for_each_force_term<F64>(p, g, st, s, sp, id, [&](uint64_t key, double fx, double fy) {
+        if ((first || key > last) && key < best) {
+          best = key;
+          bx = fx;
+          by = fy;
+        }
+      });
+      Fx += bx;
+      Fy += by;
+      last = best;
+      first = false;
+    }
+  }
+
+  double x, y;
+  abs_pos<F64>(st.pos_pre, st.cell_pre, s, g, x, y);
+  double Di, gDx, gDy;
+  dfield(p, sp, x, y, Di, gDx, gDy);
+  const U2 z = normal2(p.seed, step, EDM_S_BD_NORMAL, (uint64_t)id);
+  const double dt = p.dt;
+  int newc;
+  if constexpr (F64) {
+    const double sn = sqrt(2.0 * Di * dt);
+    double dxt = gDx * dt, dyt = gDy * dt;
+    dxt += sn * z.u0;
+    dyt += sn * z.u1;
+    dxt += Di * Fx * dt;
+    dyt += Di * Fy * dt;
+    const double dr2 = dxt * dxt + dyt * dyt;
+    if (dr2 > p.max_disp_sq) {
+      const double scale = p.max_disp / sqrt(dr2);
+      dxt *= scale;
+      dyt *= scale;
+    }
+    x += dxt;
+    y += dyt;
+    if (g.px) x = py_fmod(x, g.Lx);
+    else if (x < 0.0) x = -x;
+    else if (x >= g.Lx) x = 2.0 * g.Lx - x;
+    if (g.py) y = py_fmod(y, g.Ly);
+    else if (y < 0.0) y = -y;
+    else if (y >= g.Ly) y = 2.0 * g.Ly - y;
+    if (!isfinite(x) || !isfinite(y)) set_status(st.status, EDM_STATUS_NONFINITE);
+    ((double2*)st.pos_post)[s] = make_double2(x, y);
+    newc = cell_index(x, g.sx, g.nx) * g.ny + cell_index(y, g.sy, g.ny);
+  } else {
+    const float Dif = (float)Di, dtf = (float)dt;
+    const float sn = sqrtf(2.0f * Dif * dtf);
+    float dxt = (float)gDx * dtf + sn * (float)z.u0 + Dif * (float)Fx * dtf;
+    float dyt = (float)gDy * dtf + sn * (float)z.u1 + Dif * (float)Fy * dtf;
+    const float dr2 = dxt * dxt + dyt * dyt;
+    if ((double)dr2 > p.max_disp_sq) {
+      const float scale = (float)p.max_disp / sqrtf(dr2);
+      dxt *= scale;
+      dyt *= scale;
+    }
+    float2 o = ((const float2*)st.pos_pre)[s];
+    int cx = c / g.ny, cy = c - (c / g.ny) * g.ny;
+    o.x += dxt;
+    o.y += dyt;
+    // renormalise into [0, cell) and carry the integer cell
+    for (int it = 0; it < 64 && o.x >= g.sxf; ++it) { o.x -= g.sxf; ++cx; }
+    for (int it = 0; it < 64 && o.x < 0.0f; ++it) { o.x += g.sxf; --cx; }
+    for (int it = 0; it < 64 && o.y >= g.syf; ++it) { o.y -= g.syf; ++cy; }
+    for (int it = 0; it < 64 && o.y < 0.0f; ++it) { o.y += g.syf; --cy; }
+    if (o.x >= g.sxf || o.x < 0.0f) o.x = 0.0f;
+    if (o.y >= g.syf || o.y < 0.0f) o.y = 0.0f;
+    if (g.px) {
+      cx = cx % g.nx;
+      if (cx < 0) cx += g.nx;
+    } else if (cx < 0 || cx >= g.nx) {  // reflecting wall, in float64
+      double ax = (double)cx * g.sx + (double)o.x;
+      if (ax < 0.0) ax = -ax;
+      else if (ax >= g.Lx) ax = 2.0 * g.Lx - ax;
+      cx = cell_index(ax, g.sx, g.nx);
+      o.x = (float)(ax - (double)cx * g.sx);
+    }
+    if (g.py) {
+      cy = cy % g.ny;
+      if (cy < 0) cy += g.ny;
+    } else if (cy < 0 || cy >= g.ny) {
+      double ay = (double)cy * g.sy + (double)o.y;
+      if (ay < 0.0) ay = -ay;
+      else if (ay >= g.Ly) ay = 2.0 * g.Ly - ay;
+      cy = cell_index(ay, g.sy, g.ny);
+      o.y = (float)(ay - (double)cy * g.sy);
+    }
+    if (!isfinite(o.x) || !isfinite(o.y)) set_status(st.status, EDM_STATUS_NONFINITE);
+    ((float2*)st.pos_post)[s] = o;
+    newc = cx * g.ny + cy;
+    x = (double)cx * g.sx + (double)o.x;
+    y = (double)cy * g.sy + (double)o.y;
+  }
+  st.cell_post[s] = newc;
+  atomicAdd(&st.cnt_next[g.cbase + newc], 1);
+  grid_add(p, st.grid_cnt, sp, x, y, 1);
+}
+
+// =============================================================================
+// Reactions.
+// =============================================================================
+
+// Grid bookkeeping of a particle changing (species, alive) at one position.
+__device__ __forceinline__ void grid_change(const EdmDynParams& p, int32_t* delta, int sp_old, bool alive_old,
+                                            int sp_new, bool alive_new, double x, double y) {
+  if (alive_old) grid_add(p, delta, sp_old, x, y, -1);
+  if (alive_new) grid_add(p, delta, sp_new, x, y, +1);
+}
+
+// Catalytic pass c (dynamics.py:825-983): the set of substrates with at least
+// one accepted (enzyme, substrate) candidate pair is converted.
+template <bool F64>
+__global__ void __launch_bounds__(kBlock) k_catalytic(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk,
+                                                      DevState st, int cidx) {
+  const Tile t = tile_of(blk);
+  const EdmDynParams& p = P[t.r];
+  const int64_t s = t.s;
+  if (s >= p.particle_offset + p.n_particles) return;
+  const EdmCat& C = p.cat[cidx];
+  const uint8_t f = st.flags[s];
+  if (!fl_alive(f) || fl_species(f) != C.enzyme) return;
+  const Geo g(p);
+  const int64_t step = *st.d_step;
+  const int ide = st.ids[s] - (int)g.poff;
+  const int c = st.cell_pre[s];
+  const int cx = c / g.ny, cy = c - (c / g.ny) * g.ny;
+  for (int dcx = -1; dcx <= 1; ++dcx) {
+    int ncx = cx + dcx;
+    if (g.px) ncx = ncx < 0 ? ncx + g.nx : (ncx >= g.nx ? ncx - g.nx : ncx);
+    else if (ncx < 0 || ncx >= g.nx) continue;
+    for (int dcy = -1; dcy <= 1; ++dcy) {
+      int ncy = cy + dcy;
+      if (g.py) ncy = ncy < 0 ? ncy + g.ny : (ncy >= g.ny ? ncy - g.ny : ncy);
+      else if (ncy < 0 || ncy >= g.ny) continue;
+      const int64_t nc = g.cbase + (int64_t)ncx * g.ny + ncy;
+      const int j0 = st.cell_start[nc], j1 = st.cell_start[nc + 1];
+      for (int j = j0; j < j1; ++j) {
+        if (j == s) continue;
+        const uint8_t fj = st.flags[j];
+        if (!fl_alive(fj) || fl_species(fj) != C.substrate) continue;
+        if (!(sep_sq<F64>(st.pos_pre, st.cell_pre, s, j, g) < g.cutoff_sq)) continue;   // pair list
+        if (sep_sq<F64>(st.pos_post, st.cell_post, s, j, g) > C.contact_sq) continue;  // contact
+        const int idj = st.ids[j] - (int)g.poff;
+        const uint32_t lo = ide < idj ? ide : idj, hi = ide < idj ? idj : ide;
+        const double u = uniform1(p.seed, step, EDM_S_CAT + cidx, lo, hi);
+        double xs, ys;
+        abs_pos<F64>(st.pos_post, st.cell_post, j, g, xs, ys);
+        double peff = C.prob;
+        if (C.rule >= 0) peff = C.prob * rule_factor(p, C.rule, st, xs, ys);
+        if (u < peff) {
+          if (cas_u8(&st.flags[j], fj, fl_make(C.product, true))) {
+            atomic_add_i64(&st.counters[(int64_t)t.r * EDM_NCOUNTERS + EDM_C_CATALYTIC], 1);
+            grid_change(p, st.grid_delta, C.substrate, true, C.product, true, xs, ys);
+          }
+        }
+      }
+    }
+  }
+}
+
+// Recruitment candidates of exchange e (dynamics.py:1229-1458): dormant
+// particles of the species whose keyed draw accepts at the keyed position.
+template <bool F64>
+__global__ void __launch_bounds__(kBlock) k_recruit_candidates(const EdmDynParams* __restrict__ P,
+                                                               const int2* __restrict__ blk, DevState st, int e) {
+  const Tile t = tile_of(blk);
+  const EdmDynParams& p = P[t.r];
+  const int64_t s = t.s;
+  if (s >= p.particle_offset + p.n_particles) return;
+  const EdmExch& X = p.exch[e];
+  const uint8_t f = st.flags[s];
+  if (fl_alive(f) || fl_species(f) != X.species) return;
+  const int id = st.ids[s] - (int)p.particle_offset;
+  const int64_t step = *st.d_step;
+  const double ua = uniform1(p.seed, step, EDM_S_EX_ACCEPT + 4 * e, (uint64_t)id, 0);
+  const U2 up = uniform2(p.seed, step, EDM_S_EX_POS + 4 * e, (uint64_t)id, 0);
+  const double cx = up.u0 * p.Lx, cy = up.u1 * p.Ly;
+  double peff = X.prob_on;
+  if (X.rule_on >= 0 && X.rule_on2 >= 0) {
+    peff = X.prob_on * rule_factor(p, X.rule_on, st, cx, cy) * rule_factor(p, X.rule_on2, st, cx, cy);
+  } else if (X.rule_on >= 0) {
+    peff = X.prob_on * rule_factor(p, X.rule_on, st, cx, cy);
+  }
+  if (ua < peff) {
+    const int k = atomicAdd(&st.rec_count[t.r], 1);
+    if (k < kRecCap) {
+      st.rec_id[(int64_t)t.r * kRecCap + k] = id;
+      st.rec_xy[((int64_t)t.r * kRecCap + k) * 2] = cx;
+      st.rec_xy[((int64_t)t.r * kRecCap + k) * 2 + 1] = cy;
+    } else {
+      set_status(st.status, EDM_STATUS_RECRUIT_CAP);
+    }
+  }
+}
+
+// Apply the first max_recruits accepted candidates in particle order.
+template <bool F64>
+__global__ void k_recruit_apply(const EdmDynParams* __restrict__ P, int n_rep, DevState st, int e) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n_rep) return;
+  const EdmDynParams& p = P[r];
+  const EdmExch& X = p.exch[e];
+  int n = st.rec_count[r];
+  if (n > kRecCap) n = kRecCap;
+  st.rec_count[r] = 0;
+  if (n == 0) return;
+  int32_t* ids = st.rec_id + (int64_t)r * kRecCap;
+  double* xy = st.rec_xy + (int64_t)r * kRecCap * 2;
+  for (int a = 1; a < n; ++a) {  // insertion sort by particle index
+    const int id = ids[a];
+    const double x = xy[2 * a], y = xy[2 * a + 1];
+    int b = a - 1;
+    while (b >= 0 && ids[b] > id) {
+      ids[b + 1] = ids[b];
+      xy[2 * (b + 1)] = xy[2 * b];
+      xy[2 * (b + 1) + 1] = xy[2 * b + 1];
+      --b;
+    }
+    ids[b + 1] = id;
+    xy[2 * (b + 1)] = x;
+    xy[2 * (b + 1) + 1] = y;
+  }
+  const Geo g(p);
+  const int take = n < X.max_recruits ? n : X.max_recruits;
+  for (int a = 0; a < take; ++a) {
+    const int64_t slot = st.slot_of_id[g.poff + ids[a]];
+    const double x = xy[2 * a], y = xy[2 * a + 1];
+    const int oldc = st.cell_post[slot];
+    const int cxn = cell_index(x, g.sx, g.nx), cyn = cell_index(y, g.sy, g.ny);
+    const int newc = cxn * g.ny + cyn;
+    if constexpr (F64) {
+      ((double2*)st.pos_post)[slot] = make_double2(x, y);
+    } else {
+      ((float2*)st.pos_post)[slot] = make_float2((float)(x - (double)cxn * g.sx), (float)(y - (double)cyn * g.sy));
+    }
+    st.cell_post[slot] = newc;
+    atomicAdd(&st.cnt_next[g.cbase + oldc], -1);
+    atomicAdd(&st.cnt_next[g.cbase + newc], 1);
+    st.flags[slot] = fl_make(X.species, true);
+    grid_add(p, st.grid_delta, X.species, x, y, 1);
+  }
+  atomic_add_i64(&st.counters[(int64_t)r * EDM_NCOUNTERS + EDM_C_RECRUITED], take);
+}
+
+// Detachment of exchange e (dynamics.py:1461-1555).
+template <bool F64>
+__global__ void __launch_bounds__(kBlock) k_detach(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk,
+                                                   DevState st, int e) {
+  const Tile t = tile_of(blk);
+  const EdmDynParams& p = P[t.r];
+  const int64_t s = t.s;
+  if (s >= p.particle_offset + p.n_particles) return;
+  const EdmExch& X = p.exch[e];
+  const uint8_t f = st.flags[s];
+  if (!fl_alive(f) || fl_species(f) != X.species) return;
+  const Geo g(p);
+  const int id = st.ids[s] - (int)g.poff;
+  const int64_t step = *st.d_step;
+  double x, y;
+  abs_pos<F64>(st.pos_post, st.cell_post, s, g, x, y);
+  double peff = X.prob_off;
+  if (X.rule_off >= 0) peff = X.prob_off * rule_factor(p, X.rule_off, st, x, y);
+  const double u = uniform1(p.seed, step, EDM_S_EX_DETACH + 4 * e, (uint64_t)id, 0);
+  if (u < peff) {
+    st.flags[s] = fl_make(X.species, false);
+    atomic_add_i64(&st.counters[(int64_t)t.r * EDM_NCOUNTERS + EDM_C_DETACHED], 1);
+    grid_add(p, st.grid_delta, X.species, x, y, -1);
+  }
+}
+
+// Unimolecular conversion v (dynamics.py:1565-1657).
+template <bool F64>
+__global__ void __launch_bounds__(kBlock) k_convert(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk,
+                                                    DevState st, int v) {
+  const Tile t = tile_of(blk);
+  const EdmDynParams& p = P[t.r];
+  const int64_t s = t.s;
+  if (s >= p.particle_offset + p.n_particles) return;
+  const EdmConv& V = p.conv[v];
+  const uint8_t f = st.flags[s];
+  if (!fl_alive(f) || fl_species(f) != V.from) return;
+  const Geo g(p);
+  const int id = st.ids[s] - (int)g.poff;
+  const int64_t step = *st.d_step;
+  double x, y;
+  abs_pos<F64>(st.pos_post, st.cell_post, s, g, x, y);
+  double peff = V.prob;
+  if (V.rule >= 0) peff = V.prob * rule_factor(p, V.rule, st, x, y);
+  const double u = uniform1(p.seed, step, EDM_S_CONV + v, (uint64_t)id, 0);
+  if (u < peff) {
+    st.flags[s] = fl_make(V.to, true);
+    atomic_add_i64(&st.counters[(int64_t)t.r * EDM_NCOUNTERS + EDM_C_CONVERTED], 1);
+    grid_change(p, st.grid_delta, V.from, true, V.to, true, x, y);
+  }
+}
+
+// Binding candidates of reaction b (dynamics.py:528-606): pairs (i < j)
+// passing every test of the pass-start state, keyed by the reference's pair
+// order (i, neighbour-cell ordinal, descending j).
+template <bool F64>
+__global__ void __launch_bounds__(kBlock) k_bind_candidates(const EdmDynParams* __restrict__ P,
+                                                            const int2* __restrict__ blk, DevState st, int b) {
+  const Tile t = tile_of(blk);
+  const EdmDynParams& p = P[t.r];
+  const int64_t s = t.s;
+  if (s >= p.particle_offset + p.n_particles) return;
+  const EdmBind& B = p.bind[b];
+  const uint8_t f = st.flags[s];
+  if (!fl_alive(f)) return;
+  const int spi = fl_species(f);
+  if (spi != B.ra && spi != B.rb) return;
+  const Geo g(p);
+  const int id = st.ids[s] - (int)g.poff;
+  if (st.bond[g.poff + id] >= 0) return;
+  const int64_t step = *st.d_step;
+  const int c = st.cell_pre[s];
+  const int cx = c / g.ny, cy = c - (c / g.ny) * g.ny;
+  for (int dcx = -1; dcx <= 1; ++dcx) {
+    int ncx = cx + dcx;
+    if (g.px) ncx = ncx < 0 ? ncx + g.nx : (ncx >= g.nx ? ncx - g.nx : ncx);
+    else if (ncx < 0 || ncx >= g.nx) continue;
+    for (int dcy = -1; dcy <= 1; ++dcy) {
+      int ncy = cy + dcy;
+      if (g.py) ncy = ncy < 0 ? ncy + g.ny : (ncy >= g.ny ? ncy - g.ny : ncy);
+      else if (ncy < 0 || ncy >= g.ny) continue;
+      const int64_t nc = g.cbase + (int64_t)ncx * g.ny + ncy;
+      const int ordinal = (dcx + 1) * 3 + (dcy + 1);
+      const int j0 = st.cell_start[nc], j1 = st.cell_start[nc + 1];
+      for (int j = j0; j < j1; ++j) {
+        const int idj = st.ids[j] - (int)g.poff;
+        if (idj <= id) continue;
+        const uint8_t fj = st.flags[j];
+        if (!fl_alive(fj)) continue;
+        if (st.bond[g.poff + idj] >= 0) continue;
+        const int spj = fl_species(fj);
+        int a, bb;
+        if (spi == B.ra && spj == B.rb) { a = id; bb = idj; }
+        else if (spi == B.rb && spj == B.ra) { a = idj; bb = id; }
+        else continue;
+        if (!(sep_sq<F64>(st.pos_pre, st.cell_pre, s, j, g) < g.cutoff_sq)) continue;
+        if (sep_sq<F64>(st.pos_post, st.cell_post, s, j, g) > B.contact_sq) continue;
+        const double u = uniform1(p.seed, step, EDM_S_BIND + 2 * b, (uint64_t)id, (uint64_t)idj);
+        if (!(u < B.prob_bind)) continue;
+        const int k = atomicAdd(&st.bind_count[t.r], 1);
+        if (k < kBindCap) {
+          st.bind_key[(int64_t)t.r * kBindCap + k] =
+              ((int64_t)id << 36) | ((int64_t)ordinal << 32) | (int64_t)(0xFFFFFFFFu - (uint32_t)idj);
+          st.bind_ab[((int64_t)t.r * kBindCap + k) * 2] = a;
+          st.bind_ab[((int64_t)t.r * kBindCap + k) * 2 + 1] = bb;
+        } else {
+          set_status(st.status, EDM_STATUS_BIND_CAP);
+        }
+      }
+    }
+  }
+}
+
+// Sequential greedy application in pair order, re-checking the live state.
+template <bool F64>
+__global__ void k_bind_apply(const EdmDynParams* __restrict__ P, int n_rep, DevState st, int b) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n_rep) return;
+  const EdmDynParams& p = P[r];
+  const EdmBind& B = p.bind[b];
+  int n = st.bind_count[r];
+  if (n > kBindCap) n = kBindCap;
+  st.bind_count[r] = 0;
+  if (n == 0) return;
+  int64_t* key = st.bind_key + (int64_t)r * kBindCap;
+  int32_t* ab = st.bind_ab + (int64_t)r * kBindCap * 2;
+  for (int i = 1; i < n; ++i) {
+    const int64_t k = key[i];
+    const int a = ab[2 * i], bb = ab[2 * i + 1];
+    int j = i - 1;
+    while (j >= 0 && key[j] > k) {
+      key[j + 1] = key[j];
+      ab[2 * (j + 1)] = ab[2 * j];
+      ab[2 * (j + 1) + 1] = ab[2 * j + 1];
+      --j;
+    }
+    key[j + 1] = k;
+    ab[2 * (j + 1)] = a;
+    ab[2 * (j + 1) + 1] = bb;
+  }
+  const Geo g(p);
+  int64_t nb = 0;
+  for (int i = 0; i < n; ++i) {
+    const int a = ab[2 * i], bb = ab[2 * i + 1];
+    const int64_t sa = st.slot_of_id[g.poff + a], sb = st.slot_of_id[g.poff + bb];
+    const uint8_t fa = st.flags[sa], fb = st.flags[sb];
+    if (!fl_alive(fa) || !fl_alive(fb)) continue;
+    if (st.bond[g.poff + a] >= 0 || st.bond[g.poff + bb] >= 0) continue;
+    if (fl_species(fa) != B.ra || fl_species(fb) != B.rb) continue;
+    double xa, ya, xb, yb;
+    abs_pos<F64>(st.pos_post, st.cell_post, sa, g, xa, ya);
+    abs_pos<F64>(st.pos_post, st.cell_post, sb, g, xb, yb);
+    st.flags[sa] = fl_make(B.product, true);
+    st.flags[sb] = fl_make(B.rb, false);
+    st.bond[g.poff + a] = (int32_t)(g.poff + bb);
+    st.bond[g.poff + bb] = (int32_t)(g.poff + a);
+    grid_change(p, st.grid_delta, B.ra, true, B.product, true, xa, ya);
+    grid_change(p, st.grid_delta, B.rb, true, B.rb, false, xb, yb);
+    ++nb;
+  }
+  atomic_add_i64(&st.counters[(int64_t)r * EDM_NCOUNTERS + EDM_C_BINDINGS], nb);
+}
+
+// Dissociation of reaction b (dynamics.py:609-654).
+template <bool F64>
+__global__ void __launch_bounds__(kBlock) k_dissociate(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk,
+                                                       DevState st, int b) {
+  const Tile t = tile_of(blk);
+  const EdmDynParams& p = P[t.r];
+  const int64_t s = t.s;
+  if (s >= p.particle_offset + p.n_particles) return;
+  const EdmBind& B = p.bind[b];
+  const uint8_t f = st.flags[s];
+  if (!fl_alive(f) || fl_species(f) != B.product) return;
+  const Geo g(p);
+  const int id = st.ids[s] - (int)g.poff;
+  const int partner = st.bond[g.poff + id];
+  if (partner < 0) return;
+  const int64_t step = *st.d_step;
+  const double u = uniform1(p.seed, step, EDM_S_DISSOC + 2 * b, (uint64_t)id, 0);
+  if (!(u < B.prob_dissoc)) return;
+  const int64_t sj = st.slot_of_id[partner];
+  double x, y, xj, yj;
+  abs_pos<F64>(st.pos_post, st.cell_post, s, g, x, y);
+  abs_pos<F64>(st.pos_post, st.cell_post, sj, g, xj, yj);
+  const uint8_t fj = st.flags[sj];
+  st.flags[s] = fl_make(B.ra, true);
+  st.flags[sj] = fl_make(B.rb, true);
+  const int oldc = st.cell_post[sj], newc = st.cell_post[s];
+  if constexpr (F64) {
+    ((double2*)st.pos_post)[sj] = ((const double2*)st.pos_post)[s];
+  } else {
+    ((float2*)st.pos_post)[sj] = ((const float2*)st.pos_post)[s];
+  }
+  st.cell_post[sj] = newc;
+  atomicAdd(&st.cnt_next[g.cbase + oldc], -1);
+  atomicAdd(&st.cnt_next[g.cbase + newc], 1);
+  st.bond[g.poff + id] = -1;
+  st.bond[partner] = -1;
+  grid_change(p, st.grid_delta, B.product, true, B.ra, true, x, y);
+  grid_change(p, st.grid_delta, fl_species(fj), fl_alive(fj), B.rb, true, x, y);
+  atomic_add_i64(&st.counters[(int64_t)t.r * EDM_NCOUNTERS + EDM_C_DISSOC], 1);
+}
+
+// grid_cnt += grid_delta; grid_delta = 0
+__global__ void k_grid_merge(int32_t* __restrict__ cnt, int32_t* __restrict__ delta, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int d = delta[i];
+    if (d) {
+      cnt[i] += d;
+      delta[i] = 0;
+    }
+  }
+}
+
+__global__ void k_step_inc(int64_t* step) { *step += 1; }
+
+}  // namespace edm

@@ -1,0 +1,887 @@
+// edm_engine.cu — the engine behind the C ABI of include/edm_b200.h.
+//
+// One engine holds R replicas (R = 1 for the drop-in single-system API) in
+// replica-offset CSR layout: particles, cells, density-grid cells, emitters,
+// photon buffers and FLIM stacks of replica r are contiguous slices located
+// by the offsets of its parameter blocks.  Every kernel launch covers all
+// replicas; per-step work is enqueued on the caller's stream and can be
+// captured into CUDA graphs (the BD step index lives in device memory, so a
+// captured chunk replays with advancing keys).
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "edm_phot.cuh"
+
+using namespace edm;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                  \
+  do {                                                                                  \
+    cudaError_t _e = (expr);                                                            \
+    if (_e != cudaSuccess) return fail(EDM_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+enum PassKind { P_BIND_CAND, P_BIND_APPLY, P_DISSOC, P_CAT, P_REC_CAND, P_REC_APPLY, P_DETACH, P_CONV, P_MERGE };
+struct Pass {
+  PassKind kind;
+  int index;
+};
+
+template <typename T>
+int dalloc(T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  if (e != cudaSuccess) return fail(EDM_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  e = cudaMemset(*p, 0, n * sizeof(T));
+  if (e != cudaSuccess) return fail(EDM_ECUDA, cudaGetErrorString(e));
+  return EDM_OK;
+}
+
+// Tiles of kBlock items per replica: (replica, first index).
+std::vector<int2> tiles(const std::vector<int64_t>& first, const std::vector<int64_t>& count) {
+  std::vector<int2> out;
+  for (size_t r = 0; r < first.size(); ++r)
+    for (int64_t i = 0; i < count[r]; i += kBlock) out.push_back(make_int2((int)r, (int)(first[r] + i)));
+  return out;
+}
+
+}  // namespace
+
+struct EdmEngine {
+  int device = 0, precision = 64, R = 0;
+  bool f64 = true, has_phot = false, has_scope = false;
+  int64_t N = 0, n_cells = 0, n_grid = 0, n_hill = 0, n_emit = 0, n_phcap = 0, n_flim = 0;
+  std::vector<EdmDynParams> hdp;
+  std::vector<EdmPhotParams> hpp;
+  std::vector<EdmScopeParams> hsp;
+  EdmDynParams* dp = nullptr;
+  EdmPhotParams* pp = nullptr;
+  EdmScopeParams* sp = nullptr;
+  double* hill = nullptr;
+  int2 *pblk = nullptr, *eblk = nullptr, *phblk = nullptr, *pxblk = nullptr;
+  int npblk = 0, neblk = 0, nphblk = 0, npxblk = 0;
+  void* pos_pre = nullptr;
+  void* pos_post = nullptr;
+  int32_t *cell_pre = nullptr, *cell_post = nullptr;
+  uint8_t* flags[2] = {nullptr, nullptr};
+  int32_t* ids[2] = {nullptr, nullptr};
+  int cur = 0;
+  int32_t *slot_of_id = nullptr, *bond = nullptr;
+  uint8_t *has_dye = nullptr, *bleached = nullptr;
+  int8_t *dye = nullptr, *ctmc = nullptr;
+  int32_t *cell_start = nullptr, *cursor = nullptr, *cnt = nullptr, *bsum = nullptr;
+  int nb_scan = 0;
+  int32_t *grid_cnt = nullptr, *grid_delta = nullptr;
+  int64_t* counters = nullptr;
+  uint32_t* status = nullptr;
+  int64_t *d_step = nullptr, *d_pstep = nullptr, *d_batch_key = nullptr;
+  int32_t *rec_count = nullptr, *rec_id = nullptr, *bind_count = nullptr, *bind_ab = nullptr;
+  double* rec_xy = nullptr;
+  int64_t* bind_key = nullptr;
+  int32_t *emit_id = nullptr, *emit_n = nullptr, *emit_nd = nullptr, *emit_acc = nullptr;
+  int8_t* emit_cls = nullptr;
+  int64_t* emit_off = nullptr;
+  int32_t* ph_pid = nullptr;
+  double* ph_t = nullptr;
+  int8_t* ph_ch = nullptr;
+  uint8_t* ph_fret = nullptr;
+  int64_t* ph_count = nullptr;
+  uint32_t* flim = nullptr;
+  // host staging for get_state
+  double* st_pos = nullptr;
+  int32_t *st_sp = nullptr, *st_bond = nullptr;
+  uint8_t *st_alive = nullptr, *st_bl = nullptr;
+  int8_t* st_ctmc = nullptr;
+  std::vector<Pass> passes;
+  std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;
+  std::vector<void*> allocs;
+
+  DevState dev_state() const {
+    DevState s;
+    s.pos_pre = pos_pre;
+    s.pos_post = pos_post;
+    s.cell_pre = cell_pre;
+    s.cell_post = cell_post;
+    s.flags_old = flags[cur ^ 1];
+    s.flags = flags[cur];
+    s.ids_old = ids[cur ^ 1];
+    s.ids = ids[cur];
+    s.slot_of_id = slot_of_id;
+    s.bond = bond;
+    s.cell_start = cell_start;
+    s.cell_cursor = cursor;
+    s.cnt_next = cnt;
+    s.grid_cnt = grid_cnt;
+    s.grid_delta = grid_delta;
+    s.hill = hill;
+    s.counters = counters;
+    s.status = status;
+    s.d_step = d_step;
+    s.rec_count = rec_count;
+    s.rec_id = rec_id;
+    s.rec_xy = rec_xy;
+    s.bind_count = bind_count;
+    s.bind_key = bind_key;
+    s.bind_ab = bind_ab;
+    return s;
+  }
+
+  PhotState phot_state() const {
+    PhotState p;
+    p.emit_id = emit_id;
+    p.emit_n = emit_n;
+    p.emit_nd = emit_nd;
+    p.emit_acc = emit_acc;
+    p.emit_cls = emit_cls;
+    p.emit_off = emit_off;
+    p.has_dye = has_dye;
+    p.dye = dye;
+    p.ctmc = ctmc;
+    p.bleached = bleached;
+    p.ph_pid = ph_pid;
+    p.ph_t = ph_t;
+    p.ph_ch = ph_ch;
+    p.ph_fret = ph_fret;
+    p.ph_count = ph_count;
+    p.flim = flim;
+    p.d_pstep = d_pstep;
+    p.d_batch_key = d_batch_key;
+    return p;
+  }
+
+  template <typename T>
+  int alloc(T** p, size_t n) {
+    int rc = dalloc(p, n);
+    if (rc == EDM_OK) allocs.push_back((void*)*p);
+    return rc;
+  }
+
+  void build_schedule() {
+    const EdmDynParams& p = hdp[0];
+    std::vector<bool> dirty(EDM_MAX_GRIDS, false);
+    auto sensors_of = [&](std::vector<int> species) {
+      std::vector<int> gs;
+      for (int g = 0; g < p.n_grids; ++g)
+        for (int s : species)
+          if (p.grid[g].sensor == s) gs.push_back(g);
+      return gs;
+    };
+    auto reads = [&](std::vector<int> rules) {
+      bool need = false;
+      for (int r : rules)
+        if (r >= 0 && dirty[p.rule[r].grid]) need = true;
+      if (need) {
+        passes.push_back({P_MERGE, 0});
+        std::fill(dirty.begin(), dirty.end(), false);
+      }
+    };
+    auto writes = [&](std::vector<int> species) {
+      for (int g : sensors_of(species)) dirty[g] = true;
+    };
+    for (int b = 0; b < p.n_bind; ++b) {
+      passes.push_back({P_BIND_CAND, b});
+      passes.push_back({P_BIND_APPLY, b});
+      writes({p.bind[b].ra, p.bind[b].rb, p.bind[b].product});
+      passes.push_back({P_DISSOC, b});
+    }
+    for (int c = 0; c < p.n_cat; ++c) {
+      reads({p.cat[c].rule});
+      passes.push_back({P_CAT, c});
+      writes({p.cat[c].substrate, p.cat[c].product});
+    }
+    for (int e = 0; e < p.n_exch; ++e) {
+      reads({p.exch[e].rule_on, p.exch[e].rule_on2});
+      passes.push_back({P_REC_CAND, e});
+      passes.push_back({P_REC_APPLY, e});
+      writes({p.exch[e].species});
+      reads({p.exch[e].rule_off});
+      passes.push_back({P_DETACH, e});
+      writes({p.exch[e].species});
+    }
+    for (int v = 0; v < p.n_conv; ++v) {
+      reads({p.conv[v].rule});
+      passes.push_back({P_CONV, v});
+      writes({p.conv[v].from, p.conv[v].to});
+    }
+  }
+
+  template <bool F64>
+  void enqueue_dynamics_t(cudaStream_t s) {
+    const int nbs = nb_scan;
+    k_scan_reduce<<<nbs, kScanThreads, 0, s>>>(cnt, n_cells, bsum);
+    k_scan_bsum<<<1, 1024, 0, s>>>(bsum, nbs);
+    k_scan_down<<<nbs, kScanThreads, 0, s>>>(cnt, n_cells, bsum, cell_start, cursor);
+    cur ^= 1;
+    DevState st = dev_state();
+    k_scatter<F64><<<npblk, kBlock, 0, s>>>(dp, pblk, st);
+    if (n_grid > 0) {
+      cudaMemsetAsync(grid_cnt, 0, sizeof(int32_t) * n_grid, s);
+      cudaMemsetAsync(grid_delta, 0, sizeof(int32_t) * n_grid, s);
+    }
+    k_move<F64><<<npblk, kBlock, 0, s>>>(dp, pblk, st);
+    const int rb = (R + 127) / 128;
+    const int gm = (int)std::min<int64_t>((n_grid + 255) / 256, 4096);
+    for (const Pass& ps : passes) {
+      switch (ps.kind) {
+        case P_BIND_CAND: k_bind_candidates<F64><<<npblk, kBlock, 0, s>>>(dp, pblk, st, ps.index); break;
+        case P_BIND_APPLY: k_bind_apply<F64><<<rb, 128, 0, s>>>(dp, R, st, ps.index); break;
+        case P_DISSOC: k_dissociate<F64><<<npblk, kBlock, 0, s>>>(dp, pblk, st, ps.index); break;
+        case P_CAT: k_catalytic<F64><<<npblk, kBlock, 0, s>>>(dp, pblk, st, ps.index); break;
+        case P_REC_CAND: k_recruit_candidates<F64><<<npblk, kBlock, 0, s>>>(dp, pblk, st, ps.index); break;
+        case P_REC_APPLY: k_recruit_apply<F64><<<rb, 128, 0, s>>>(dp, R, st, ps.index); break;
+        case P_DETACH: k_detach<F64><<<npblk, kBlock, 0, s>>>(dp, pblk, st, ps.index); break;
+        case P_CONV: k_convert<F64><<<npblk, kBlock, 0, s>>>(dp, pblk, st, ps.index); break;
+        case P_MERGE: k_grid_merge<<<gm > 0 ? gm : 1, 256, 0, s>>>(grid_cnt, grid_delta, n_grid); break;
+      }
+    }
+    k_step_inc<<<1, 1, 0, s>>>(d_step);
+  }
+
+  void enqueue_dynamics(cudaStream_t s) {
+    if (f64) enqueue_dynamics_t<true>(s);
+    else enqueue_dynamics_t<false>(s);
+  }
+
+  template <bool F64>
+  void enqueue_photons_t(cudaStream_t s) {
+    DevState st = dev_state();
+    PhotState ph = phot_state();
+    if (neblk > 0) k_phot_count<F64><<<neblk, kBlock, 0, s>>>(dp, pp, eblk, st, ph);
+    k_phot_scan<<<R, 256, 0, s>>>(pp, ph, counters, status);
+    if (neblk > 0) k_phot_write<<<neblk, kBlock, 0, s>>>(dp, pp, eblk, ph, counters);
+    k_phot_advance<<<1, 1, 0, s>>>(d_pstep, d_batch_key);
+  }
+
+  void enqueue_photons(cudaStream_t s) {
+    if (f64) enqueue_photons_t<true>(s);
+    else enqueue_photons_t<false>(s);
+  }
+
+  template <bool F64>
+  void enqueue_scope_t(cudaStream_t s) {
+    DevState st = dev_state();
+    PhotState ph = phot_state();
+    if (nphblk > 0) k_scope<F64><<<nphblk, kBlock, 0, s>>>(dp, pp, sp, phblk, st, ph);
+    k_scope_received<<<(R + 127) / 128, 128, 0, s>>>(pp, R, ph, counters);
+  }
+
+  void enqueue_scope(cudaStream_t s) {
+    if (f64) enqueue_scope_t<true>(s);
+    else enqueue_scope_t<false>(s);
+  }
+
+  ~EdmEngine() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    for (void* p : allocs) cudaFree(p);
+  }
+};
+
+// ============================================================================
+// C ABI
+// ============================================================================
+extern "C" {
+
+int edm_abi_version(void) { return EDM_ABI_VERSION; }
+
+int64_t edm_abi_sizeof(int which) {
+  switch (which) {
+    case 0: return (int64_t)sizeof(EdmDynParams);
+    case 1: return (int64_t)sizeof(EdmPhotParams);
+    case 2: return (int64_t)sizeof(EdmScopeParams);
+    case 3: return (int64_t)sizeof(EdmHostState);
+    default: return -1;
+  }
+}
+
+const char* edm_last_error(void) { return g_last_error.c_str(); }
+
+int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScopeParams* scope, int32_t n_replicas,
+               const double* hill, int64_t n_hill, int32_t precision, int32_t device, EdmEngine** out) {
+  if (!dyn || !out || n_replicas <= 0) return fail(EDM_EINVAL, "edm_create: null argument or no replicas");
+  if (precision != 32 && precision != 64) return fail(EDM_EINVAL, "edm_create: precision must be 32 or 64");
+  *out = nullptr;
+  CUDA_TRY(cudaSetDevice(device));
+  EdmEngine* E = new EdmEngine();
+  E->device = device;
+  E->precision = precision;
+  E->f64 = precision == 64;
+  E->R = n_replicas;
+  E->hdp.assign(dyn, dyn + n_replicas);
+  E->has_phot = phot != nullptr;
+  E->has_scope = scope != nullptr && phot != nullptr;
+  if (E->has_phot) E->hpp.assign(phot, phot + n_replicas);
+  if (E->has_scope) E->hsp.assign(scope, scope + n_replicas);
+  // validate the CSR layout and that every replica has the same pass structure
+  int64_t np = 0, nc = 0, ng = 0, ne = 0, nph = 0, nfl = 0;
+  std::vector<int64_t> pfirst, pcount, efirst, ecount, phfirst, phcount, pxfirst, pxcount;
+  const EdmDynParams& p0 = E->hdp[0];
+  for (int r = 0; r < n_replicas; ++r) {
+    const EdmDynParams& p = E->hdp[r];
+    if (p.particle_offset != np || p.cell_offset != nc) {
+      delete E;
+      return fail(EDM_EINVAL, "edm_create: replica offsets must be contiguous and in order");
+    }
+    if (p.n_species > EDM_MAX_SPECIES || p.n_species > 127 || p.nx < 3 || p.ny < 3 || p.n_bind > EDM_MAX_BIND ||
+        p.n_cat > EDM_MAX_CAT || p.n_exch > EDM_MAX_EXCH || p.n_conv > EDM_MAX_CONV || p.n_grids > EDM_MAX_GRIDS ||
+        p.n_rules > EDM_MAX_RULES) {
+      delete E;
+      return fail(EDM_EINVAL, "edm_create: parameter block out of range");
+    }
+    if (p.n_bind != p0.n_bind || p.n_cat != p0.n_cat || p.n_exch != p0.n_exch || p.n_conv != p0.n_conv ||
+        p.n_grids != p0.n_grids) {
+      delete E;
+      return fail(EDM_EINVAL, "edm_create: replicas must share one reaction structure");
+    }
+    for (int g = 0; g < p.n_grids; ++g) {
+      if (p.grid[g].offset != ng) {
+        delete E;
+        return fail(EDM_EINVAL, "edm_create: density-grid offsets must be contiguous");
+      }
+      ng += (int64_t)p.grid[g].nx * p.grid[g].ny;
+    }
+    for (int k = 0; k < p.n_rules; ++k) {
+      if (p.rule[k].table_offset < 0 || p.rule[k].table_offset + p.rule[k].table_len > n_hill) {
+        delete E;
+        return fail(EDM_EINVAL, "edm_create: Hill table out of range");
+      }
+    }
+    pfirst.push_back(np);
+    pcount.push_back(p.n_particles);
+    np += p.n_particles;
+    nc += (int64_t)p.nx * p.ny;
+    if (E->has_phot) {
+      const EdmPhotParams& q = E->hpp[r];
+      if (q.photon_offset != nph) {
+        delete E;
+        return fail(EDM_EINVAL, "edm_create: photon buffer offsets must be contiguous");
+      }
+      phfirst.push_back(nph);
+      phcount.push_back(q.max_photons);
+      nph += q.max_photons;
+    }
+    if (E->has_scope) {
+      const EdmScopeParams& s = E->hsp[r];
+      if (s.flim_offset != nfl) {
+        delete E;
+        return fail(EDM_EINVAL, "edm_create: FLIM stack offsets must be contiguous");
+      }
+      const int64_t npx = (int64_t)s.n_channels * s.nx * s.ny;
+      pxfirst.push_back(0);
+      pxcount.push_back(npx);
+      nfl += npx * s.n_bins;
+    }
+  }
+  if (np >= (int64_t)1 << 31) {
+    delete E;
+    return fail(EDM_EINVAL, "edm_create: more than 2^31 particles");
+  }
+  E->N = np;
+  E->n_cells = nc;
+  E->n_grid = ng;
+  E->n_hill = n_hill;
+  E->n_phcap = nph;
+  E->n_flim = nfl;
+  int rc = EDM_OK;
+#define ALLOC(ptr, n)                        \
+  if ((rc = E->alloc(&(ptr), (n))) != EDM_OK) { \
+    delete E;                                \
+    return rc;                               \
+  }
+  ALLOC(E->dp, (size_t)n_replicas);
+  CUDA_TRY(cudaMemcpy(E->dp, dyn, sizeof(EdmDynParams) * n_replicas, cudaMemcpyHostToDevice));
+  ALLOC(E->hill, (size_t)n_hill);
+  if (n_hill > 0) CUDA_TRY(cudaMemcpy(E->hill, hill, sizeof(double) * n_hill, cudaMemcpyHostToDevice));
+  const size_t psz = E->f64 ? sizeof(double2) : sizeof(float2);
+  uint8_t *pp0 = nullptr, *pp1 = nullptr;
+  ALLOC(pp0, psz * np);
+  ALLOC(pp1, psz * np);
+  E->pos_pre = pp0;
+  E->pos_post = pp1;
+  ALLOC(E->cell_pre, np);
+  ALLOC(E->cell_post, np);
+  ALLOC(E->flags[0], np + 4);
+  ALLOC(E->flags[1], np + 4);
+  ALLOC(E->ids[0], np);
+  ALLOC(E->ids[1], np);
+  ALLOC(E->slot_of_id, np);
+  ALLOC(E->bond, np);
+  ALLOC(E->has_dye, np);
+  ALLOC(E->bleached, np);
+  ALLOC(E->dye, np);
+  ALLOC(E->ctmc, np);
+  ALLOC(E->cell_start, nc + 1);
+  ALLOC(E->cursor, nc);
+  ALLOC(E->cnt, nc);
+  E->nb_scan = (int)((nc + kScanTile - 1) / kScanTile);
+  if (E->nb_scan < 1) E->nb_scan = 1;
+  ALLOC(E->bsum, (size_t)E->nb_scan);
+  ALLOC(E->grid_cnt, ng);
+  ALLOC(E->grid_delta, ng);
+  ALLOC(E->counters, (size_t)n_replicas * EDM_NCOUNTERS);
+  ALLOC(E->status, 1);
+  ALLOC(E->d_step, 1);
+  ALLOC(E->d_pstep, 1);
+  ALLOC(E->d_batch_key, 1);
+  ALLOC(E->rec_count, n_replicas);
+  ALLOC(E->rec_id, (size_t)n_replicas * kRecCap);
+  ALLOC(E->rec_xy, (size_t)n_replicas * kRecCap * 2);
+  ALLOC(E->bind_count, n_replicas);
+  ALLOC(E->bind_key, (size_t)n_replicas * kBindCap);
+  ALLOC(E->bind_ab, (size_t)n_replicas * kBindCap * 2);
+  std::vector<int2> pt = tiles(pfirst, pcount);
+  E->npblk = (int)pt.size();
+  ALLOC(E->pblk, pt.size());
+  if (!pt.empty()) CUDA_TRY(cudaMemcpy(E->pblk, pt.data(), sizeof(int2) * pt.size(), cudaMemcpyHostToDevice));
+  if (E->has_phot) {
+    ALLOC(E->pp, (size_t)n_replicas);
+    ALLOC(E->emit_id, np);
+    ALLOC(E->emit_n, np);
+    ALLOC(E->emit_nd, np);
+    ALLOC(E->emit_acc, np);
+    ALLOC(E->emit_cls, np);
+    ALLOC(E->emit_off, np);
+    ALLOC(E->ph_pid, nph);
+    ALLOC(E->ph_t, nph);
+    ALLOC(E->ph_ch, nph);
+    ALLOC(E->ph_fret, nph);
+    ALLOC(E->ph_count, n_replicas);
+    std::vector<int2> ph = tiles(phfirst, phcount);
+    E->nphblk = (int)ph.size();
+    ALLOC(E->phblk, ph.size());
+    if (!ph.empty()) CUDA_TRY(cudaMemcpy(E->phblk, ph.data(), sizeof(int2) * ph.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(E->pp, E->hpp.data(), sizeof(EdmPhotParams) * n_replicas, cudaMemcpyHostToDevice));
+  }
+  if (E->has_scope) {
+    ALLOC(E->sp, (size_t)n_replicas);
+    CUDA_TRY(cudaMemcpy(E->sp, E->hsp.data(), sizeof(EdmScopeParams) * n_replicas, cudaMemcpyHostToDevice));
+    ALLOC(E->flim, (size_t)nfl);
+    std::vector<int2> px = tiles(pxfirst, pxcount);
+    E->npxblk = (int)px.size();
+    ALLOC(E->pxblk, px.size());
+    if (!px.empty()) CUDA_TRY(cudaMemcpy(E->pxblk, px.data(), sizeof(int2) * px.size(), cudaMemcpyHostToDevice));
+  }
+  ALLOC(E->st_sp, np);
+  ALLOC(E->st_bond, np);
+  ALLOC(E->st_alive, np);
+  ALLOC(E->st_bl, np);
+  ALLOC(E->st_ctmc, np);
+  ALLOC(E->st_pos, (size_t)np * 2);
+#undef ALLOC
+  E->build_schedule();
+  CUDA_TRY(cudaDeviceSynchronize());
+  *out = E;
+  return EDM_OK;
+}
+
+int edm_destroy(EdmEngine* eng) {
+  if (!eng) return EDM_OK;
+  cudaSetDevice(eng->device);
+  cudaDeviceSynchronize();
+  delete eng;
+  return EDM_OK;
+}
+
+}  // extern "C"
+
+// ---- state upload / download ------------------------------------------------
+namespace {
+
+template <bool F64>
+__global__ void k_set_state(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk, const double* pos,
+                            const int32_t* species, const uint8_t* alive, void* pos_post, int32_t* cell_post,
+                            uint8_t* flags, int32_t* ids, int32_t* slot_of_id, int32_t* cnt) {
+  const Tile t = tile_of(blk);
+  const EdmDynParams& p = P[t.r];
+  const int64_t s = t.s;
+  if (s >= p.particle_offset + p.n_particles) return;
+  const Geo g(p);
+  const double x = pos[2 * s], y = pos[2 * s + 1];
+  const int cx = cell_index(x, g.sx, g.nx), cy = cell_index(y, g.sy, g.ny);
+  if constexpr (F64) {
+    ((double2*)pos_post)[s] = make_double2(x, y);
+  } else {
+    ((float2*)pos_post)[s] = make_float2((float)(x - (double)cx * g.sx), (float)(y - (double)cy * g.sy));
+  }
+  const int c = cx * g.ny + cy;
+  cell_post[s] = c;
+  flags[s] = fl_make(species[s], alive[s] != 0);
+  ids[s] = (int32_t)s;
+  slot_of_id[s] = (int32_t)s;
+  atomicAdd(&cnt[g.cbase + c], 1);
+}
+
+template <bool F64>
+__global__ void k_get_state(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk, const void* pos_post,
+                            const int32_t* cell_post, const uint8_t* flags, const int32_t* slot_of_id,
+                            const int32_t* bond, double* pos, int32_t* species, uint8_t* alive, int32_t* bond_local) {
+  const Tile t = tile_of(blk);
+  const EdmDynParams& p = P[t.r];
+  const int64_t id = t.s;
+  if (id >= p.particle_offset + p.n_particles) return;
+  const Geo g(p);
+  const int64_t s = slot_of_id[id];
+  double x, y;
+  abs_pos<F64>(pos_post, cell_post, s, g, x, y);
+  pos[2 * id] = x;
+  pos[2 * id + 1] = y;
+  const uint8_t f = flags[s];
+  species[id] = fl_species(f);
+  alive[id] = fl_alive(f) ? 1 : 0;
+  const int b = bond[id];
+  bond_local[id] = b >= 0 ? (int32_t)(b - p.particle_offset) : -1;
+}
+
+__global__ void k_bond_to_global(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk, int32_t* bond) {
+  const Tile t = tile_of(blk);
+  const EdmDynParams& p = P[t.r];
+  const int64_t id = t.s;
+  if (id >= p.particle_offset + p.n_particles) return;
+  const int b = bond[id];
+  bond[id] = b >= 0 ? (int32_t)(b + p.particle_offset) : -1;
+}
+
+}  // namespace
+
+extern "C" {
+
+int edm_set_state(EdmEngine* E, const EdmHostState* st, void* stream) {
+  if (!E || !st || st->n != E->N) return fail(EDM_EINVAL, "edm_set_state: size mismatch");
+  cudaStream_t s = (cudaStream_t)stream;
+  CUDA_TRY(cudaSetDevice(E->device));
+  const int64_t N = E->N;
+  double* dpos = E->st_pos;
+  CUDA_TRY(cudaMemcpyAsync(dpos, st->positions, sizeof(double) * 2 * N, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(E->st_sp, st->species_id, sizeof(int32_t) * N, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(E->st_alive, st->is_alive, N, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(E->bond, st->bond_partner, sizeof(int32_t) * N, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(E->has_dye, st->has_dye, N, cudaMemcpyHostToDevice, s));
+  std::vector<int8_t> dye8(N);
+  for (int64_t i = 0; i < N; ++i) dye8[i] = (int8_t)st->dye_type_id[i];
+  CUDA_TRY(cudaMemcpyAsync(E->dye, dye8.data(), N, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(E->ctmc, st->ctmc_state, N, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(E->bleached, st->is_bleached, N, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemsetAsync(E->cnt, 0, sizeof(int32_t) * (E->n_cells > 0 ? E->n_cells : 1), s));
+  if (E->npblk > 0) {
+    if (E->f64)
+      k_set_state<true><<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, dpos, E->st_sp, E->st_alive, E->pos_post,
+                                                    E->cell_post, E->flags[E->cur], E->ids[E->cur], E->slot_of_id,
+                                                    E->cnt);
+    else
+      k_set_state<false><<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, dpos, E->st_sp, E->st_alive, E->pos_post,
+                                                     E->cell_post, E->flags[E->cur], E->ids[E->cur], E->slot_of_id,
+                                                     E->cnt);
+    k_bond_to_global<<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, E->bond);
+  }
+  // emitters: particles carrying a dye, in particle order per replica
+  if (E->has_phot) {
+    std::vector<int32_t> eid;
+    eid.reserve(N);
+    int64_t off = 0;
+    std::vector<int64_t> efirst, ecount;
+    for (int r = 0; r < E->R; ++r) {
+      const EdmDynParams& p = E->hdp[r];
+      const int64_t before = (int64_t)eid.size();
+      for (int64_t i = p.particle_offset; i < p.particle_offset + p.n_particles; ++i)
+        if (st->has_dye[i]) eid.push_back((int32_t)i);
+      E->hpp[r].emitter_offset = before;
+      E->hpp[r].n_emitters = (int64_t)eid.size() - before;
+      efirst.push_back(before);
+      ecount.push_back((int64_t)eid.size() - before);
+      off = (int64_t)eid.size();
+    }
+    (void)off;
+    E->n_emit = (int64_t)eid.size();
+    if (!eid.empty())
+      CUDA_TRY(cudaMemcpyAsync(E->emit_id, eid.data(), sizeof(int32_t) * eid.size(), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(E->pp, E->hpp.data(), sizeof(EdmPhotParams) * E->R, cudaMemcpyHostToDevice, s));
+    std::vector<int2> et = tiles(efirst, ecount);
+    if (E->eblk) cudaFree(E->eblk);
+    for (auto& a : E->allocs)
+      if (a == (void*)E->eblk) a = nullptr;
+    E->eblk = nullptr;
+    E->neblk = (int)et.size();
+    if (!et.empty()) {
+      CUDA_TRY(cudaMalloc(&E->eblk, sizeof(int2) * et.size()));
+      E->allocs.push_back(E->eblk);
+      CUDA_TRY(cudaMemcpyAsync(E->eblk, et.data(), sizeof(int2) * et.size(), cudaMemcpyHostToDevice, s));
+    }
+    CUDA_TRY(cudaStreamSynchronize(s));  // host vectors above go out of scope
+    for (auto& kv : E->graphs) cudaGraphExecDestroy(kv.second);
+    E->graphs.clear();
+  } else {
+    CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  CUDA_TRY(cudaGetLastError());
+  return EDM_OK;
+}
+
+int edm_get_state(EdmEngine* E, EdmHostState* st, void* stream) {
+  if (!E || !st || st->n != E->N) return fail(EDM_EINVAL, "edm_get_state: size mismatch");
+  cudaStream_t s = (cudaStream_t)stream;
+  CUDA_TRY(cudaSetDevice(E->device));
+  const int64_t N = E->N;
+  if (E->npblk > 0) {
+    if (E->f64)
+      k_get_state<true><<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, E->pos_post, E->cell_post, E->flags[E->cur],
+                                                    E->slot_of_id, E->bond, E->st_pos, E->st_sp, E->st_alive,
+                                                    E->st_bond);
+    else
+      k_get_state<false><<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, E->pos_post, E->cell_post, E->flags[E->cur],
+                                                     E->slot_of_id, E->bond, E->st_pos, E->st_sp, E->st_alive,
+                                                     E->st_bond);
+  }
+  CUDA_TRY(cudaGetLastError());
+  if (st->positions) CUDA_TRY(cudaMemcpyAsync(st->positions, E->st_pos, sizeof(double) * 2 * N, cudaMemcpyDeviceToHost, s));
+  if (st->species_id) CUDA_TRY(cudaMemcpyAsync(st->species_id, E->st_sp, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, s));
+  if (st->is_alive) CUDA_TRY(cudaMemcpyAsync(st->is_alive, E->st_alive, N, cudaMemcpyDeviceToHost, s));
+  if (st->bond_partner) CUDA_TRY(cudaMemcpyAsync(st->bond_partner, E->st_bond, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, s));
+  if (st->ctmc_state) CUDA_TRY(cudaMemcpyAsync(st->ctmc_state, E->ctmc, N, cudaMemcpyDeviceToHost, s));
+  if (st->is_bleached) CUDA_TRY(cudaMemcpyAsync(st->is_bleached, E->bleached, N, cudaMemcpyDeviceToHost, s));
+  if (st->has_dye) CUDA_TRY(cudaMemcpyAsync(st->has_dye, E->has_dye, N, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return EDM_OK;
+}
+
+int edm_set_step(EdmEngine* E, int64_t step_index) {
+  if (!E) return fail(EDM_EINVAL, "null engine");
+  CUDA_TRY(cudaSetDevice(E->device));
+  CUDA_TRY(cudaMemcpy(E->d_step, &step_index, sizeof(int64_t), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(E->d_pstep, &step_index, sizeof(int64_t), cudaMemcpyHostToDevice));
+  return EDM_OK;
+}
+
+int64_t edm_get_step(EdmEngine* E) {
+  if (!E) return -1;
+  int64_t v = -1;
+  cudaSetDevice(E->device);
+  if (cudaMemcpy(&v, E->d_step, sizeof(int64_t), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+  return v;
+}
+
+int edm_dynamics_step(EdmEngine* E, int32_t n_steps, void* stream) {
+  if (!E || n_steps < 0) return fail(EDM_EINVAL, "edm_dynamics_step: bad argument");
+  CUDA_TRY(cudaSetDevice(E->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  for (int i = 0; i < n_steps; ++i) E->enqueue_dynamics(s);
+  CUDA_TRY(cudaGetLastError());
+  return EDM_OK;
+}
+
+int edm_photon_step(EdmEngine* E, void* stream) {
+  if (!E || !E->has_phot) return fail(EDM_EINVAL, "edm_photon_step: engine has no photophysics");
+  CUDA_TRY(cudaSetDevice(E->device));
+  E->enqueue_photons((cudaStream_t)stream);
+  CUDA_TRY(cudaGetLastError());
+  return EDM_OK;
+}
+
+int edm_get_photon_counts(EdmEngine* E, int64_t* counts, void* stream) {
+  if (!E || !E->has_phot || !counts) return fail(EDM_EINVAL, "edm_get_photon_counts: bad argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  CUDA_TRY(cudaMemcpyAsync(counts, E->ph_count, sizeof(int64_t) * E->R, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return EDM_OK;
+}
+
+int edm_get_photons(EdmEngine* E, int32_t replica, int32_t* particle_idx, double* arrival_time, int8_t* channel,
+                    uint8_t* is_fret, int64_t capacity, void* stream) {
+  if (!E || !E->has_phot || replica < 0 || replica >= E->R) return fail(EDM_EINVAL, "edm_get_photons: bad argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  int64_t n = 0;
+  CUDA_TRY(cudaMemcpyAsync(&n, E->ph_count + replica, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  if (n > capacity) return fail(EDM_EINVAL, "edm_get_photons: capacity too small");
+  const int64_t o = E->hpp[replica].photon_offset;
+  if (n > 0) {
+    if (particle_idx) CUDA_TRY(cudaMemcpyAsync(particle_idx, E->ph_pid + o, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
+    if (arrival_time) CUDA_TRY(cudaMemcpyAsync(arrival_time, E->ph_t + o, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    if (channel) CUDA_TRY(cudaMemcpyAsync(channel, E->ph_ch + o, n, cudaMemcpyDeviceToHost, s));
+    if (is_fret) CUDA_TRY(cudaMemcpyAsync(is_fret, E->ph_fret + o, n, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  return (int)n;
+}
+
+int edm_scope_process(EdmEngine* E, void* stream) {
+  if (!E || !E->has_scope) return fail(EDM_EINVAL, "edm_scope_process: engine has no microscope");
+  CUDA_TRY(cudaSetDevice(E->device));
+  E->enqueue_scope((cudaStream_t)stream);
+  CUDA_TRY(cudaGetLastError());
+  return EDM_OK;
+}
+
+int edm_set_photons(EdmEngine* E, int32_t replica, const int32_t* particle_idx, const double* arrival_time,
+                    const int8_t* channel, const uint8_t* is_fret, int64_t n, int64_t batch_key, void* stream) {
+  if (!E || !E->has_phot || replica < 0 || replica >= E->R || n < 0) return fail(EDM_EINVAL, "edm_set_photons: bad argument");
+  if (n > E->hpp[replica].max_photons) return fail(EDM_EINVAL, "edm_set_photons: batch larger than the photon buffer");
+  CUDA_TRY(cudaSetDevice(E->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t o = E->hpp[replica].photon_offset;
+  if (n > 0) {
+    CUDA_TRY(cudaMemcpyAsync(E->ph_pid + o, particle_idx, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(E->ph_t + o, arrival_time, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(E->ph_ch + o, channel, n, cudaMemcpyHostToDevice, s));
+    if (is_fret) CUDA_TRY(cudaMemcpyAsync(E->ph_fret + o, is_fret, n, cudaMemcpyHostToDevice, s));
+  }
+  std::vector<int64_t> counts(E->R, 0);
+  counts[replica] = n;
+  CUDA_TRY(cudaMemcpyAsync(E->ph_count, counts.data(), sizeof(int64_t) * E->R, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(E->d_batch_key, &batch_key, sizeof(int64_t), cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return EDM_OK;
+}
+
+int edm_pipeline_steps(EdmEngine* E, int32_t n_steps, int32_t with_photons, int32_t graph_chunk, void* stream) {
+  if (!E || n_steps < 0) return fail(EDM_EINVAL, "edm_pipeline_steps: bad argument");
+  if (with_photons && !E->has_scope) return fail(EDM_EINVAL, "edm_pipeline_steps: no photophysics/microscope");
+  CUDA_TRY(cudaSetDevice(E->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  auto body = [&](cudaStream_t st) {
+    E->enqueue_dynamics(st);
+    if (with_photons) {
+      E->enqueue_photons(st);
+      E->enqueue_scope(st);
+    }
+  };
+  int done = 0;
+  if (graph_chunk > 0 && s != nullptr) {
+    while (n_steps - done >= graph_chunk) {
+      const auto key = std::make_tuple(graph_chunk, with_photons ? 1 : 0, E->cur);
+      auto it = E->graphs.find(key);
+      if (it == E->graphs.end()) {
+        const int cur0 = E->cur;
+        cudaGraph_t g;
+        CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        for (int i = 0; i < graph_chunk; ++i) body(s);
+        CUDA_TRY(cudaStreamEndCapture(s, &g));
+        cudaGraphExec_t ge;
+        CUDA_TRY(cudaGraphInstantiate(&ge, g, 0));
+        cudaGraphDestroy(g);
+        E->cur = cur0;  // capture advanced the parity; the launch below replays it
+        it = E->graphs.emplace(key, ge).first;
+      }
+      CUDA_TRY(cudaGraphLaunch(it->second, s));
+      if (graph_chunk & 1) E->cur ^= 1;
+      done += graph_chunk;
+    }
+  }
+  for (; done < n_steps; ++done) body(s);
+  CUDA_TRY(cudaGetLastError());
+  return EDM_OK;
+}
+
+int edm_scope_finalize(EdmEngine* E, int64_t frame_index, void* stream) {
+  if (!E || !E->has_scope) return fail(EDM_EINVAL, "edm_scope_finalize: engine has no microscope");
+  CUDA_TRY(cudaSetDevice(E->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  if (E->npxblk > 0) {
+    k_dark<<<E->npxblk, kBlock, 0, s>>>(E->dp, E->sp, E->pxblk, E->flim, frame_index, E->counters);
+    k_afterpulse<<<E->npxblk, kBlock, 0, s>>>(E->dp, E->sp, E->pxblk, E->flim, frame_index, E->counters);
+  }
+  CUDA_TRY(cudaGetLastError());
+  return EDM_OK;
+}
+
+int edm_get_flim(EdmEngine* E, int32_t replica, uint32_t* host_out, int64_t n_elems, void* stream) {
+  if (!E || !E->has_scope || replica < 0 || replica >= E->R) return fail(EDM_EINVAL, "edm_get_flim: bad argument");
+  const EdmScopeParams& p = E->hsp[replica];
+  const int64_t n = (int64_t)p.n_channels * p.nx * p.ny * p.n_bins;
+  if (n_elems < n) return fail(EDM_EINVAL, "edm_get_flim: buffer too small");
+  cudaStream_t s = (cudaStream_t)stream;
+  CUDA_TRY(cudaMemcpyAsync(host_out, E->flim + p.flim_offset, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return EDM_OK;
+}
+
+int edm_reset_flim(EdmEngine* E, void* stream) {
+  if (!E || !E->has_scope) return fail(EDM_EINVAL, "edm_reset_flim: engine has no microscope");
+  CUDA_TRY(cudaMemsetAsync(E->flim, 0, sizeof(uint32_t) * E->n_flim, (cudaStream_t)stream));
+  return EDM_OK;
+}
+
+int edm_get_counters(EdmEngine* E, int64_t* out, void* stream) {
+  if (!E || !out) return fail(EDM_EINVAL, "edm_get_counters: bad argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  CUDA_TRY(cudaMemcpyAsync(out, E->counters, sizeof(int64_t) * E->R * EDM_NCOUNTERS, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return EDM_OK;
+}
+
+int edm_get_status(EdmEngine* E, uint32_t* status, void* stream) {
+  if (!E || !status) return fail(EDM_EINVAL, "edm_get_status: bad argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  CUDA_TRY(cudaMemcpyAsync(status, E->status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return EDM_OK;
+}
+
+int edm_get_cells(EdmEngine* E, int32_t replica, int32_t* cell_start, int32_t* members, int64_t cap_cells,
+                  int64_t cap_members, void* stream) {
+  if (!E || replica < 0 || replica >= E->R) return fail(EDM_EINVAL, "edm_get_cells: bad argument");
+  const EdmDynParams& p = E->hdp[replica];
+  const int64_t nc = (int64_t)p.nx * p.ny;
+  if (cap_cells < nc + 1 || cap_members < p.n_particles) return fail(EDM_EINVAL, "edm_get_cells: buffers too small");
+  cudaStream_t s = (cudaStream_t)stream;
+  CUDA_TRY(cudaMemcpyAsync(cell_start, E->cell_start + p.cell_offset, sizeof(int32_t) * (nc + 1), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(members, E->ids[E->cur] + p.particle_offset, sizeof(int32_t) * p.n_particles,
+                           cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  for (int64_t c = 0; c <= nc; ++c) cell_start[c] -= (int32_t)p.particle_offset;
+  for (int64_t i = 0; i < p.n_particles; ++i) members[i] -= (int32_t)p.particle_offset;
+  return EDM_OK;
+}
+
+}  // extern "C"
+
+// ---- noise hooks ----------------------------------------------------------------
+namespace {
+__global__ void k_noise_normals(uint64_t seed, int64_t step, int stream, const int64_t* keys, int64_t n, double* out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const U2 z = normal2(seed, step, stream, (uint64_t)keys[i]);
+  out[2 * i] = z.u0;
+  out[2 * i + 1] = z.u1;
+}
+__global__ void k_noise_uniforms(uint64_t seed, int64_t step, int stream, const int64_t* a, const int64_t* b, int64_t n,
+                                 double* out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const U2 u = uniform2(seed, step, stream, (uint64_t)a[i], b ? (uint64_t)b[i] : 0u);
+  out[2 * i] = u.u0;
+  out[2 * i + 1] = u.u1;
+}
+}  // namespace
+
+extern "C" {
+int edm_noise_normal_pairs(uint64_t seed, int64_t step, int32_t stream_id, const int64_t* keys_dev, int64_t n,
+                           double* out_dev, void* stream) {
+  if (n < 0 || (n > 0 && (!keys_dev || !out_dev))) return fail(EDM_EINVAL, "edm_noise_normal_pairs: bad argument");
+  if (n == 0) return EDM_OK;
+  k_noise_normals<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(seed, step, stream_id, keys_dev, n,
+                                                                               out_dev);
+  CUDA_TRY(cudaGetLastError());
+  return EDM_OK;
+}
+int edm_noise_uniforms(uint64_t seed, int64_t step, int32_t stream_id, const int64_t* keys_a_dev,
+                       const int64_t* keys_b_dev, int64_t n, double* out2_dev, void* stream) {
+  if (n < 0 || (n > 0 && (!keys_a_dev || !out2_dev))) return fail(EDM_EINVAL, "edm_noise_uniforms: bad argument");
+  if (n == 0) return EDM_OK;
+  k_noise_uniforms<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(seed, step, stream_id, keys_a_dev,
+                                                                                keys_b_dev, n, out2_dev);
+  CUDA_TRY(cudaGetLastError());
+  return EDM_OK;
+}
+}  // extern "C"

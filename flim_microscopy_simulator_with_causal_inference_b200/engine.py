@@ -1,0 +1,335 @@
+"""ctypes binding of the C ABI (include/edm_b200.h) and the device system.
+
+`Engine` is a thin, typed wrapper over one `EdmEngine*`: R replicas of the
+per-timestep path on one GPU.  `DeviceSystem` binds an Engine to one host
+`ParticleState` and implements the reference API's in-place semantics: the
+host arrays are uploaded before a device call when they differ from what the
+device last saw, and downloaded after calls that must leave them current.
+
+There is no CPU fallback: if the CUDA library is missing or no GPU is
+visible, constructing an Engine raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import params as PR
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "_lib" / "libedm_b200.so"
+
+_lib = None
+
+
+def build_library(force: bool = False) -> Path:
+    """Compile the CUDA library in-tree with nvcc (sm_100a)."""
+    csrc = PKG / "csrc"
+    deps = list(csrc.glob("*.cu")) + list(csrc.glob("*.cuh")) + [PKG.parent / "include" / "edm_b200.h"]
+    if force or not LIB_PATH.exists() or any(d.stat().st_mtime > LIB_PATH.stat().st_mtime for d in deps):
+        subprocess.run(["make", "-C", str(csrc)], check=True)
+    return LIB_PATH
+
+
+def load_library():
+    """Load the CUDA engine library (fails loudly when it is absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"CUDA engine library not built: {LIB_PATH} (run __graft_entry__.build())")
+    L = C.CDLL(str(LIB_PATH))
+    vp, i32, i64, u64 = C.c_void_p, C.c_int32, C.c_int64, C.c_uint64
+    L.edm_abi_version.restype = C.c_int
+    L.edm_abi_sizeof.argtypes = [C.c_int]
+    L.edm_abi_sizeof.restype = i64
+    L.edm_last_error.restype = C.c_char_p
+    L.edm_create.argtypes = [vp, vp, vp, i32, vp, i64, i32, i32, C.POINTER(vp)]
+    L.edm_destroy.argtypes = [vp]
+    L.edm_set_state.argtypes = [vp, vp, vp]
+    L.edm_get_state.argtypes = [vp, vp, vp]
+    L.edm_set_step.argtypes = [vp, i64]
+    L.edm_get_step.argtypes = [vp]
+    L.edm_get_step.restype = i64
+    L.edm_dynamics_step.argtypes = [vp, i32, vp]
+    L.edm_photon_step.argtypes = [vp, vp]
+    L.edm_get_photon_counts.argtypes = [vp, vp, vp]
+    L.edm_get_photons.argtypes = [vp, i32, vp, vp, vp, vp, i64, vp]
+    L.edm_scope_process.argtypes = [vp, vp]
+    L.edm_set_photons.argtypes = [vp, i32, vp, vp, vp, vp, i64, i64, vp]
+    L.edm_pipeline_steps.argtypes = [vp, i32, i32, i32, vp]
+    L.edm_scope_finalize.argtypes = [vp, i64, vp]
+    L.edm_get_flim.argtypes = [vp, i32, vp, i64, vp]
+    L.edm_reset_flim.argtypes = [vp, vp]
+    L.edm_get_counters.argtypes = [vp, vp, vp]
+    L.edm_get_status.argtypes = [vp, vp, vp]
+    L.edm_get_cells.argtypes = [vp, i32, vp, vp, i64, i64, vp]
+    L.edm_noise_normal_pairs.argtypes = [u64, i64, i32, vp, i64, vp, vp]
+    L.edm_noise_uniforms.argtypes = [u64, i64, i32, vp, vp, i64, vp, vp]
+    for which, cls in ((0, PR.EdmDynParams), (1, PR.EdmPhotParams), (2, PR.EdmScopeParams), (3, PR.EdmHostState)):
+        if L.edm_abi_sizeof(which) != C.sizeof(cls):
+            raise ImportError(f"ABI mismatch for {cls.__name__}: C {L.edm_abi_sizeof(which)} vs ctypes {C.sizeof(cls)}")
+    _lib = L
+    return L
+
+
+def _check(rc: int, what: str) -> int:
+    if rc < 0:
+        msg = load_library().edm_last_error().decode(errors="replace")
+        raise RuntimeError(f"{what} failed ({rc}): {msg}")
+    return rc
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _stream_handle(stream) -> Optional[int]:
+    if stream is None:
+        return None
+    return int(getattr(stream, "cuda_stream", stream))
+
+
+class Engine:
+    """R replicas of the per-timestep path on one GPU (one EdmEngine*)."""
+
+    def __init__(self, dyn: Sequence[PR.EdmDynParams], hill: np.ndarray,
+                 phot: Optional[Sequence[PR.EdmPhotParams]] = None,
+                 scope: Optional[Sequence[PR.EdmScopeParams]] = None, precision: int = 64, device: int = 0):
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError("no CUDA device visible: the B200 engine has no CPU fallback")
+        self.L = load_library()
+        self.R = len(dyn)
+        self.precision = int(precision)
+        self._dyn = (PR.EdmDynParams * self.R)(*dyn)
+        self._phot = (PR.EdmPhotParams * self.R)(*phot) if phot is not None else None
+        self._scope = (PR.EdmScopeParams * self.R)(*scope) if scope is not None else None
+        self._hill = np.ascontiguousarray(hill, dtype=np.float64)
+        self.N = int(sum(p.n_particles for p in dyn))
+        self.handle = C.c_void_p()
+        _check(self.L.edm_create(C.byref(self._dyn), C.byref(self._phot) if self._phot is not None else None,
+                                 C.byref(self._scope) if self._scope is not None else None, self.R,
+                                 _ptr(self._hill), self._hill.size, self.precision, device,
+                                 C.byref(self.handle)), "edm_create")
+
+    def close(self):
+        if getattr(self, "handle", None) and self.handle.value:
+            self.L.edm_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- state ---------------------------------------------------------------
+    def set_state(self, positions, species, alive, bond, has_dye, dye_type, ctmc, bleached, stream=None):
+        arrs = dict(positions=np.ascontiguousarray(positions, dtype=np.float64),
+                    species=np.ascontiguousarray(species, dtype=np.int32),
+                    alive=np.ascontiguousarray(alive, dtype=np.uint8),
+                    bond=np.ascontiguousarray(bond, dtype=np.int32),
+                    has_dye=np.ascontiguousarray(has_dye, dtype=np.uint8),
+                    dye=np.ascontiguousarray(dye_type, dtype=np.int32),
+                    ctmc=np.ascontiguousarray(ctmc, dtype=np.int8),
+                    bleached=np.ascontiguousarray(bleached, dtype=np.uint8))
+        hs = PR.EdmHostState(self.N, _ptr(arrs["positions"]), _ptr(arrs["species"]), _ptr(arrs["alive"]),
+                             _ptr(arrs["bond"]), _ptr(arrs["has_dye"]), _ptr(arrs["dye"]), _ptr(arrs["ctmc"]),
+                             _ptr(arrs["bleached"]))
+        _check(self.L.edm_set_state(self.handle, C.byref(hs), _stream_handle(stream)), "edm_set_state")
+
+    def get_state(self, stream=None) -> dict:
+        N = self.N
+        out = dict(positions=np.empty((N, 2)), species=np.empty(N, np.int32), alive=np.empty(N, np.uint8),
+                   bond=np.empty(N, np.int32), ctmc=np.empty(N, np.int8), bleached=np.empty(N, np.uint8),
+                   has_dye=np.empty(N, np.uint8))
+        hs = PR.EdmHostState(N, _ptr(out["positions"]), _ptr(out["species"]), _ptr(out["alive"]), _ptr(out["bond"]),
+                             _ptr(out["has_dye"]), None, _ptr(out["ctmc"]), _ptr(out["bleached"]))
+        _check(self.L.edm_get_state(self.handle, C.byref(hs), _stream_handle(stream)), "edm_get_state")
+        return out
+
+    def set_step(self, k: int):
+        _check(self.L.edm_set_step(self.handle, int(k)), "edm_set_step")
+
+    def get_step(self) -> int:
+        return int(self.L.edm_get_step(self.handle))
+
+    # ---- stepping ------------------------------------------------------------
+    def dynamics_step(self, n: int = 1, stream=None):
+        _check(self.L.edm_dynamics_step(self.handle, int(n), _stream_handle(stream)), "edm_dynamics_step")
+
+    def photon_step(self, stream=None):
+        _check(self.L.edm_photon_step(self.handle, _stream_handle(stream)), "edm_photon_step")
+
+    def scope_process(self, stream=None):
+        _check(self.L.edm_scope_process(self.handle, _stream_handle(stream)), "edm_scope_process")
+
+    def pipeline_steps(self, n: int, with_photons: bool = True, graph_chunk: int = 0, stream=None):
+        _check(self.L.edm_pipeline_steps(self.handle, int(n), int(bool(with_photons)), int(graph_chunk),
+                                         _stream_handle(stream)), "edm_pipeline_steps")
+
+    def set_photons(self, replica: int, particle_idx, arrival_time, channel, is_fret, batch_key: int, stream=None):
+        pid = np.ascontiguousarray(particle_idx, dtype=np.int32)
+        t = np.ascontiguousarray(arrival_time, dtype=np.float64)
+        ch = np.ascontiguousarray(channel, dtype=np.int8)
+        fr = np.ascontiguousarray(is_fret, dtype=np.uint8)
+        _check(self.L.edm_set_photons(self.handle, replica, _ptr(pid), _ptr(t), _ptr(ch), _ptr(fr), pid.size,
+                                      int(batch_key), _stream_handle(stream)), "edm_set_photons")
+
+    def finalize(self, frame_index: int, stream=None):
+        _check(self.L.edm_scope_finalize(self.handle, int(frame_index), _stream_handle(stream)), "edm_scope_finalize")
+
+    # ---- outputs -------------------------------------------------------------
+    def photon_counts(self, stream=None) -> np.ndarray:
+        out = np.zeros(self.R, dtype=np.int64)
+        _check(self.L.edm_get_photon_counts(self.handle, _ptr(out), _stream_handle(stream)), "edm_get_photon_counts")
+        return out
+
+    def photons(self, replica: int = 0, stream=None):
+        cap = int(self._phot[replica].max_photons)
+        pid = np.empty(cap, np.int32)
+        t = np.empty(cap, np.float64)
+        ch = np.empty(cap, np.int8)
+        fr = np.empty(cap, np.uint8)
+        n = _check(self.L.edm_get_photons(self.handle, replica, _ptr(pid), _ptr(t), _ptr(ch), _ptr(fr), cap,
+                                          _stream_handle(stream)), "edm_get_photons")
+        return pid[:n].copy(), t[:n].copy(), ch[:n].copy(), fr[:n].astype(bool)
+
+    def flim(self, replica: int = 0, stream=None) -> np.ndarray:
+        sp = self._scope[replica]
+        shape = (sp.n_channels, sp.nx, sp.ny, sp.n_bins)
+        out = np.empty(shape, dtype=np.uint32)
+        _check(self.L.edm_get_flim(self.handle, replica, _ptr(out), out.size, _stream_handle(stream)), "edm_get_flim")
+        return out
+
+    def reset_flim(self, stream=None):
+        _check(self.L.edm_reset_flim(self.handle, _stream_handle(stream)), "edm_reset_flim")
+
+    def counters(self, stream=None) -> np.ndarray:
+        out = np.zeros((self.R, PR.NCOUNTERS), dtype=np.int64)
+        _check(self.L.edm_get_counters(self.handle, _ptr(out), _stream_handle(stream)), "edm_get_counters")
+        return out
+
+    def status(self, stream=None) -> int:
+        v = C.c_uint32(0)
+        _check(self.L.edm_get_status(self.handle, C.byref(v), _stream_handle(stream)), "edm_get_status")
+        return int(v.value)
+
+    def cells(self, replica: int = 0, stream=None):
+        p = self._dyn[replica]
+        nc = p.nx * p.ny
+        start = np.empty(nc + 1, np.int32)
+        mem = np.empty(max(p.n_particles, 1), np.int32)
+        _check(self.L.edm_get_cells(self.handle, replica, _ptr(start), _ptr(mem), nc + 1, mem.size,
+                                    _stream_handle(stream)), "edm_get_cells")
+        return start, mem[:p.n_particles]
+
+
+# ---------------------------------------------------------------------------
+# keyed noise of the device generator (for injection / tests)
+# ---------------------------------------------------------------------------
+def device_normals(seed: int, step: int, stream_id: int, keys) -> np.ndarray:
+    import torch
+    L = load_library()
+    k = torch.as_tensor(np.asarray(keys, dtype=np.int64), device="cuda")
+    out = torch.empty((k.numel(), 2), dtype=torch.float64, device="cuda")
+    _check(L.edm_noise_normal_pairs(seed, step, stream_id, C.c_void_p(k.data_ptr()), k.numel(),
+                                    C.c_void_p(out.data_ptr()), None), "edm_noise_normal_pairs")
+    return out.cpu().numpy()
+
+
+def device_uniforms(seed: int, step: int, stream_id: int, a, b=None) -> np.ndarray:
+    import torch
+    L = load_library()
+    ka = torch.as_tensor(np.asarray(a, dtype=np.int64), device="cuda")
+    kb = None if b is None else torch.as_tensor(np.asarray(b, dtype=np.int64), device="cuda")
+    out = torch.empty((ka.numel(), 2), dtype=torch.float64, device="cuda")
+    _check(L.edm_noise_uniforms(seed, step, stream_id, C.c_void_p(ka.data_ptr()),
+                                None if kb is None else C.c_void_p(kb.data_ptr()), ka.numel(),
+                                C.c_void_p(out.data_ptr()), None), "edm_noise_uniforms")
+    return out.cpu().numpy()
+
+
+# ---------------------------------------------------------------------------
+# Device-resident system bound to one ParticleState
+# ---------------------------------------------------------------------------
+_SYNC_FIELDS = ("positions", "species_id", "is_alive", "bond_partner", "has_dye", "dye_type_id",
+                "ctmc_state", "is_bleached")
+
+
+class DeviceSystem:
+    """One replica on the GPU, bound to a host ParticleState.
+
+    Shared by the DynamicsEngine / PhotonSimulator / VirtualMicroscope of the
+    same state (state._device_owner).  Host arrays are uploaded lazily when
+    they changed since the last sync, and downloaded on request."""
+
+    def __init__(self, config, state, scan_duty_fraction: Optional[float] = None, precision: int = 64,
+                 device: int = 0):
+        self.config = config
+        self.state = state
+        self.precision = precision
+        self.dp, self.hill, self.derived = PR.build_dyn_params(config, state.N)
+        self.duty = scan_duty_fraction
+        phot = scope = None
+        self.pd = self.sd = None
+        if scan_duty_fraction is not None and len(config.fluorophores) > 0:
+            self.pp, self.pd = PR.build_phot_params(config, state.N, int(np.count_nonzero(state.has_dye)),
+                                                    scan_duty_fraction)
+            self.sp, self.sd = PR.build_scope_params(config)
+            phot, scope = [self.pp], [self.sp]
+        self.engine = Engine([self.dp], self.hill, phot, scope, precision=precision, device=device)
+        self._snapshot = None
+        self._host_current = True
+        self.upload()
+        state._device_owner = self
+        self._host_dirty = False
+
+    @property
+    def has_photophysics(self) -> bool:
+        return self.pd is not None and self.pd.active
+
+    def _host_changed(self) -> bool:
+        if self._snapshot is None:
+            return True
+        s = self.state
+        return any(not np.array_equal(getattr(s, f), self._snapshot[f]) for f in _SYNC_FIELDS)
+
+    def upload(self):
+        s = self.state
+        self.engine.set_state(s.positions, s.species_id, s.is_alive, s.bond_partner, s.has_dye, s.dye_type_id,
+                              s.ctmc_state, s.is_bleached)
+        self._snapshot = {f: getattr(s, f).copy() for f in _SYNC_FIELDS}
+        self._host_current = True
+
+    def ensure_device(self):
+        """Upload host arrays if the user changed them since the last sync."""
+        if self._host_current and (self._host_dirty or self._host_changed()):
+            self.upload()
+            self._host_dirty = False
+
+    def mark_device_newer(self):
+        self._host_current = False
+
+    def _download_state(self):
+        if self._host_current:
+            return
+        st = self.engine.get_state()
+        s = self.state
+        s.positions[:] = st["positions"]
+        s.species_id[:] = st["species"]
+        s.is_alive[:] = st["alive"].astype(bool)
+        s.bond_partner[:] = st["bond"]
+        s.ctmc_state[:] = st["ctmc"]
+        s.is_bleached[:] = st["bleached"].astype(bool)
+        self._snapshot = {f: getattr(s, f).copy() for f in _SYNC_FIELDS}
+        self._host_current = True
+
+    def sync_host(self):
+        self._download_state()

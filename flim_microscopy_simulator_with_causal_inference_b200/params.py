@@ -129,6 +129,7 @@ class EdmPhotParams(C.Structure):
         ("tau_all", C.c_double * MAX_FLUO),
         ("has_fret_cls", C.c_int32 * MAX_FCLASS),
         ("fret", EdmFret * MAX_FRET),
+        ("donor_channel", C.c_int32), ("acceptor_channel", C.c_int32),
         ("max_photons", C.c_int64), ("est_photons", C.c_int64),
         ("photon_offset", C.c_int64), ("emitter_offset", C.c_int64), ("n_emitters", C.c_int64),
     ]
@@ -804,6 +805,7 @@ def build_phot_params(config: SimulationConfig, n_particles: int, n_labeled: int
                 P.T00[t][pss][c], P.T0001[t][pss][c] = t00, t00 + t01
     for c, k in enumerate(ks):
         P.has_fret_cls[c] = int(k > 0.0)
+    P.donor_channel, P.acceptor_channel = d.donor_channel, d.acceptor_channel
     P.max_photons, P.est_photons = d.max_photons, d.est_photons
     P.photon_offset, P.emitter_offset, P.n_emitters = photon_offset, emitter_offset, n_emitters
     return P, d

@@ -184,6 +184,7 @@ typedef struct {
   double tau_all[EDM_MAX_FLUO];
   int32_t has_fret_cls[EDM_MAX_FCLASS];               /* k_fret > 0         */
   EdmFret fret[EDM_MAX_FRET];
+  int32_t donor_channel, acceptor_channel;            /* photophysics.py:782-787 */
   int64_t max_photons, est_photons;
   int64_t photon_offset; /* start of this replica's slice of the photon buffer */
   int64_t emitter_offset, n_emitters;
@@ -269,6 +270,14 @@ int edm_get_photons(EdmEngine* eng, int32_t replica, int32_t* particle_idx,
 /* VirtualMicroscope.process_photons(batch) (microscope.py:1069-1157) on the
  * last device batch. */
 int edm_scope_process(EdmEngine* eng, void* stream);
+
+/* Load a host photon batch (PhotonBatch fields, photophysics.py:184-211) of
+ * one replica as the current device batch; its per-photon draws are keyed
+ * by batch_key.  For batches not produced by edm_photon_step. */
+int edm_set_photons(EdmEngine* eng, int32_t replica, const int32_t* particle_idx,
+                    const double* arrival_time, const int8_t* channel,
+                    const uint8_t* is_fret, int64_t n, int64_t batch_key,
+                    void* stream);
 
 /* One fused BD step of the whole pipeline loop body (pipeline.py:554-564):
  * dynamics step, photophysics, photon processing; n_steps times, with the

@@ -1,0 +1,131 @@
+"""CUDA engine vs the CPU oracle (the reference's algorithm restated in C).
+
+float64 path: same inputs, same keyed noise -> identical cell lists, event
+sets, counters and photon streams; positions equal to <= 1e-12 µm (bit-exact
+except where the device's exp/sin/log differ from the host libm by an ulp:
+the D(x) field and photon arrival times).
+float32 path (cell-relative positions): lockstep, i.e. the oracle's state is
+loaded before every step; positions within 1e-5 µm per step, identical event
+sets.
+"""
+import numpy as np
+import pytest
+
+from tests import cases
+from tests.harness import Pair, compare_state, cell_sets_oracle
+
+pytestmark = pytest.mark.gpu
+
+F64_TOL = 1e-12      # µm, float64 path vs oracle, free running
+F32_TOL = 1e-5       # µm per step, float32 path vs oracle, lockstep
+
+
+def test_noise_streams_bit_identical():
+    from flim_microscopy_simulator_with_causal_inference_b200.engine import device_normals, device_uniforms
+    from oracle import oracle as O
+    keys = np.arange(0, 200000, 7, dtype=np.int64)
+    for seed, step, stream in ((42, 0, 1), (2 ** 40 + 3, 123456789012, 122), (7, 5, 32)):
+        assert np.array_equal(device_normals(seed, step, stream, keys), O.normals(seed, step, stream, keys))
+        b = keys[::-1].copy()
+        assert np.array_equal(device_uniforms(seed, step, stream, keys, b), O.uniforms(seed, step, stream, keys, b, two=True))
+
+
+@pytest.mark.parametrize("case", ["rich_small", "binding_regions", "harmonic_small"])
+def test_fp64_free_running_matches_oracle(case):
+    P = Pair(cases.get(case), precision=64)
+    steps = 40
+    for t in range(steps):
+        P.eng.dynamics_step(1)
+        P.orc.dynamics_step()
+        P.orc.step_index += 1
+        if t % 10 == 9 or t == 0:
+            compare_state(P.gpu_state(), P.orc, F64_TOL)
+    g = P.eng.counters()[0]
+    assert np.array_equal(g[:6], P.orc.counters[:6]), (g[:6], P.orc.counters[:6])
+    if case in ("rich_small", "binding_regions"):
+        assert P.orc.counters[:6].sum() > 0, "test system produced no reaction events"
+
+
+def test_fp64_cell_lists_match_oracle():
+    P = Pair(cases.get("rich_small"), precision=64)
+    for _ in range(3):
+        P.eng.dynamics_step(1)
+        P.orc.dynamics_step()
+        P.orc.step_index += 1
+        start, mem = P.eng.cells(0)
+        gsets = [sorted(mem[start[c]:start[c + 1]].tolist()) for c in range(P.dp.nx * P.dp.ny)]
+        assert gsets == cell_sets_oracle(P.orc, P.dp.nx, P.dp.ny)
+
+
+@pytest.mark.parametrize("case", ["rich_small", "binding_regions"])
+def test_fp64_pipeline_photons_and_tcspc_match_oracle(case):
+    P = Pair(cases.get(case), precision=64)
+    total = 0
+    for t in range(30):
+        P.eng.dynamics_step(1)
+        P.eng.photon_step()
+        P.eng.scope_process()
+        ob = P.orc.bd_step()
+        pid, tt, ch, fr = P.eng.photons(0)
+        assert np.array_equal(pid, ob[0]), f"photon emitters differ at step {t}"
+        assert np.array_equal(ch, ob[2]) and np.array_equal(fr, ob[3])
+        np.testing.assert_allclose(tt, ob[1], rtol=1e-14, atol=0)
+        total += pid.size
+        if t % 10 == 9:
+            assert np.array_equal(P.eng.flim(0), P.orc.flim), f"TCSPC stacks differ at step {t}"
+    assert total > 0
+    P.eng.finalize(0)
+    of = P.orc.finalize_frame()
+    assert np.array_equal(P.eng.flim(0), of)
+    compare_state(P.gpu_state(), P.orc, F64_TOL)
+
+
+def test_fp64_graph_chunks_match_eager():
+    raw = cases.get("rich_small")
+    A = Pair(raw, precision=64)
+    B = Pair(raw, precision=64)
+    import torch
+    s = torch.cuda.Stream()
+    A.eng.pipeline_steps(40, True, 10, stream=s)
+    s.synchronize()
+    B.eng.pipeline_steps(40, True, 0)
+    ga, gb = A.gpu_state(), B.gpu_state()
+    for k in ga:
+        assert np.array_equal(ga[k], gb[k]), k
+    assert np.array_equal(A.eng.flim(0), B.eng.flim(0))
+    assert np.array_equal(A.eng.counters(), B.eng.counters())
+
+
+@pytest.mark.parametrize("case", ["rich_small", "binding_regions", "sine_small"])
+def test_fp32_lockstep_matches_oracle(case):
+    P = Pair(cases.get(case), precision=32)
+    worst = 0.0
+    for t in range(25):
+        P.load_oracle_state_into_gpu()
+        P.eng.dynamics_step(1)
+        P.orc.dynamics_step()
+        P.orc.step_index += 1
+        worst = max(worst, compare_state(P.gpu_state(), P.orc, F32_TOL))
+    assert worst < F32_TOL
+
+
+def test_sine_field_fp64_close():
+    P = Pair(cases.get("sine_small"), precision=64)
+    for t in range(20):
+        P.eng.dynamics_step(1)
+        P.orc.dynamics_step()
+        P.orc.step_index += 1
+    compare_state(P.gpu_state(), P.orc, 1e-9)
+
+
+def test_determinism_two_runs_bitwise():
+    raw = cases.get("rich_small")
+    runs = []
+    for _ in range(2):
+        P = Pair(raw, precision=32)
+        P.eng.pipeline_steps(30, True, 0)
+        runs.append((P.gpu_state(), P.eng.flim(0), P.eng.counters()))
+    for k in runs[0][0]:
+        assert np.array_equal(runs[0][0][k], runs[1][0][k]), k
+    assert np.array_equal(runs[0][1], runs[1][1])
+    assert np.array_equal(runs[0][2], runs[1][2])
