@@ -1,0 +1,357 @@
+"""Benchmark of the per-timestep hot path on B200.
+
+Workload (headline): the batched ensemble -- 512 independent PIP3/PTEN
+membrane replicas, particle count log-uniform in 1,000-50,000 per replica,
+box side scaled to keep the density, k_cat and K_half jittered, float32
+cell-relative path, every BD step = dynamics + reactions + PSS photophysics
++ PSF/TCSPC detection of all replicas, captured as CUDA graphs of 100 steps.
+
+A bench "step" is one FLIM frame of 100 BD timesteps over all replicas:
+pipeline steps, then finalize_frame (dark counts, afterpulsing).
+
+* value      particle-steps/s (membrane particles x BD steps / s) with the
+             state resident on the GPU, whole job over all ranks;
+* e2e        the same metric through the C-ABI frame loop a caller runs with
+             host buffers: per frame upload the state from pinned memory,
+             100 pipeline steps, finalize, read back every FLIM stack and
+             the state;
+* roofline   the dominant kernel group's algorithmic bytes / CUDA-event time;
+* fp64_plain the plain float64 path (same kernels, one 13,000-particle
+             system, per-step launches, no graphs) for the FP32/FP64 ratio;
+* cpu_baseline the CPU oracle (the reference algorithm restated in C) on
+             this host's cores on a bounded sample of the same workload.
+
+`--impl reference` runs the CPU oracle alone on a bounded sample of the
+same workload with every host core (rank 0 only) and prints its line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "particle-steps/s & FLIM px/s: batched FP32 vs plain FP64, 1 B200, fixed error"
+UNIT = "particle-steps/s"
+STEPS_PER_FRAME = 100
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5, help="timed frames (100 BD steps each)")
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--replicas", type=int, default=512)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 5 + i and s[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the oracle on a bounded sample
+# ---------------------------------------------------------------------------
+def oracle_sample(raws, steps: int, threads: int):
+    """Run `steps` BD steps (full per-step path) of each replica in `raws` on
+    the CPU oracle, replicas in parallel threads; returns particle-steps/s."""
+    from flim_microscopy_simulator_with_causal_inference_b200 import params as PR
+    from flim_microscopy_simulator_with_causal_inference_b200.config import config_from_dict
+    from flim_microscopy_simulator_with_causal_inference_b200.particles import ParticleState
+    from oracle import oracle as O
+
+    sims = []
+    for raw in raws:
+        cfg = config_from_dict(raw)
+        st = ParticleState(cfg)
+        dp, _, _ = PR.build_dyn_params(cfg, st.N, hill_len=2)
+        duty = min(1.0, cfg.scan.dwell_time / cfg.scan.frame_interval)
+        _, pd = PR.build_phot_params(cfg, st.N, int(st.has_dye.sum()), duty)
+        sp, _ = PR.build_scope_params(cfg)
+        sims.append((O.OracleSimulation(cfg, st, dp, pd, sp, duty), int(sum(cfg.initial_populations.values()))))
+
+    def run(sim):
+        o, _ = sim
+        for _ in range(steps):
+            o.bd_step()
+
+    O.lib()
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        list(ex.map(run, sims))
+    dt = time.perf_counter() - t0
+    ps = sum(n for _, n in sims) * steps
+    return ps / dt, dt, ps
+
+
+def reference_arm(args, rank: int, world: int):
+    if rank != 0:
+        return
+    from flim_microscopy_simulator_with_causal_inference_b200 import workloads as W
+    raws = W.ensemble_replicas(args.replicas, seed=args.seed)
+    cores = os.cpu_count() or 1
+    # bounded sample: the 16 replicas nearest the median size, 10 BD steps each
+    sizes = np.array([sum(r["initial_populations"].values()) for r in raws])
+    order = np.argsort(np.abs(sizes - np.median(sizes)))[:16]
+    sample = [raws[i] for i in order]
+    for _ in range(max(0, args.warmup)):
+        oracle_sample(sample[:2], 1, cores)
+    vals = []
+    for _ in range(max(1, args.steps)):
+        v, dt, ps = oracle_sample(sample, 10, cores)
+        vals.append(v)
+    value = float(statistics.median(vals))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"batched ensemble, {args.replicas} replicas (sample: 16 median-size replicas x 10 BD "
+                               "steps per timed step)", "replicas": args.replicas},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": "16 median-size replicas x 10 full BD steps (dynamics+photophysics+TCSPC)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU side
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    device = local
+    torch.cuda.set_device(device)
+    from flim_microscopy_simulator_with_causal_inference_b200 import params as PR
+    from flim_microscopy_simulator_with_causal_inference_b200 import workloads as W
+    from flim_microscopy_simulator_with_causal_inference_b200.batch import Ensemble
+
+    raws = W.ensemble_replicas(args.replicas, seed=args.seed + 7919 * rank)
+    ens = Ensemble(raws, precision=32, photons=True, device=device)
+    eng = ens.engine
+    stream = torch.cuda.Stream(device=device)
+    frame = 0
+
+    def run_frame():
+        nonlocal frame
+        eng.pipeline_steps(STEPS_PER_FRAME, True, STEPS_PER_FRAME, stream=stream)
+        eng.finalize(frame, stream=stream)
+        eng.reset_flim(stream=stream)
+        frame += 1
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(3, args.warmup)):
+            run_frame()
+    stream.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(device) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            run_frame()
+        e1.record(stream)
+        stream.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    n_mem = ens.total_membrane
+    value = n_mem * world * STEPS_PER_FRAME * args.steps / (ms / 1e3)
+    launches = eng.launches_per_step(True) * STEPS_PER_FRAME * args.steps + 2 * args.steps
+    status = eng.status()
+
+    # ---- e2e through the C ABI with host buffers ---------------------------
+    h = ens.host
+    pinned = {k: torch.from_numpy(v).pin_memory().numpy() for k, v in h.items()}
+    flim_elems = sum(sp.n_channels * sp.nx * sp.ny * sp.n_bins for sp in eng._scope)
+    flim_host = torch.empty(flim_elems, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+    state_bytes_in = sum(v.nbytes for v in pinned.values())
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        eng.set_state(pinned["positions"], pinned["species"], pinned["alive"], pinned["bond"], pinned["has_dye"],
+                      pinned["dye"], pinned["ctmc"], pinned["bleached"], stream=stream)
+        eng.pipeline_steps(STEPS_PER_FRAME, True, STEPS_PER_FRAME, stream=stream)
+        eng.finalize(frame, stream=stream)
+        off = 0
+        for r in range(ens.R):
+            sp = eng._scope[r]
+            n = sp.n_channels * sp.nx * sp.ny * sp.n_bins
+            eng.L.edm_get_flim(eng.handle, r, flim_host[off:off + n].ctypes.data_as(__import__("ctypes").c_void_p), n,
+                               int(stream.cuda_stream))
+            off += n
+        eng.reset_flim(stream=stream)
+        st = eng.get_state(stream=stream)
+        frame += 1
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = n_mem * world * STEPS_PER_FRAME * args.steps / e2e_s
+    state_bytes_out = sum(v.nbytes for v in st.values())
+    h2d = state_bytes_in / STEPS_PER_FRAME
+    d2h = (flim_elems * 4 + state_bytes_out) / STEPS_PER_FRAME
+
+    # ---- per-kernel-group timing (CUDA events, eager) -----------------------
+    prof = eng.profile_steps(20, True, stream=stream)
+    N = ens.total_particles
+    alg = {  # algorithmic bytes per particle of each group (float32 path)
+        "scatter": 2 * (8 + 4 + 1 + 4) + 4,   # read + write slot record, inverse map
+        "move": (8 + 4 + 1 + 4) + (8 + 4),     # read pre-move slot, write post-move position/cell
+    }
+    groups = {k: prof[k] for k in ("cell_scan", "scatter", "move", "reactions", "photophysics", "detection")}
+    dom = max(("scatter", "move"), key=lambda k: groups[k])
+    peak, peak_kind = peaks()
+    achieved = alg[dom] * N / (groups[dom] / 1e3) / 1e9
+    traffic = None
+    tr_file = ROOT / "profiles" / "traffic.json"
+    if tr_file.exists():
+        traffic = json.loads(tr_file.read_text()).get(dom)
+
+    # ---- plain float64 path: one 13,000-particle system, per-step launches ---
+    fp64 = None
+    if not args.no_fp64 and rank == 0:
+        from flim_microscopy_simulator_with_causal_inference_b200.batch import Ensemble as E2
+        c1 = E2([W.config1(n_frames=1)], precision=64, photons=True, device=device)
+        c1.engine.pipeline_steps(20, True, 0, stream=stream)
+        stream.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        n64 = 200
+        f0.record(stream)
+        c1.engine.pipeline_steps(n64, True, 0, stream=stream)
+        f1.record(stream)
+        stream.synchronize()
+        fp64 = c1.total_membrane * n64 / (f0.elapsed_time(f1) / 1e3)
+        del c1
+
+    # ---- CPU baseline (oracle) on a bounded sample ---------------------------
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0:
+        sizes = np.array([sum(r["initial_populations"].values()) for r in raws])
+        order = np.argsort(np.abs(sizes - np.median(sizes)))[:16]
+        cores = os.cpu_count() or 1
+        v, dt, ps = oracle_sample([raws[i] for i in order], 10, cores)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"16 median-size replicas x 10 full BD steps ({ps} particle-steps, {dt:.1f} s)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"batched ensemble: {args.replicas} PIP3/PTEN replicas per GPU, N log-uniform "
+                                   f"1k-50k ({n_mem} membrane + {N - n_mem} dormant particles), full BD step "
+                                   "(dynamics+reactions+PSS photons+TCSPC), CUDA graphs of 100 steps; step = one "
+                                   "frame of 100 BD steps",
+                       "replicas": args.replicas, "particles": N, "membrane_particles": n_mem,
+                       "bd_steps_per_step": STEPS_PER_FRAME, "precision": "f32 cell-relative positions",
+                       "l2": "working set > 126 MB L2 (resident state ~45 B/particle)"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "note": "per frame: state H2D from pinned host, 100 BD steps, finalize, all FLIM stacks + state "
+                            "D2H; bytes are per BD step"},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "alg_bytes_per_particle": alg[dom], "kernel_ms": groups[dom]},
+            "kernel_ms_per_step": groups,
+            "fp64_plain": None if fp64 is None else {"value": fp64, "unit": UNIT,
+                                                     "workload": "13,000-particle system with sine D(x), float64, "
+                                                                 "per-step launches, full BD step"},
+            "fp32_over_fp64": None if fp64 is None else value / world / fp64,
+            "cpu_baseline": cpu,
+            "gpu_launches": launches,
+            "status_word": status,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -106,6 +106,7 @@ struct EdmEngine {
   uint8_t *st_alive = nullptr, *st_bl = nullptr;
   int8_t* st_ctmc = nullptr;
   std::vector<Pass> passes;
+  std::vector<int32_t> emit_host;  // emitter list last uploaded
   std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;
   std::vector<void*> allocs;
 
@@ -218,12 +219,20 @@ struct EdmEngine {
     }
   }
 
+  // optional CUDA events between kernel groups (profiling only)
+  cudaEvent_t* prof = nullptr;
+  void mark(int k, cudaStream_t s) {
+    if (prof) cudaEventRecord(prof[k], s);
+  }
+
   template <bool F64>
   void enqueue_dynamics_t(cudaStream_t s) {
     const int nbs = nb_scan;
+    mark(0, s);
     k_scan_reduce<<<nbs, kScanThreads, 0, s>>>(cnt, n_cells, bsum);
     k_scan_bsum<<<1, 1024, 0, s>>>(bsum, nbs);
     k_scan_down<<<nbs, kScanThreads, 0, s>>>(cnt, n_cells, bsum, cell_start, cursor);
+    mark(1, s);
     cur ^= 1;
     DevState st = dev_state();
     k_scatter<F64><<<npblk, kBlock, 0, s>>>(dp, pblk, st);
@@ -231,7 +240,9 @@ struct EdmEngine {
       cudaMemsetAsync(grid_cnt, 0, sizeof(int32_t) * n_grid, s);
       cudaMemsetAsync(grid_delta, 0, sizeof(int32_t) * n_grid, s);
     }
+    mark(2, s);
     k_move<F64><<<npblk, kBlock, 0, s>>>(dp, pblk, st);
+    mark(3, s);
     const int rb = (R + 127) / 128;
     const int gm = (int)std::min<int64_t>((n_grid + 255) / 256, 4096);
     for (const Pass& ps : passes) {
@@ -248,6 +259,13 @@ struct EdmEngine {
       }
     }
     k_step_inc<<<1, 1, 0, s>>>(d_step);
+    mark(4, s);
+  }
+
+  int launches_per_step(bool with_photons) const {
+    int n = 3 + 1 + 1 + (int)passes.size() + 1;
+    if (with_photons) n += (neblk > 0 ? 3 : 1) + 1 + (nphblk > 0 ? 1 : 0) + 1;
+    return n;
   }
 
   void enqueue_dynamics(cudaStream_t s) {
@@ -603,6 +621,12 @@ int edm_set_state(EdmEngine* E, const EdmHostState* st, void* stream) {
       off = (int64_t)eid.size();
     }
     (void)off;
+    if (eid == E->emit_host) {  // same emitters: keep tiles and captured graphs
+      CUDA_TRY(cudaStreamSynchronize(s));
+      CUDA_TRY(cudaGetLastError());
+      return EDM_OK;
+    }
+    E->emit_host = eid;
     E->n_emit = (int64_t)eid.size();
     if (!eid.empty())
       CUDA_TRY(cudaMemcpyAsync(E->emit_id, eid.data(), sizeof(int32_t) * eid.size(), cudaMemcpyHostToDevice, s));
@@ -781,6 +805,53 @@ int edm_pipeline_steps(EdmEngine* E, int32_t n_steps, int32_t with_photons, int3
   for (; done < n_steps; ++done) body(s);
   CUDA_TRY(cudaGetLastError());
   return EDM_OK;
+}
+
+int edm_profile_steps(EdmEngine* E, int32_t n_steps, int32_t with_photons, float* ms_out, void* stream) {
+  if (!E || n_steps <= 0 || !ms_out) return fail(EDM_EINVAL, "edm_profile_steps: bad argument");
+  if (with_photons && !E->has_scope) return fail(EDM_EINVAL, "edm_profile_steps: no photophysics/microscope");
+  CUDA_TRY(cudaSetDevice(E->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaEvent_t ev[7];
+  for (int k = 0; k < 7; ++k) CUDA_TRY(cudaEventCreate(&ev[k]));
+  double acc[EDM_NPROF] = {0, 0, 0, 0, 0, 0, 0};
+  E->prof = ev;
+  for (int i = 0; i < n_steps; ++i) {
+    E->enqueue_dynamics(s);
+    if (with_photons) {
+      E->enqueue_photons(s);
+      cudaEventRecord(ev[5], s);
+      E->enqueue_scope(s);
+      cudaEventRecord(ev[6], s);
+    }
+    cudaError_t e = cudaEventSynchronize(with_photons ? ev[6] : ev[4]);
+    if (e != cudaSuccess) {
+      E->prof = nullptr;
+      return fail(EDM_ECUDA, cudaGetErrorString(e));
+    }
+    float t;
+    for (int k = 0; k < 4; ++k) {
+      cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+      acc[k] += t;
+    }
+    if (with_photons) {
+      cudaEventElapsedTime(&t, ev[4], ev[5]);
+      acc[4] += t;
+      cudaEventElapsedTime(&t, ev[5], ev[6]);
+      acc[5] += t;
+    }
+    cudaEventElapsedTime(&t, ev[0], with_photons ? ev[6] : ev[4]);
+    acc[6] += t;
+  }
+  E->prof = nullptr;
+  for (int k = 0; k < 7; ++k) cudaEventDestroy(ev[k]);
+  for (int k = 0; k < EDM_NPROF; ++k) ms_out[k] = (float)(acc[k] / n_steps);
+  return EDM_OK;
+}
+
+int edm_launches_per_step(EdmEngine* E, int32_t with_photons) {
+  if (!E) return fail(EDM_EINVAL, "null engine");
+  return E->launches_per_step(with_photons != 0);
 }
 
 int edm_scope_finalize(EdmEngine* E, int64_t frame_index, void* stream) {

@@ -69,6 +69,8 @@ def load_library():
     L.edm_get_counters.argtypes = [vp, vp, vp]
     L.edm_get_status.argtypes = [vp, vp, vp]
     L.edm_get_cells.argtypes = [vp, i32, vp, vp, i64, i64, vp]
+    L.edm_profile_steps.argtypes = [vp, i32, i32, vp, vp]
+    L.edm_launches_per_step.argtypes = [vp, i32]
     L.edm_noise_normal_pairs.argtypes = [u64, i64, i32, vp, i64, vp, vp]
     L.edm_noise_uniforms.argtypes = [u64, i64, i32, vp, vp, i64, vp, vp]
     for which, cls in ((0, PR.EdmDynParams), (1, PR.EdmPhotParams), (2, PR.EdmScopeParams), (3, PR.EdmHostState)):
@@ -181,6 +183,18 @@ class Engine:
         fr = np.ascontiguousarray(is_fret, dtype=np.uint8)
         _check(self.L.edm_set_photons(self.handle, replica, _ptr(pid), _ptr(t), _ptr(ch), _ptr(fr), pid.size,
                                       int(batch_key), _stream_handle(stream)), "edm_set_photons")
+
+    PROFILE_GROUPS = ("cell_scan", "scatter", "move", "reactions", "photophysics", "detection", "step")
+
+    def profile_steps(self, n: int, with_photons: bool = True, stream=None) -> dict:
+        """Mean device ms per step of each kernel group (CUDA events, eager)."""
+        out = np.zeros(7, dtype=np.float32)
+        _check(self.L.edm_profile_steps(self.handle, int(n), int(bool(with_photons)), _ptr(out),
+                                        _stream_handle(stream)), "edm_profile_steps")
+        return dict(zip(self.PROFILE_GROUPS, out.astype(float).tolist()))
+
+    def launches_per_step(self, with_photons: bool = True) -> int:
+        return _check(self.L.edm_launches_per_step(self.handle, int(bool(with_photons))), "edm_launches_per_step")
 
     def finalize(self, frame_index: int, stream=None):
         _check(self.L.edm_scope_finalize(self.handle, int(frame_index), _stream_handle(stream)), "edm_scope_finalize")

@@ -381,6 +381,11 @@ def check_supported(config: SimulationConfig) -> None:
             raise NotImplementedError(
                 f"catalytic reaction '{cat.name}': enzyme == product/substrate makes a pass "
                 "order-dependent; not supported by the parallel pass")
+    for rx in config.reactions:
+        if rx.is_bimolecular and rx.products and rx.products[0] in rx.reactants:
+            raise NotImplementedError(
+                f"binding reaction '{rx.name}': a product equal to a reactant re-enters the same pass; "
+                "not supported by the candidate-list pass")
     df = config.diffusion_field
     if df.type not in ("uniform", "regions", "sine_x"):
         raise NotImplementedError(f"diffusion_field.type '{df.type}'")

@@ -297,6 +297,16 @@ int edm_reset_flim(EdmEngine* eng, void* stream);
 int edm_get_counters(EdmEngine* eng, int64_t* out, void* stream);
 int edm_get_status(EdmEngine* eng, uint32_t* status, void* stream);
 
+/* Instrumented eager steps: runs n_steps pipeline steps with CUDA events
+ * around each kernel group and writes the mean device time per step (ms) of
+ * ms_out[EDM_NPROF]: cell-list scan, scatter, force+move, reaction passes,
+ * photophysics, photon detection, whole step.  No reference counterpart. */
+#define EDM_NPROF 7
+int edm_profile_steps(EdmEngine* eng, int32_t n_steps, int32_t with_photons,
+                      float* ms_out, void* stream);
+/* Kernels of this library launched per pipeline step. */
+int edm_launches_per_step(EdmEngine* eng, int32_t with_photons);
+
 /* Device pointer to the cell-list arrays of the last dynamics step
  * (CellList.head/next equivalent, dynamics.py:109-138): per replica cell c
  * holds particle indices sorted[start[c] .. start[c+1]) (global indices).  */

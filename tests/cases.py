@@ -48,10 +48,14 @@ def binding_regions(seed: int = 11) -> dict:
 
 
 def harmonic_small(seed: int = 5) -> dict:
-    """Dense harmonic soft repulsion (many simultaneous overlaps)."""
+    """Dense harmonic soft repulsion (many simultaneous overlaps).  Contact
+    radii are short (10 nm) so the candidate pair list stays below the
+    reference's silent cap of min(30 N, 500000) pairs (dynamics.py:233)."""
     d = W.membrane_pip3_pten(counts={"PIP2": 3000, "PIP3": 300, "PI3K": 100, "PTEN_T1": 200, "PTEN_T2": 100},
                              pools={"PI3K": 50, "PTEN_T1": 50}, box=0.6, potential="harmonic", pixels=8,
-                             pixel_size_nm=70.0, seed=seed, k_cat_scale=50.0)
+                             pixel_size_nm=70.0, seed=seed, k_cat_scale=5000.0)
+    for c in d["catalytic_reactions"]:
+        c["contact_radius"] = 10.0
     for p in d["potentials"]:
         p["parameters"]["sigma"] = 12.0
         p["parameters"]["spring_constant"] = 2.0e5
