@@ -61,6 +61,35 @@ def parse():
     return ap.parse_args()
 
 
+def rank_replicas(n_replicas: int, seed: int, rank: int):
+    """The replicas of one rank: each rank runs its own ensemble (weak
+    scaling, no exchange between ranks), seeded per rank."""
+    from flim_microscopy_simulator_with_causal_inference_b200 import workloads as W
+    return W.ensemble_replicas(n_replicas, seed=seed + 7919 * rank)
+
+
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    """Job time = the slowest rank's time (all-reduce MAX)."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device if device is not None else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_particle_steps(n_membrane_local: int, world: int, steps: int, device=None) -> int:
+    """Membrane particle-steps of the whole job (sum over ranks)."""
+    if world <= 1:
+        return n_membrane_local * steps
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([n_membrane_local], dtype=torch.int64, device=device if device is not None else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return int(t.item()) * steps
+
+
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -201,7 +230,7 @@ def main():
     from flim_microscopy_simulator_with_causal_inference_b200 import workloads as W
     from flim_microscopy_simulator_with_causal_inference_b200.batch import Ensemble
 
-    raws = W.ensemble_replicas(args.replicas, seed=args.seed + 7919 * rank)
+    raws = rank_replicas(args.replicas, args.seed, rank)
     ens = Ensemble(raws, precision=32, photons=True, device=device)
     eng = ens.engine
     stream = torch.cuda.Stream(device=device)
@@ -230,13 +259,10 @@ def main():
         e1.record(stream)
         stream.synchronize()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), world, "cuda")
     n_mem = ens.total_membrane
-    value = n_mem * world * STEPS_PER_FRAME * args.steps / (ms / 1e3)
+    job_ps = job_particle_steps(n_mem, world, STEPS_PER_FRAME * args.steps, "cuda")
+    value = job_ps / (ms / 1e3)
     launches = eng.launches_per_step(True) * STEPS_PER_FRAME * args.steps + 2 * args.steps
     status = eng.status()
 
@@ -266,12 +292,8 @@ def main():
         st = eng.get_state(stream=stream)
         frame += 1
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = n_mem * world * STEPS_PER_FRAME * args.steps / e2e_s
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world, "cuda")
+    e2e_value = job_ps / e2e_s
     state_bytes_out = sum(v.nbytes for v in st.values())
     h2d = state_bytes_in / STEPS_PER_FRAME
     d2h = (flim_elems * 4 + state_bytes_out) / STEPS_PER_FRAME

@@ -36,7 +36,7 @@ class Ensemble:
             dps.append(dp)
             hills.append(hill)
             poff += st.N
-            coff += d.nx * d.ny
+            coff += PR.n_buckets(d)
             goff += dp.grid_cells
             hoff += hill.size
             if photons:

@@ -86,22 +86,28 @@ __device__ __forceinline__ double ln_series(double q) {
 }
 
 // Standard normal pair, Marsaglia polar method; attempt t uses counter b = t.
+// The rejection loop only draws candidates; the logarithm and square root run
+// once after it, so lanes of a warp that accept at different attempts do not
+// each run them.
 __device__ __forceinline__ U2 normal2(uint64_t seed, int64_t step, int stream, uint64_t a) {
-  U2 z;
-  for (uint32_t t = 0; t < 64; ++t) {
+  double x = 0.0, y = 0.0, q = 0.0;
+  uint32_t t = 0;
+  for (; t < 64; ++t) {
     const U2 u = uniform2(seed, step, stream, a, t);
-    const double x = __dadd_rn(__dmul_rn(2.0, u.u0), -1.0);
-    const double y = __dadd_rn(__dmul_rn(2.0, u.u1), -1.0);
-    const double q = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
-    if (q > 0.0 && q < 1.0) {
-      const double f = __dsqrt_rn(__ddiv_rn(__dmul_rn(-2.0, ln_series(q)), q));
-      z.u0 = __dmul_rn(x, f);
-      z.u1 = __dmul_rn(y, f);
-      return z;
-    }
+    x = __dadd_rn(__dmul_rn(2.0, u.u0), -1.0);
+    y = __dadd_rn(__dmul_rn(2.0, u.u1), -1.0);
+    q = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
+    if (q > 0.0 && q < 1.0) break;
   }
-  z.u0 = 0.0;
-  z.u1 = 0.0;
+  U2 z;
+  if (t == 64) {
+    z.u0 = 0.0;
+    z.u1 = 0.0;
+    return z;
+  }
+  const double f = __dsqrt_rn(__ddiv_rn(__dmul_rn(-2.0, ln_series(q)), q));
+  z.u0 = __dmul_rn(x, f);
+  z.u1 = __dmul_rn(y, f);
   return z;
 }
 

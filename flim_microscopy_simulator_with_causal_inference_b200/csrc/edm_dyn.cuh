@@ -1,17 +1,21 @@
 // edm_dyn.cuh — dynamics kernels (one BD step of DynamicsEngine.step,
 // ed_mrdt/dynamics.py:2150-2465) for all replicas of an engine.
 //
-// Layout.  Per step the particles of every replica are counting-sorted by
-// their reference cell (dynamics.py:176-196: cx = int(x/cell_sx) clamped,
-// key cx*ny + cy) into "slots"; replica r owns slots
-// [particle_offset, particle_offset + n_particles) and cells
-// [cell_offset, cell_offset + nx*ny).  Slot arrays: position (float64
-// absolute, or float32 offset inside the cell + the integer cell), the cell,
-// one flag byte (species | alive<<7) and the particle id.  Id-indexed arrays
-// (bond partner, dye, photophysical state) do not move.
+// Layout.  Every step the particles of every replica are counting-sorted into
+// "slots" by a key: the reference cell cx*ny + cy of alive particles
+// (dynamics.py:176-196: cx = int(x/cell_sx) clamped), and one extra bucket
+// (key nx*ny) holding every particle that is not alive.  Replica r owns slots
+// [particle_offset, +n_particles) and sort buckets [cell_offset, +nx*ny+1).
+// Non-alive particles never take part in a pair computation
+// (dynamics.py:680-681, 767-768, 850-851), so keeping them out of the cells
+// leaves the neighbour sweeps with alive particles only; their reference
+// cell is still stored per slot.  Slot arrays: position (float64 absolute, or
+// float32 offset inside the cell), the cell, one flag byte (species |
+// alive<<7) and the particle id.  Id-indexed arrays (bond partner, dye,
+// photophysical state) do not move.
 //
-// Order independence.  The slot order inside a cell comes from atomics and is
-// not deterministic; nothing downstream depends on it:
+// Order independence.  The slot order inside a bucket comes from atomics and
+// is not deterministic; nothing downstream depends on it:
 //  - pair forces are summed per particle in the reference's own pair order
 //    (its (j, i) pairs by ascending j, then its (i, j) pairs by neighbour-cell
 //    ordinal and descending j; WCA terms before harmonic terms), recovered
@@ -28,11 +32,13 @@
 namespace edm {
 
 constexpr int kBlock = 256;
+constexpr int kRecCap = 128;
+constexpr int kBindCap = 512;
 
 struct DevState {
   void* pos_pre;      // double2 (f64) or float2 (f32 offsets), slot order, before the move
   void* pos_post;     // same, after the move
-  int32_t* cell_pre;  // local cell of each slot, before the move
+  int32_t* cell_pre;  // reference cell of each slot, before the move
   int32_t* cell_post;
   const uint8_t* flags_old;
   uint8_t* flags;     // slot flags of the current step
@@ -40,9 +46,9 @@ struct DevState {
   int32_t* ids;       // global particle id of each slot
   int32_t* slot_of_id;
   int32_t* bond;      // id-indexed, global id or -1
-  int32_t* cell_start;   // [n_cells + 1]
+  int32_t* cell_start;   // sort-bucket starts [n_buckets + 1]
   int32_t* cell_cursor;
-  int32_t* cnt_next;     // cell counts of the post-move positions
+  int32_t* cnt_next;     // bucket counts for the next step's sort
   int32_t* grid_cnt;     // density-grid counts (snapshot of the current pass)
   int32_t* grid_delta;   // pending changes of the current pass
   const double* hill;
@@ -56,10 +62,48 @@ struct DevState {
   int32_t* bind_count;   // [R]
   int64_t* bind_key;     // [R][kBindCap]
   int32_t* bind_ab;      // [R][kBindCap][2] local ids (a = reactant A role, b = B role)
+  // catalytic contacts of the step: (enzyme slot, substrate-capable slot)
+  int2* contacts;
+  int32_t* contact_count;
+  int64_t contact_cap;
+  const int64_t* rep_first;  // [R + 1] first slot of each replica
+  int n_rep;
+  int64_t n_slots;
 };
 
-constexpr int kRecCap = 128;
-constexpr int kBindCap = 512;
+__device__ __forceinline__ int replica_of(const int64_t* __restrict__ rep_first, int R, int64_t s) {
+  int lo = 0, hi = R - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (rep_first[mid] <= s) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Particles a per-particle pass visits: species in `species_mask` and alive
+// (alive = 1) or not alive (alive = 0).
+struct Match {
+  uint32_t species_mask;
+  int alive;
+};
+__device__ __forceinline__ bool matches(uint8_t f, const Match& m) {
+  return ((m.species_mask >> fl_species(f)) & 1u) && (fl_alive(f) == (m.alive != 0));
+}
+
+// Vectorised flag sweep: 4 slots per thread; body(replica, slot) for matches.
+template <typename Body>
+__device__ __forceinline__ void sweep4(const DevState& st, const Match& m, Body body) {
+  const int64_t s0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  if (s0 >= st.n_slots) return;
+  const uchar4 f4 = *reinterpret_cast<const uchar4*>(st.flags + s0);
+  const uint8_t f[4] = {f4.x, f4.y, f4.z, f4.w};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int64_t s = s0 + k;
+    if (s < st.n_slots && matches(f[k], m)) body(replica_of(st.rep_first, st.n_rep, s), s);
+  }
+}
 
 // ---- replica geometry --------------------------------------------------------
 struct Geo {
@@ -67,10 +111,11 @@ struct Geo {
   double Lx, Ly, sx, sy, cutoff_sq;
   float sxf, syf;
   int64_t cbase, poff;
+  int grave;  // bucket of non-alive particles
   __device__ __forceinline__ explicit Geo(const EdmDynParams& p)
       : nx(p.nx), ny(p.ny), px(p.periodic_x), py(p.periodic_y), Lx(p.Lx), Ly(p.Ly),
         sx(p.cell_sx), sy(p.cell_sy), cutoff_sq(p.cutoff_sq), sxf((float)p.cell_sx),
-        syf((float)p.cell_sy), cbase(p.cell_offset), poff(p.particle_offset) {}
+        syf((float)p.cell_sy), cbase(p.cell_offset), poff(p.particle_offset), grave(p.nx * p.ny) {}
 };
 
 // Absolute position of a slot (float64).
@@ -152,6 +197,23 @@ __device__ __forceinline__ Tile tile_of(const int2* blk) {
   return t;
 }
 
+// Visit the 3x3 neighbour cells of cell c (dynamics.py:243-260): f(bucket, ordinal, dcx, dcy).
+template <typename F>
+__device__ __forceinline__ void for_neighbour_cells(const Geo& g, int c, F f) {
+  const int cx = c / g.ny, cy = c - (c / g.ny) * g.ny;
+  for (int dcx = -1; dcx <= 1; ++dcx) {
+    int ncx = cx + dcx;
+    if (g.px) ncx = ncx < 0 ? ncx + g.nx : (ncx >= g.nx ? ncx - g.nx : ncx);
+    else if (ncx < 0 || ncx >= g.nx) continue;
+    for (int dcy = -1; dcy <= 1; ++dcy) {
+      int ncy = cy + dcy;
+      if (g.py) ncy = ncy < 0 ? ncy + g.ny : (ncy >= g.ny ? ncy - g.ny : ncy);
+      else if (ncy < 0 || ncy >= g.ny) continue;
+      f(g.cbase + (int64_t)ncx * g.ny + ncy, (dcx + 1) * 3 + (dcy + 1), dcx, dcy);
+    }
+  }
+}
+
 // ---- density grids -----------------------------------------------------------
 __device__ __forceinline__ int64_t grid_cell_of(const EdmGrid& G, double x, double y) {
   const int gx = clampi((int)__ddiv_rn(x, G.sx), G.nx);
@@ -173,8 +235,22 @@ __device__ __forceinline__ double rule_factor(const EdmDynParams& p, int rule, c
   return hill_of(R, st.hill, k, st.status);
 }
 
+// Grid bookkeeping of a particle changing (species, alive) at one position.
+__device__ __forceinline__ void grid_change(const EdmDynParams& p, int32_t* delta, int sp_old, bool alive_old,
+                                            int sp_new, bool alive_new, double x, double y) {
+  if (alive_old) grid_add(p, delta, sp_old, x, y, -1);
+  if (alive_new) grid_add(p, delta, sp_new, x, y, +1);
+}
+
+// Next step's bucket counts when a particle changes bucket.
+__device__ __forceinline__ void rebucket(const DevState& st, const Geo& g, int from, int to) {
+  if (from == to) return;
+  atomicAdd(&st.cnt_next[g.cbase + from], -1);
+  atomicAdd(&st.cnt_next[g.cbase + to], 1);
+}
+
 // =============================================================================
-// Cell list: exclusive scan of the post-move cell counts, scatter into slots.
+// Sort: exclusive scan of the bucket counts, scatter into slots.
 // =============================================================================
 constexpr int kScanThreads = 512;
 constexpr int kScanItems = 8;
@@ -264,14 +340,16 @@ __global__ void __launch_bounds__(kBlock) k_scatter(const EdmDynParams* __restri
   const EdmDynParams& p = P[t.r];
   if (t.s >= p.particle_offset + p.n_particles) return;
   const int c = st.cell_post[t.s];
-  const int d = atomicAdd(&st.cell_cursor[p.cell_offset + c], 1);
+  const uint8_t f = st.flags_old[t.s];
+  const int key = fl_alive(f) ? c : p.nx * p.ny;
+  const int d = atomicAdd(&st.cell_cursor[p.cell_offset + key], 1);
   if constexpr (F64) {
     ((double2*)st.pos_pre)[d] = ((const double2*)st.pos_post)[t.s];
   } else {
     ((float2*)st.pos_pre)[d] = ((const float2*)st.pos_post)[t.s];
   }
   st.cell_pre[d] = c;
-  st.flags[d] = st.flags_old[t.s];
+  st.flags[d] = f;
   const int id = st.ids_old[t.s];
   st.ids[d] = id;
   st.slot_of_id[id] = d;
@@ -280,17 +358,11 @@ __global__ void __launch_bounds__(kBlock) k_scatter(const EdmDynParams* __restri
 // =============================================================================
 // Forces + Ermak–McCammon move (dynamics.py:440-519, 665-816, 323-406).
 // =============================================================================
-struct ForceTerm {
-  uint64_t key;
-  double fx, fy;
-};
 
 // Enumerate the pair-force terms of slot s; pass `emit(key, fx, fy)`.
 template <bool F64, typename Emit>
 __device__ __forceinline__ void for_each_force_term(const EdmDynParams& p, const Geo& g, const DevState& st,
                                                     int64_t s, int sp, int id, Emit emit) {
-  const int c = st.cell_pre[s];
-  const int cx = c / g.ny, cy = c - (c / g.ny) * g.ny;
   double xi = 0, yi = 0;
   float2 oi = make_float2(0.f, 0.f);
   if constexpr (F64) {
@@ -300,98 +372,91 @@ __device__ __forceinline__ void for_each_force_term(const EdmDynParams& p, const
   } else {
     oi = ((const float2*)st.pos_pre)[s];
   }
-  for (int dcx = -1; dcx <= 1; ++dcx) {
-    int ncx = cx + dcx;
-    if (g.px) ncx = ncx < 0 ? ncx + g.nx : (ncx >= g.nx ? ncx - g.nx : ncx);
-    else if (ncx < 0 || ncx >= g.nx) continue;
-    for (int dcy = -1; dcy <= 1; ++dcy) {
-      int ncy = cy + dcy;
-      if (g.py) ncy = ncy < 0 ? ncy + g.ny : (ncy >= g.ny ? ncy - g.ny : ncy);
-      else if (ncy < 0 || ncy >= g.ny) continue;
-      const int64_t nc = g.cbase + (int64_t)ncx * g.ny + ncy;
-      const int ordinal = (dcx + 1) * 3 + (dcy + 1);
-      const int j0 = st.cell_start[nc], j1 = st.cell_start[nc + 1];
-      for (int j = j0; j < j1; ++j) {
-        if (j == s) continue;
-        const uint8_t fj = st.flags[j];
-        if (!fl_alive(fj)) continue;
-        const int spj = fl_species(fj);
-        const double sig = p.sigma[sp * EDM_MAX_SPECIES + spj];
-        if (!(sig > 0.0)) continue;
-        // separation i - j and the pair-list cutoff test (dynamics.py:262-268)
-        double dx, dy, dsq;
-        if constexpr (F64) {
-          const double2 v = ((const double2*)st.pos_pre)[j];
-          dsq = min_image_sq(xi, yi, v.x, v.y, g, dx, dy);
-          if (!(dsq < g.cutoff_sq)) continue;
-        } else {
-          const float2 oj = ((const float2*)st.pos_pre)[j];
-          const float fdx = -(float)dcx * g.sxf + (oi.x - oj.x);
-          const float fdy = -(float)dcy * g.syf + (oi.y - oj.y);
-          const float fdsq = fdx * fdx + fdy * fdy;
-          if (!((double)fdsq < g.cutoff_sq)) continue;
-          dx = fdx;
-          dy = fdy;
-          dsq = fdsq;
-        }
-        const int idj = st.ids[j] - (int)g.poff;
-        const uint64_t order = idj < id ? (uint64_t)idj
-                                        : ((1ull << 60) | ((uint64_t)ordinal << 32) | (uint64_t)(0xFFFFFFFFu - (uint32_t)idj));
-        if (p.use_wca) {
-          const double eps = p.eps[sp * EDM_MAX_SPECIES + spj];
-          if (eps > 0.0) {
-            if constexpr (F64) {
-              const double rcut2 = sig * sig * 1.2599210498948732;
-              if (dsq < rcut2 && dsq >= 1e-30) {
-                const double inv_r2 = 1.0 / dsq;
-                const double s2 = sig * sig * inv_r2;
-                const double s6 = s2 * s2 * s2;
-                const double s12 = s6 * s6;
-                double f = 24.0 * eps * (2.0 * s12 - s6) * inv_r2;
-                const double fmax = 2400.0 * eps / (sig * sig);
-                if (f > fmax) f = fmax;
-                emit(order, f * dx, f * dy);
-              }
-            } else {
-              const float sgf = (float)sig, epf = (float)eps;
-              const float fd = (float)dsq;
-              const float rcut2 = sgf * sgf * 1.2599210498948732f;
-              if (fd < rcut2 && fd >= 1e-30f) {
-                const float inv_r2 = 1.0f / fd;
-                const float s2 = sgf * sgf * inv_r2;
-                const float s6 = s2 * s2 * s2;
-                const float s12 = s6 * s6;
-                float f = 24.0f * epf * (2.0f * s12 - s6) * inv_r2;
-                const float fmax = 2400.0f * epf / (sgf * sgf);
-                if (f > fmax) f = fmax;
-                emit(order, (double)(f * (float)dx), (double)(f * (float)dy));
-              }
+  // pairs beyond both the pair-list cutoff and every potential's range carry no force
+  const double range_sq = p.force_range_sq < g.cutoff_sq ? p.force_range_sq : g.cutoff_sq;
+  const float range_sqf = (float)range_sq * 1.0001f;
+  for_neighbour_cells(g, st.cell_pre[s], [&](int64_t nc, int ordinal, int dcx, int dcy) {
+    const int j0 = st.cell_start[nc], j1 = st.cell_start[nc + 1];
+    for (int j = j0; j < j1; ++j) {
+      if (j == s) continue;
+      double dx, dy, dsq;
+      if constexpr (F64) {
+        const double2 v = ((const double2*)st.pos_pre)[j];
+        dsq = min_image_sq(xi, yi, v.x, v.y, g, dx, dy);
+        if (!(dsq < range_sq)) continue;
+      } else {
+        const float2 oj = ((const float2*)st.pos_pre)[j];
+        const float fdx = -(float)dcx * g.sxf + (oi.x - oj.x);
+        const float fdy = -(float)dcy * g.syf + (oi.y - oj.y);
+        const float fdsq = fdx * fdx + fdy * fdy;
+        if (!(fdsq < range_sqf)) continue;
+        if (!((double)fdsq < g.cutoff_sq)) continue;
+        dx = fdx;
+        dy = fdy;
+        dsq = fdsq;
+      }
+      const uint8_t fj = st.flags[j];
+      if (!fl_alive(fj)) continue;
+      const int spj = fl_species(fj);
+      const double sig = p.sigma[sp * EDM_MAX_SPECIES + spj];
+      if (!(sig > 0.0)) continue;
+      const int idj = st.ids[j] - (int)g.poff;
+      const uint64_t order = idj < id ? (uint64_t)idj
+                                      : ((1ull << 60) | ((uint64_t)ordinal << 32) | (uint64_t)(0xFFFFFFFFu - (uint32_t)idj));
+      if (p.use_wca) {
+        const double eps = p.eps[sp * EDM_MAX_SPECIES + spj];
+        if (eps > 0.0) {
+          if constexpr (F64) {
+            const double rcut2 = sig * sig * 1.2599210498948732;
+            if (dsq < rcut2 && dsq >= 1e-30) {
+              const double inv_r2 = 1.0 / dsq;
+              const double s2 = sig * sig * inv_r2;
+              const double s6 = s2 * s2 * s2;
+              const double s12 = s6 * s6;
+              double f = 24.0 * eps * (2.0 * s12 - s6) * inv_r2;
+              const double fmax = 2400.0 * eps / (sig * sig);
+              if (f > fmax) f = fmax;
+              emit(order, f * dx, f * dy);
+            }
+          } else {
+            const float sgf = (float)sig, epf = (float)eps;
+            const float fd = (float)dsq;
+            const float rcut2 = sgf * sgf * 1.2599210498948732f;
+            if (fd < rcut2 && fd >= 1e-30f) {
+              const float inv_r2 = 1.0f / fd;
+              const float s2 = sgf * sgf * inv_r2;
+              const float s6 = s2 * s2 * s2;
+              const float s12 = s6 * s6;
+              float f = 24.0f * epf * (2.0f * s12 - s6) * inv_r2;
+              const float fmax = 2400.0f * epf / (sgf * sgf);
+              if (f > fmax) f = fmax;
+              emit(order, (double)(f * (float)dx), (double)(f * (float)dy));
             }
           }
         }
-        if (p.use_harmonic) {
-          const double k = p.kharm[sp * EDM_MAX_SPECIES + spj];
-          if (k > 0.0) {
-            if constexpr (F64) {
-              const double s2 = sig * sig;
-              if (dsq < s2 && dsq >= 1e-30) {
-                const double r = sqrt(dsq);
-                const double f = k * (sig - r) / r;
-                emit(order | (1ull << 62), f * dx, f * dy);
-              }
-            } else {
-              const float sgf = (float)sig, kf = (float)k, fd = (float)dsq;
-              if (fd < sgf * sgf && fd >= 1e-30f) {
-                const float r = sqrtf(fd);
-                const float f = kf * (sgf - r) / r;
-                emit(order | (1ull << 62), (double)(f * (float)dx), (double)(f * (float)dy));
-              }
+      }
+      if (p.use_harmonic) {
+        const double k = p.kharm[sp * EDM_MAX_SPECIES + spj];
+        if (k > 0.0) {
+          if constexpr (F64) {
+            const double s2 = sig * sig;
+            if (dsq < s2 && dsq >= 1e-30) {
+              const double r = sqrt(dsq);
+              const double f = k * (sig - r) / r;
+              emit(order | (1ull << 62), f * dx, f * dy);
+            }
+          } else {
+            const float sgf = (float)sig, kf = (float)k, fd = (float)dsq;
+            if (fd < sgf * sgf && fd >= 1e-30f) {
+              const float r = sqrtf(fd);
+              const float f = kf * (sgf - r) / r;
+              emit(order | (1ull << 62), (double)(f * (float)dx), (double)(f * (float)dy));
             }
           }
         }
       }
     }
-  }
+  });
 }
 
 // D(x) and grad D at an absolute position (dynamics.py:440-519; sine-x field).
@@ -462,7 +527,7 @@ __global__ void __launch_bounds__(kBlock) k_move(const EdmDynParams* __restrict_
       ((float2*)st.pos_post)[s] = ((const float2*)st.pos_pre)[s];
     }
     st.cell_post[s] = c;
-    atomicAdd(&st.cnt_next[g.cbase + c], 1);
+    atomicAdd(&st.cnt_next[g.cbase + g.grave], 1);
     return;
   }
   const int sp = fl_species(f);
@@ -587,59 +652,80 @@ __global__ void __launch_bounds__(kBlock) k_move(const EdmDynParams* __restrict_
 // Reactions.
 // =============================================================================
 
-// Grid bookkeeping of a particle changing (species, alive) at one position.
-__device__ __forceinline__ void grid_change(const EdmDynParams& p, int32_t* delta, int sp_old, bool alive_old,
-                                            int sp_new, bool alive_new, double x, double y) {
-  if (alive_old) grid_add(p, delta, sp_old, x, y, -1);
-  if (alive_new) grid_add(p, delta, sp_new, x, y, +1);
-}
+// Catalytic contacts (pairs of the reference's pre-move pair list, dynamics.py
+// :219-278, in post-move contact): enzyme-capable alive particles sweep their
+// neighbour cells once per step, after the binding passes.  During the
+// catalytic passes enzymes keep their species and nobody moves or dies, so
+// every pass of the step reads this list instead of sweeping again.
+constexpr int kContactSmem = 2048;
 
-// Catalytic pass c (dynamics.py:825-983): the set of substrates with at least
-// one accepted (enzyme, substrate) candidate pair is converted.
 template <bool F64>
-__global__ void __launch_bounds__(kBlock) k_catalytic(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk,
-                                                      DevState st, int cidx) {
-  const Tile t = tile_of(blk);
-  const EdmDynParams& p = P[t.r];
-  const int64_t s = t.s;
-  if (s >= p.particle_offset + p.n_particles) return;
-  const EdmCat& C = p.cat[cidx];
-  const uint8_t f = st.flags[s];
-  if (!fl_alive(f) || fl_species(f) != C.enzyme) return;
-  const Geo g(p);
-  const int64_t step = *st.d_step;
-  const int ide = st.ids[s] - (int)g.poff;
-  const int c = st.cell_pre[s];
-  const int cx = c / g.ny, cy = c - (c / g.ny) * g.ny;
-  for (int dcx = -1; dcx <= 1; ++dcx) {
-    int ncx = cx + dcx;
-    if (g.px) ncx = ncx < 0 ? ncx + g.nx : (ncx >= g.nx ? ncx - g.nx : ncx);
-    else if (ncx < 0 || ncx >= g.nx) continue;
-    for (int dcy = -1; dcy <= 1; ++dcy) {
-      int ncy = cy + dcy;
-      if (g.py) ncy = ncy < 0 ? ncy + g.ny : (ncy >= g.ny ? ncy - g.ny : ncy);
-      else if (ncy < 0 || ncy >= g.ny) continue;
-      const int64_t nc = g.cbase + (int64_t)ncx * g.ny + ncy;
+__global__ void __launch_bounds__(kBlock) k_contacts(const EdmDynParams* __restrict__ P, DevState st, Match m,
+                                                     uint32_t partner_mask, double contact_sq) {
+  __shared__ int2 buf[kContactSmem];
+  __shared__ int nbuf, base;
+  if (threadIdx.x == 0) nbuf = 0;
+  __syncthreads();
+  sweep4(st, m, [&](int r, int64_t s) {
+    const EdmDynParams& p = P[r];
+    const Geo g(p);
+    for_neighbour_cells(g, st.cell_pre[s], [&](int64_t nc, int, int, int) {
       const int j0 = st.cell_start[nc], j1 = st.cell_start[nc + 1];
       for (int j = j0; j < j1; ++j) {
         if (j == s) continue;
         const uint8_t fj = st.flags[j];
-        if (!fl_alive(fj) || fl_species(fj) != C.substrate) continue;
-        if (!(sep_sq<F64>(st.pos_pre, st.cell_pre, s, j, g) < g.cutoff_sq)) continue;   // pair list
-        if (sep_sq<F64>(st.pos_post, st.cell_post, s, j, g) > C.contact_sq) continue;  // contact
-        const int idj = st.ids[j] - (int)g.poff;
-        const uint32_t lo = ide < idj ? ide : idj, hi = ide < idj ? idj : ide;
-        const double u = uniform1(p.seed, step, EDM_S_CAT + cidx, lo, hi);
-        double xs, ys;
-        abs_pos<F64>(st.pos_post, st.cell_post, j, g, xs, ys);
-        double peff = C.prob;
-        if (C.rule >= 0) peff = C.prob * rule_factor(p, C.rule, st, xs, ys);
-        if (u < peff) {
-          if (cas_u8(&st.flags[j], fj, fl_make(C.product, true))) {
-            atomic_add_i64(&st.counters[(int64_t)t.r * EDM_NCOUNTERS + EDM_C_CATALYTIC], 1);
-            grid_change(p, st.grid_delta, C.substrate, true, C.product, true, xs, ys);
-          }
+        if (!fl_alive(fj) || !((partner_mask >> fl_species(fj)) & 1u)) continue;
+        if (!(sep_sq<F64>(st.pos_pre, st.cell_pre, s, j, g) < g.cutoff_sq)) continue;
+        if (sep_sq<F64>(st.pos_post, st.cell_post, s, j, g) > contact_sq) continue;
+        const int k = atomicAdd(&nbuf, 1);
+        if (k < kContactSmem) {
+          buf[k] = make_int2((int)s, j);
+        } else {  // shared buffer full: append directly
+          const int q = atomicAdd(st.contact_count, 1);
+          if (q < st.contact_cap) st.contacts[q] = make_int2((int)s, j);
+          else set_status(st.status, EDM_STATUS_BIND_CAP);
         }
+      }
+    });
+  });
+  __syncthreads();
+  const int n = nbuf < kContactSmem ? nbuf : kContactSmem;
+  if (threadIdx.x == 0) base = n > 0 ? atomicAdd(st.contact_count, n) : 0;
+  __syncthreads();
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    const int64_t q = (int64_t)base + k;
+    if (q < st.contact_cap) st.contacts[q] = buf[k];
+    else set_status(st.status, EDM_STATUS_BIND_CAP);
+  }
+}
+
+// Catalytic pass c (dynamics.py:825-983) over the step's contacts: the set of
+// substrates with at least one accepted (enzyme, substrate) pair converts.
+template <bool F64>
+__global__ void __launch_bounds__(kBlock) k_catalytic(const EdmDynParams* __restrict__ P, DevState st, int cidx) {
+  const int n = *st.contact_count;
+  const int lim = (int64_t)n < st.contact_cap ? n : (int)st.contact_cap;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < lim; q += (int64_t)gridDim.x * blockDim.x) {
+    const int2 es = st.contacts[q];
+    const uint8_t fe = st.flags[es.x];
+    const uint8_t fs = st.flags[es.y];
+    const int r = replica_of(st.rep_first, st.n_rep, es.x);
+    const EdmDynParams& p = P[r];
+    const EdmCat& C = p.cat[cidx];
+    if (!fl_alive(fe) || !fl_alive(fs) || fl_species(fe) != C.enzyme || fl_species(fs) != C.substrate) continue;
+    const Geo g(p);
+    if (sep_sq<F64>(st.pos_post, st.cell_post, es.x, es.y, g) > C.contact_sq) continue;
+    const int ide = st.ids[es.x] - (int)g.poff, ids = st.ids[es.y] - (int)g.poff;
+    const uint32_t lo = ide < ids ? ide : ids, hi = ide < ids ? ids : ide;
+    const double u = uniform1(p.seed, *st.d_step, EDM_S_CAT + cidx, lo, hi);
+    double xs, ys;
+    abs_pos<F64>(st.pos_post, st.cell_post, es.y, g, xs, ys);
+    double peff = C.prob;
+    if (C.rule >= 0) peff = C.prob * rule_factor(p, C.rule, st, xs, ys);
+    if (u < peff) {
+      if (cas_u8(&st.flags[es.y], fs, fl_make(C.product, true))) {
+        atomic_add_i64(&st.counters[(int64_t)r * EDM_NCOUNTERS + EDM_C_CATALYTIC], 1);
+        grid_change(p, st.grid_delta, C.substrate, true, C.product, true, xs, ys);
       }
     }
   }
@@ -648,36 +734,33 @@ __global__ void __launch_bounds__(kBlock) k_catalytic(const EdmDynParams* __rest
 // Recruitment candidates of exchange e (dynamics.py:1229-1458): dormant
 // particles of the species whose keyed draw accepts at the keyed position.
 template <bool F64>
-__global__ void __launch_bounds__(kBlock) k_recruit_candidates(const EdmDynParams* __restrict__ P,
-                                                               const int2* __restrict__ blk, DevState st, int e) {
-  const Tile t = tile_of(blk);
-  const EdmDynParams& p = P[t.r];
-  const int64_t s = t.s;
-  if (s >= p.particle_offset + p.n_particles) return;
-  const EdmExch& X = p.exch[e];
-  const uint8_t f = st.flags[s];
-  if (fl_alive(f) || fl_species(f) != X.species) return;
-  const int id = st.ids[s] - (int)p.particle_offset;
-  const int64_t step = *st.d_step;
-  const double ua = uniform1(p.seed, step, EDM_S_EX_ACCEPT + 4 * e, (uint64_t)id, 0);
-  const U2 up = uniform2(p.seed, step, EDM_S_EX_POS + 4 * e, (uint64_t)id, 0);
-  const double cx = up.u0 * p.Lx, cy = up.u1 * p.Ly;
-  double peff = X.prob_on;
-  if (X.rule_on >= 0 && X.rule_on2 >= 0) {
-    peff = X.prob_on * rule_factor(p, X.rule_on, st, cx, cy) * rule_factor(p, X.rule_on2, st, cx, cy);
-  } else if (X.rule_on >= 0) {
-    peff = X.prob_on * rule_factor(p, X.rule_on, st, cx, cy);
-  }
-  if (ua < peff) {
-    const int k = atomicAdd(&st.rec_count[t.r], 1);
-    if (k < kRecCap) {
-      st.rec_id[(int64_t)t.r * kRecCap + k] = id;
-      st.rec_xy[((int64_t)t.r * kRecCap + k) * 2] = cx;
-      st.rec_xy[((int64_t)t.r * kRecCap + k) * 2 + 1] = cy;
-    } else {
-      set_status(st.status, EDM_STATUS_RECRUIT_CAP);
+__global__ void __launch_bounds__(kBlock) k_recruit_candidates(const EdmDynParams* __restrict__ P, DevState st,
+                                                               Match m, int e) {
+  sweep4(st, m, [&](int r, int64_t s) {
+    const EdmDynParams& p = P[r];
+    const EdmExch& X = p.exch[e];
+    const int id = st.ids[s] - (int)p.particle_offset;
+    const int64_t step = *st.d_step;
+    const double ua = uniform1(p.seed, step, EDM_S_EX_ACCEPT + 4 * e, (uint64_t)id, 0);
+    const U2 up = uniform2(p.seed, step, EDM_S_EX_POS + 4 * e, (uint64_t)id, 0);
+    const double cx = up.u0 * p.Lx, cy = up.u1 * p.Ly;
+    double peff = X.prob_on;
+    if (X.rule_on >= 0 && X.rule_on2 >= 0) {
+      peff = X.prob_on * rule_factor(p, X.rule_on, st, cx, cy) * rule_factor(p, X.rule_on2, st, cx, cy);
+    } else if (X.rule_on >= 0) {
+      peff = X.prob_on * rule_factor(p, X.rule_on, st, cx, cy);
     }
-  }
+    if (ua < peff) {
+      const int k = atomicAdd(&st.rec_count[r], 1);
+      if (k < kRecCap) {
+        st.rec_id[(int64_t)r * kRecCap + k] = id;
+        st.rec_xy[((int64_t)r * kRecCap + k) * 2] = cx;
+        st.rec_xy[((int64_t)r * kRecCap + k) * 2 + 1] = cy;
+      } else {
+        set_status(st.status, EDM_STATUS_RECRUIT_CAP);
+      }
+    }
+  });
 }
 
 // Apply the first max_recruits accepted candidates in particle order.
@@ -712,7 +795,6 @@ __global__ void k_recruit_apply(const EdmDynParams* __restrict__ P, int n_rep, D
   for (int a = 0; a < take; ++a) {
     const int64_t slot = st.slot_of_id[g.poff + ids[a]];
     const double x = xy[2 * a], y = xy[2 * a + 1];
-    const int oldc = st.cell_post[slot];
     const int cxn = cell_index(x, g.sx, g.nx), cyn = cell_index(y, g.sy, g.ny);
     const int newc = cxn * g.ny + cyn;
     if constexpr (F64) {
@@ -721,8 +803,7 @@ __global__ void k_recruit_apply(const EdmDynParams* __restrict__ P, int n_rep, D
       ((float2*)st.pos_post)[slot] = make_float2((float)(x - (double)cxn * g.sx), (float)(y - (double)cyn * g.sy));
     }
     st.cell_post[slot] = newc;
-    atomicAdd(&st.cnt_next[g.cbase + oldc], -1);
-    atomicAdd(&st.cnt_next[g.cbase + newc], 1);
+    rebucket(st, g, g.grave, newc);
     st.flags[slot] = fl_make(X.species, true);
     grid_add(p, st.grid_delta, X.species, x, y, 1);
   }
@@ -731,87 +812,62 @@ __global__ void k_recruit_apply(const EdmDynParams* __restrict__ P, int n_rep, D
 
 // Detachment of exchange e (dynamics.py:1461-1555).
 template <bool F64>
-__global__ void __launch_bounds__(kBlock) k_detach(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk,
-                                                   DevState st, int e) {
-  const Tile t = tile_of(blk);
-  const EdmDynParams& p = P[t.r];
-  const int64_t s = t.s;
-  if (s >= p.particle_offset + p.n_particles) return;
-  const EdmExch& X = p.exch[e];
-  const uint8_t f = st.flags[s];
-  if (!fl_alive(f) || fl_species(f) != X.species) return;
-  const Geo g(p);
-  const int id = st.ids[s] - (int)g.poff;
-  const int64_t step = *st.d_step;
-  double x, y;
-  abs_pos<F64>(st.pos_post, st.cell_post, s, g, x, y);
-  double peff = X.prob_off;
-  if (X.rule_off >= 0) peff = X.prob_off * rule_factor(p, X.rule_off, st, x, y);
-  const double u = uniform1(p.seed, step, EDM_S_EX_DETACH + 4 * e, (uint64_t)id, 0);
-  if (u < peff) {
-    st.flags[s] = fl_make(X.species, false);
-    atomic_add_i64(&st.counters[(int64_t)t.r * EDM_NCOUNTERS + EDM_C_DETACHED], 1);
-    grid_add(p, st.grid_delta, X.species, x, y, -1);
-  }
+__global__ void __launch_bounds__(kBlock) k_detach(const EdmDynParams* __restrict__ P, DevState st, Match m, int e) {
+  sweep4(st, m, [&](int r, int64_t s) {
+    const EdmDynParams& p = P[r];
+    const EdmExch& X = p.exch[e];
+    const Geo g(p);
+    const int id = st.ids[s] - (int)g.poff;
+    double x, y;
+    abs_pos<F64>(st.pos_post, st.cell_post, s, g, x, y);
+    double peff = X.prob_off;
+    if (X.rule_off >= 0) peff = X.prob_off * rule_factor(p, X.rule_off, st, x, y);
+    const double u = uniform1(p.seed, *st.d_step, EDM_S_EX_DETACH + 4 * e, (uint64_t)id, 0);
+    if (u < peff) {
+      st.flags[s] = fl_make(X.species, false);
+      rebucket(st, g, st.cell_post[s], g.grave);
+      atomic_add_i64(&st.counters[(int64_t)r * EDM_NCOUNTERS + EDM_C_DETACHED], 1);
+      grid_add(p, st.grid_delta, X.species, x, y, -1);
+    }
+  });
 }
 
 // Unimolecular conversion v (dynamics.py:1565-1657).
 template <bool F64>
-__global__ void __launch_bounds__(kBlock) k_convert(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk,
-                                                    DevState st, int v) {
-  const Tile t = tile_of(blk);
-  const EdmDynParams& p = P[t.r];
-  const int64_t s = t.s;
-  if (s >= p.particle_offset + p.n_particles) return;
-  const EdmConv& V = p.conv[v];
-  const uint8_t f = st.flags[s];
-  if (!fl_alive(f) || fl_species(f) != V.from) return;
-  const Geo g(p);
-  const int id = st.ids[s] - (int)g.poff;
-  const int64_t step = *st.d_step;
-  double x, y;
-  abs_pos<F64>(st.pos_post, st.cell_post, s, g, x, y);
-  double peff = V.prob;
-  if (V.rule >= 0) peff = V.prob * rule_factor(p, V.rule, st, x, y);
-  const double u = uniform1(p.seed, step, EDM_S_CONV + v, (uint64_t)id, 0);
-  if (u < peff) {
-    st.flags[s] = fl_make(V.to, true);
-    atomic_add_i64(&st.counters[(int64_t)t.r * EDM_NCOUNTERS + EDM_C_CONVERTED], 1);
-    grid_change(p, st.grid_delta, V.from, true, V.to, true, x, y);
-  }
+__global__ void __launch_bounds__(kBlock) k_convert(const EdmDynParams* __restrict__ P, DevState st, Match m, int v) {
+  sweep4(st, m, [&](int r, int64_t s) {
+    const EdmDynParams& p = P[r];
+    const EdmConv& V = p.conv[v];
+    const Geo g(p);
+    const int id = st.ids[s] - (int)g.poff;
+    double x, y;
+    abs_pos<F64>(st.pos_post, st.cell_post, s, g, x, y);
+    double peff = V.prob;
+    if (V.rule >= 0) peff = V.prob * rule_factor(p, V.rule, st, x, y);
+    const double u = uniform1(p.seed, *st.d_step, EDM_S_CONV + v, (uint64_t)id, 0);
+    if (u < peff) {
+      st.flags[s] = fl_make(V.to, true);
+      atomic_add_i64(&st.counters[(int64_t)r * EDM_NCOUNTERS + EDM_C_CONVERTED], 1);
+      grid_change(p, st.grid_delta, V.from, true, V.to, true, x, y);
+    }
+  });
 }
 
 // Binding candidates of reaction b (dynamics.py:528-606): pairs (i < j)
 // passing every test of the pass-start state, keyed by the reference's pair
 // order (i, neighbour-cell ordinal, descending j).
 template <bool F64>
-__global__ void __launch_bounds__(kBlock) k_bind_candidates(const EdmDynParams* __restrict__ P,
-                                                            const int2* __restrict__ blk, DevState st, int b) {
-  const Tile t = tile_of(blk);
-  const EdmDynParams& p = P[t.r];
-  const int64_t s = t.s;
-  if (s >= p.particle_offset + p.n_particles) return;
-  const EdmBind& B = p.bind[b];
-  const uint8_t f = st.flags[s];
-  if (!fl_alive(f)) return;
-  const int spi = fl_species(f);
-  if (spi != B.ra && spi != B.rb) return;
-  const Geo g(p);
-  const int id = st.ids[s] - (int)g.poff;
-  if (st.bond[g.poff + id] >= 0) return;
-  const int64_t step = *st.d_step;
-  const int c = st.cell_pre[s];
-  const int cx = c / g.ny, cy = c - (c / g.ny) * g.ny;
-  for (int dcx = -1; dcx <= 1; ++dcx) {
-    int ncx = cx + dcx;
-    if (g.px) ncx = ncx < 0 ? ncx + g.nx : (ncx >= g.nx ? ncx - g.nx : ncx);
-    else if (ncx < 0 || ncx >= g.nx) continue;
-    for (int dcy = -1; dcy <= 1; ++dcy) {
-      int ncy = cy + dcy;
-      if (g.py) ncy = ncy < 0 ? ncy + g.ny : (ncy >= g.ny ? ncy - g.ny : ncy);
-      else if (ncy < 0 || ncy >= g.ny) continue;
-      const int64_t nc = g.cbase + (int64_t)ncx * g.ny + ncy;
-      const int ordinal = (dcx + 1) * 3 + (dcy + 1);
+__global__ void __launch_bounds__(kBlock) k_bind_candidates(const EdmDynParams* __restrict__ P, DevState st,
+                                                            Match m, int b) {
+  sweep4(st, m, [&](int r, int64_t s) {
+    const EdmDynParams& p = P[r];
+    const EdmBind& B = p.bind[b];
+    const int spi = fl_species(st.flags[s]);
+    const Geo g(p);
+    const int id = st.ids[s] - (int)g.poff;
+    if (st.bond[g.poff + id] >= 0) return;
+    const int64_t step = *st.d_step;
+    for_neighbour_cells(g, st.cell_pre[s], [&](int64_t nc, int ordinal, int, int) {
       const int j0 = st.cell_start[nc], j1 = st.cell_start[nc + 1];
       for (int j = j0; j < j1; ++j) {
         const int idj = st.ids[j] - (int)g.poff;
@@ -821,25 +877,31 @@ __global__ void __launch_bounds__(kBlock) k_bind_candidates(const EdmDynParams* 
         if (st.bond[g.poff + idj] >= 0) continue;
         const int spj = fl_species(fj);
         int a, bb;
-        if (spi == B.ra && spj == B.rb) { a = id; bb = idj; }
-        else if (spi == B.rb && spj == B.ra) { a = idj; bb = id; }
-        else continue;
+        if (spi == B.ra && spj == B.rb) {
+          a = id;
+          bb = idj;
+        } else if (spi == B.rb && spj == B.ra) {
+          a = idj;
+          bb = id;
+        } else {
+          continue;
+        }
         if (!(sep_sq<F64>(st.pos_pre, st.cell_pre, s, j, g) < g.cutoff_sq)) continue;
         if (sep_sq<F64>(st.pos_post, st.cell_post, s, j, g) > B.contact_sq) continue;
         const double u = uniform1(p.seed, step, EDM_S_BIND + 2 * b, (uint64_t)id, (uint64_t)idj);
         if (!(u < B.prob_bind)) continue;
-        const int k = atomicAdd(&st.bind_count[t.r], 1);
+        const int k = atomicAdd(&st.bind_count[r], 1);
         if (k < kBindCap) {
-          st.bind_key[(int64_t)t.r * kBindCap + k] =
+          st.bind_key[(int64_t)r * kBindCap + k] =
               ((int64_t)id << 36) | ((int64_t)ordinal << 32) | (int64_t)(0xFFFFFFFFu - (uint32_t)idj);
-          st.bind_ab[((int64_t)t.r * kBindCap + k) * 2] = a;
-          st.bind_ab[((int64_t)t.r * kBindCap + k) * 2 + 1] = bb;
+          st.bind_ab[((int64_t)r * kBindCap + k) * 2] = a;
+          st.bind_ab[((int64_t)r * kBindCap + k) * 2 + 1] = bb;
         } else {
           set_status(st.status, EDM_STATUS_BIND_CAP);
         }
       }
-    }
-  }
+    });
+  });
 }
 
 // Sequential greedy application in pair order, re-checking the live state.
@@ -883,6 +945,7 @@ __global__ void k_bind_apply(const EdmDynParams* __restrict__ P, int n_rep, DevS
     abs_pos<F64>(st.pos_post, st.cell_post, sb, g, xb, yb);
     st.flags[sa] = fl_make(B.product, true);
     st.flags[sb] = fl_make(B.rb, false);
+    rebucket(st, g, st.cell_post[sb], g.grave);
     st.bond[g.poff + a] = (int32_t)(g.poff + bb);
     st.bond[g.poff + bb] = (int32_t)(g.poff + a);
     grid_change(p, st.grid_delta, B.ra, true, B.product, true, xa, ya);
@@ -894,43 +957,37 @@ __global__ void k_bind_apply(const EdmDynParams* __restrict__ P, int n_rep, DevS
 
 // Dissociation of reaction b (dynamics.py:609-654).
 template <bool F64>
-__global__ void __launch_bounds__(kBlock) k_dissociate(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk,
-                                                       DevState st, int b) {
-  const Tile t = tile_of(blk);
-  const EdmDynParams& p = P[t.r];
-  const int64_t s = t.s;
-  if (s >= p.particle_offset + p.n_particles) return;
-  const EdmBind& B = p.bind[b];
-  const uint8_t f = st.flags[s];
-  if (!fl_alive(f) || fl_species(f) != B.product) return;
-  const Geo g(p);
-  const int id = st.ids[s] - (int)g.poff;
-  const int partner = st.bond[g.poff + id];
-  if (partner < 0) return;
-  const int64_t step = *st.d_step;
-  const double u = uniform1(p.seed, step, EDM_S_DISSOC + 2 * b, (uint64_t)id, 0);
-  if (!(u < B.prob_dissoc)) return;
-  const int64_t sj = st.slot_of_id[partner];
-  double x, y, xj, yj;
-  abs_pos<F64>(st.pos_post, st.cell_post, s, g, x, y);
-  abs_pos<F64>(st.pos_post, st.cell_post, sj, g, xj, yj);
-  const uint8_t fj = st.flags[sj];
-  st.flags[s] = fl_make(B.ra, true);
-  st.flags[sj] = fl_make(B.rb, true);
-  const int oldc = st.cell_post[sj], newc = st.cell_post[s];
-  if constexpr (F64) {
-    ((double2*)st.pos_post)[sj] = ((const double2*)st.pos_post)[s];
-  } else {
-    ((float2*)st.pos_post)[sj] = ((const float2*)st.pos_post)[s];
-  }
-  st.cell_post[sj] = newc;
-  atomicAdd(&st.cnt_next[g.cbase + oldc], -1);
-  atomicAdd(&st.cnt_next[g.cbase + newc], 1);
-  st.bond[g.poff + id] = -1;
-  st.bond[partner] = -1;
-  grid_change(p, st.grid_delta, B.product, true, B.ra, true, x, y);
-  grid_change(p, st.grid_delta, fl_species(fj), fl_alive(fj), B.rb, true, x, y);
-  atomic_add_i64(&st.counters[(int64_t)t.r * EDM_NCOUNTERS + EDM_C_DISSOC], 1);
+__global__ void __launch_bounds__(kBlock) k_dissociate(const EdmDynParams* __restrict__ P, DevState st, Match m,
+                                                       int b) {
+  sweep4(st, m, [&](int r, int64_t s) {
+    const EdmDynParams& p = P[r];
+    const EdmBind& B = p.bind[b];
+    const Geo g(p);
+    const int id = st.ids[s] - (int)g.poff;
+    const int partner = st.bond[g.poff + id];
+    if (partner < 0) return;
+    const double u = uniform1(p.seed, *st.d_step, EDM_S_DISSOC + 2 * b, (uint64_t)id, 0);
+    if (!(u < B.prob_dissoc)) return;
+    const int64_t sj = st.slot_of_id[partner];
+    double x, y;
+    abs_pos<F64>(st.pos_post, st.cell_post, s, g, x, y);
+    const uint8_t fj = st.flags[sj];
+    st.flags[s] = fl_make(B.ra, true);
+    st.flags[sj] = fl_make(B.rb, true);
+    const int newc = st.cell_post[s];
+    if constexpr (F64) {
+      ((double2*)st.pos_post)[sj] = ((const double2*)st.pos_post)[s];
+    } else {
+      ((float2*)st.pos_post)[sj] = ((const float2*)st.pos_post)[s];
+    }
+    rebucket(st, g, fl_alive(fj) ? st.cell_post[sj] : g.grave, newc);
+    st.cell_post[sj] = newc;
+    st.bond[g.poff + id] = -1;
+    st.bond[partner] = -1;
+    grid_change(p, st.grid_delta, B.product, true, B.ra, true, x, y);
+    grid_change(p, st.grid_delta, fl_species(fj), fl_alive(fj), B.rb, true, x, y);
+    atomic_add_i64(&st.counters[(int64_t)r * EDM_NCOUNTERS + EDM_C_DISSOC], 1);
+  });
 }
 
 // grid_cnt += grid_delta; grid_delta = 0

@@ -33,10 +33,11 @@ int fail(int code, const std::string& msg) {
     if (_e != cudaSuccess) return fail(EDM_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
   } while (0)
 
-enum PassKind { P_BIND_CAND, P_BIND_APPLY, P_DISSOC, P_CAT, P_REC_CAND, P_REC_APPLY, P_DETACH, P_CONV, P_MERGE };
+enum PassKind { P_BIND_CAND, P_BIND_APPLY, P_DISSOC, P_CONTACTS, P_CAT, P_REC_CAND, P_REC_APPLY, P_DETACH, P_CONV, P_MERGE };
 struct Pass {
   PassKind kind;
   int index;
+  Match match;  // particles a per-particle pass visits
 };
 
 template <typename T>
@@ -106,6 +107,12 @@ struct EdmEngine {
   uint8_t *st_alive = nullptr, *st_bl = nullptr;
   int8_t* st_ctmc = nullptr;
   std::vector<Pass> passes;
+  int2* contacts = nullptr;
+  int32_t* contact_count = nullptr;
+  int64_t contact_cap = 0;
+  uint32_t enzyme_mask = 0, partner_mask = 0;
+  double contact_sq_max = 0.0;
+  int64_t* rep_first = nullptr;
   std::vector<int32_t> emit_host;  // emitter list last uploaded
   std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;
   std::vector<void*> allocs;
@@ -137,6 +144,12 @@ struct EdmEngine {
     s.bind_count = bind_count;
     s.bind_key = bind_key;
     s.bind_ab = bind_ab;
+    s.contacts = contacts;
+    s.contact_count = contact_count;
+    s.contact_cap = contact_cap;
+    s.rep_first = rep_first;
+    s.n_rep = R;
+    s.n_slots = N;
     return s;
   }
 
@@ -170,7 +183,10 @@ struct EdmEngine {
     return rc;
   }
 
-  void build_schedule() {
+  // Host schedule of the reaction passes (reference order, dynamics.py:2205-2465)
+  // and the grid merges they need.  Per-particle passes read the current flags,
+  // so a pass visits exactly the particles that hold its species when it runs.
+  int build_schedule() {
     const EdmDynParams& p = hdp[0];
     std::vector<bool> dirty(EDM_MAX_GRIDS, false);
     auto sensors_of = [&](std::vector<int> species) {
@@ -180,12 +196,20 @@ struct EdmEngine {
           if (p.grid[g].sensor == s) gs.push_back(g);
       return gs;
     };
+    auto match = [](std::vector<int> species, int alive) {
+      Match m;
+      m.species_mask = 0;
+      for (int s : species) m.species_mask |= 1u << s;
+      m.alive = alive;
+      return m;
+    };
+    const Match none = match({}, 1);
     auto reads = [&](std::vector<int> rules) {
       bool need = false;
       for (int r : rules)
         if (r >= 0 && dirty[p.rule[r].grid]) need = true;
       if (need) {
-        passes.push_back({P_MERGE, 0});
+        passes.push_back({P_MERGE, 0, none});
         std::fill(dirty.begin(), dirty.end(), false);
       }
     };
@@ -193,30 +217,48 @@ struct EdmEngine {
       for (int g : sensors_of(species)) dirty[g] = true;
     };
     for (int b = 0; b < p.n_bind; ++b) {
-      passes.push_back({P_BIND_CAND, b});
-      passes.push_back({P_BIND_APPLY, b});
-      writes({p.bind[b].ra, p.bind[b].rb, p.bind[b].product});
-      passes.push_back({P_DISSOC, b});
+      const EdmBind& B = p.bind[b];
+      passes.push_back({P_BIND_CAND, b, match({B.ra, B.rb}, 1)});
+      passes.push_back({P_BIND_APPLY, b, none});
+      passes.push_back({P_DISSOC, b, match({B.product}, 1)});
+      writes({B.ra, B.rb, B.product});
+    }
+    if (p.n_cat > 0) {
+      enzyme_mask = partner_mask = 0;
+      contact_sq_max = 0.0;
+      for (int c = 0; c < p.n_cat; ++c) {
+        enzyme_mask |= 1u << p.cat[c].enzyme;
+        partner_mask |= (1u << p.cat[c].substrate) | (1u << p.cat[c].product);
+      }
+      for (int r = 0; r < R; ++r)
+        for (int c = 0; c < hdp[r].n_cat; ++c)
+          if (hdp[r].cat[c].contact_sq > contact_sq_max) contact_sq_max = hdp[r].cat[c].contact_sq;
+      if (enzyme_mask & partner_mask) return fail(EDM_EUNSUP, "an enzyme species is also a catalytic substrate/product");
+      Match m;
+      m.species_mask = enzyme_mask;
+      m.alive = 1;
+      passes.push_back({P_CONTACTS, 0, m});
     }
     for (int c = 0; c < p.n_cat; ++c) {
       reads({p.cat[c].rule});
-      passes.push_back({P_CAT, c});
+      passes.push_back({P_CAT, c, none});
       writes({p.cat[c].substrate, p.cat[c].product});
     }
     for (int e = 0; e < p.n_exch; ++e) {
       reads({p.exch[e].rule_on, p.exch[e].rule_on2});
-      passes.push_back({P_REC_CAND, e});
-      passes.push_back({P_REC_APPLY, e});
+      passes.push_back({P_REC_CAND, e, match({p.exch[e].species}, 0)});
+      passes.push_back({P_REC_APPLY, e, none});
       writes({p.exch[e].species});
       reads({p.exch[e].rule_off});
-      passes.push_back({P_DETACH, e});
+      passes.push_back({P_DETACH, e, match({p.exch[e].species}, 1)});
       writes({p.exch[e].species});
     }
     for (int v = 0; v < p.n_conv; ++v) {
       reads({p.conv[v].rule});
-      passes.push_back({P_CONV, v});
+      passes.push_back({P_CONV, v, match({p.conv[v].from}, 1)});
       writes({p.conv[v].from, p.conv[v].to});
     }
+    return EDM_OK;
   }
 
   // optional CUDA events between kernel groups (profiling only)
@@ -244,17 +286,23 @@ struct EdmEngine {
     k_move<F64><<<npblk, kBlock, 0, s>>>(dp, pblk, st);
     mark(3, s);
     const int rb = (R + 127) / 128;
+    const int sgrid = (int)std::max<int64_t>(1, (N / 4 + kBlock) / kBlock);  // 4 slots per thread
+    const int cgrid = 148 * 8;
     const int gm = (int)std::min<int64_t>((n_grid + 255) / 256, 4096);
     for (const Pass& ps : passes) {
       switch (ps.kind) {
-        case P_BIND_CAND: k_bind_candidates<F64><<<npblk, kBlock, 0, s>>>(dp, pblk, st, ps.index); break;
+        case P_BIND_CAND: k_bind_candidates<F64><<<sgrid, kBlock, 0, s>>>(dp, st, ps.match, ps.index); break;
         case P_BIND_APPLY: k_bind_apply<F64><<<rb, 128, 0, s>>>(dp, R, st, ps.index); break;
-        case P_DISSOC: k_dissociate<F64><<<npblk, kBlock, 0, s>>>(dp, pblk, st, ps.index); break;
-        case P_CAT: k_catalytic<F64><<<npblk, kBlock, 0, s>>>(dp, pblk, st, ps.index); break;
-        case P_REC_CAND: k_recruit_candidates<F64><<<npblk, kBlock, 0, s>>>(dp, pblk, st, ps.index); break;
+        case P_DISSOC: k_dissociate<F64><<<sgrid, kBlock, 0, s>>>(dp, st, ps.match, ps.index); break;
+        case P_CONTACTS:
+          cudaMemsetAsync(contact_count, 0, sizeof(int32_t), s);
+          k_contacts<F64><<<sgrid, kBlock, 0, s>>>(dp, st, ps.match, partner_mask, contact_sq_max);
+          break;
+        case P_CAT: k_catalytic<F64><<<cgrid, kBlock, 0, s>>>(dp, st, ps.index); break;
+        case P_REC_CAND: k_recruit_candidates<F64><<<sgrid, kBlock, 0, s>>>(dp, st, ps.match, ps.index); break;
         case P_REC_APPLY: k_recruit_apply<F64><<<rb, 128, 0, s>>>(dp, R, st, ps.index); break;
-        case P_DETACH: k_detach<F64><<<npblk, kBlock, 0, s>>>(dp, pblk, st, ps.index); break;
-        case P_CONV: k_convert<F64><<<npblk, kBlock, 0, s>>>(dp, pblk, st, ps.index); break;
+        case P_DETACH: k_detach<F64><<<sgrid, kBlock, 0, s>>>(dp, st, ps.match, ps.index); break;
+        case P_CONV: k_convert<F64><<<sgrid, kBlock, 0, s>>>(dp, st, ps.match, ps.index); break;
         case P_MERGE: k_grid_merge<<<gm > 0 ? gm : 1, 256, 0, s>>>(grid_cnt, grid_delta, n_grid); break;
       }
     }
@@ -379,7 +427,7 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
     pfirst.push_back(np);
     pcount.push_back(p.n_particles);
     np += p.n_particles;
-    nc += (int64_t)p.nx * p.ny;
+    nc += (int64_t)p.nx * p.ny + 1;
     if (E->has_phot) {
       const EdmPhotParams& q = E->hpp[r];
       if (q.photon_offset != nph) {
@@ -459,6 +507,19 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
   ALLOC(E->bind_count, n_replicas);
   ALLOC(E->bind_key, (size_t)n_replicas * kBindCap);
   ALLOC(E->bind_ab, (size_t)n_replicas * kBindCap * 2);
+  if ((rc = E->build_schedule()) != EDM_OK) {
+    delete E;
+    return rc;
+  }
+  E->contact_cap = std::max<int64_t>(4 * np, 1 << 20);
+  ALLOC(E->contacts, (size_t)E->contact_cap);
+  ALLOC(E->contact_count, 1);
+  ALLOC(E->rep_first, (size_t)n_replicas + 1);
+  {
+    std::vector<int64_t> rf(pfirst);
+    rf.push_back(np);
+    CUDA_TRY(cudaMemcpy(E->rep_first, rf.data(), sizeof(int64_t) * rf.size(), cudaMemcpyHostToDevice));
+  }
   std::vector<int2> pt = tiles(pfirst, pcount);
   E->npblk = (int)pt.size();
   ALLOC(E->pblk, pt.size());
@@ -498,7 +559,6 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
   ALLOC(E->st_ctmc, np);
   ALLOC(E->st_pos, (size_t)np * 2);
 #undef ALLOC
-  E->build_schedule();
   CUDA_TRY(cudaDeviceSynchronize());
   *out = E;
   return EDM_OK;
@@ -538,7 +598,7 @@ __global__ void k_set_state(const EdmDynParams* __restrict__ P, const int2* __re
   flags[s] = fl_make(species[s], alive[s] != 0);
   ids[s] = (int32_t)s;
   slot_of_id[s] = (int32_t)s;
-  atomicAdd(&cnt[g.cbase + c], 1);
+  atomicAdd(&cnt[g.cbase + (alive[s] ? c : g.grave)], 1);
 }
 
 template <bool F64>
@@ -905,13 +965,21 @@ int edm_get_cells(EdmEngine* E, int32_t replica, int32_t* cell_start, int32_t* m
   const EdmDynParams& p = E->hdp[replica];
   const int64_t nc = (int64_t)p.nx * p.ny;
   if (cap_cells < nc + 1 || cap_members < p.n_particles) return fail(EDM_EINVAL, "edm_get_cells: buffers too small");
+  // The sort buckets hold alive particles only; the reference's cell list
+  // holds every particle (dynamics.py:181-196), so group all slots by the
+  // reference cell each slot stores.
   cudaStream_t s = (cudaStream_t)stream;
-  CUDA_TRY(cudaMemcpyAsync(cell_start, E->cell_start + p.cell_offset, sizeof(int32_t) * (nc + 1), cudaMemcpyDeviceToHost, s));
-  CUDA_TRY(cudaMemcpyAsync(members, E->ids[E->cur] + p.particle_offset, sizeof(int32_t) * p.n_particles,
+  std::vector<int32_t> cells(p.n_particles), ids(p.n_particles);
+  CUDA_TRY(cudaMemcpyAsync(cells.data(), E->cell_pre + p.particle_offset, sizeof(int32_t) * p.n_particles,
+                           cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(ids.data(), E->ids[E->cur] + p.particle_offset, sizeof(int32_t) * p.n_particles,
                            cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
-  for (int64_t c = 0; c <= nc; ++c) cell_start[c] -= (int32_t)p.particle_offset;
-  for (int64_t i = 0; i < p.n_particles; ++i) members[i] -= (int32_t)p.particle_offset;
+  for (int64_t c = 0; c <= nc; ++c) cell_start[c] = 0;
+  for (int64_t i = 0; i < p.n_particles; ++i) cell_start[cells[i] + 1] += 1;
+  for (int64_t c = 0; c < nc; ++c) cell_start[c + 1] += cell_start[c];
+  std::vector<int32_t> fill(cell_start, cell_start + nc);
+  for (int64_t i = 0; i < p.n_particles; ++i) members[fill[cells[i]]++] = ids[i] - (int32_t)p.particle_offset;
   return EDM_OK;
 }
 

@@ -90,7 +90,7 @@ class EdmDynParams(C.Structure):
         ("cell_sx", C.c_double), ("cell_sy", C.c_double), ("cutoff_sq", C.c_double),
         ("particle_offset", C.c_int64), ("n_particles", C.c_int64),
         ("cell_offset", C.c_int64), ("grid_cells", C.c_int64),
-        ("max_disp", C.c_double), ("max_disp_sq", C.c_double),
+        ("max_disp", C.c_double), ("max_disp_sq", C.c_double), ("force_range_sq", C.c_double),
         ("use_wca", C.c_int32), ("use_harmonic", C.c_int32), ("n_species", C.c_int32),
         ("dfield", C.c_int32),
         ("D_base", C.c_double * MAX_SPECIES),
@@ -368,6 +368,29 @@ def derive_dynamics(config: SimulationConfig) -> DynDerived:
     return d
 
 
+def force_range_sq(d: DynDerived) -> float:
+    """Largest squared separation at which any pair force is non-zero: the
+    WCA range 2^(1/3) sigma^2 (dynamics.py:711) or the harmonic sigma^2
+    (dynamics.py:796), evaluated with the kernels' own expressions."""
+    best = 0.0
+    n = d.sigma_matrix.shape[0]
+    for i in range(n):
+        for j in range(n):
+            sig = float(d.sigma_matrix[i, j])
+            if sig <= 0.0:
+                continue
+            if d.use_wca and d.epsilon_matrix[i, j] > 0.0:
+                best = max(best, sig * sig * 1.2599210498948732)
+            if d.use_harmonic and d.harmonic_matrix[i, j] > 0.0:
+                best = max(best, sig * sig)
+    return best
+
+
+def n_buckets(d: DynDerived) -> int:
+    """Sort buckets of one replica: its cells plus one for non-alive particles."""
+    return d.nx * d.ny + 1
+
+
 def check_supported(config: SimulationConfig) -> None:
     """Features of the reference outside this engine raise here, loudly."""
     if getattr(config, "use_adaptation", False):
@@ -381,6 +404,12 @@ def check_supported(config: SimulationConfig) -> None:
             raise NotImplementedError(
                 f"catalytic reaction '{cat.name}': enzyme == product/substrate makes a pass "
                 "order-dependent; not supported by the parallel pass")
+    enzymes = {c.enzyme for c in config.catalytic_reactions}
+    converted = {c.substrate for c in config.catalytic_reactions} | {c.product for c in config.catalytic_reactions}
+    if enzymes & converted:
+        raise NotImplementedError(
+            f"species {sorted(enzymes & converted)} are both enzymes and catalytic substrates/products; "
+            "the per-step contact list requires enzymes to keep their species during the catalytic passes")
     for rx in config.reactions:
         if rx.is_bimolecular and rx.products and rx.products[0] in rx.reactants:
             raise NotImplementedError(
@@ -416,6 +445,7 @@ def build_dyn_params(config: SimulationConfig, n_particles: int, seed: Optional[
     P.particle_offset, P.n_particles, P.cell_offset = particle_offset, n_particles, cell_offset
     P.max_disp = d.max_displacement
     P.max_disp_sq = d.max_displacement * d.max_displacement
+    P.force_range_sq = force_range_sq(d)
     P.use_wca, P.use_harmonic, P.n_species = int(d.use_wca), int(d.use_harmonic), config.n_species
     for i, s in enumerate(config.species):
         P.D_base[i] = s.diffusion_coefficient

@@ -57,6 +57,7 @@ extern "C" {
 #define EDM_STATUS_BIND_CAP 0x10u      /* binding candidate buffer overflow                             */
 #define EDM_STATUS_RECRUIT_CAP 0x20u   /* recruitment candidate buffer overflow                         */
 #define EDM_STATUS_POISSON_NORMAL 0x40u /* a Poisson mean >= 30 used the normal approximation            */
+#define EDM_STATUS_CONTACT_CAP 0x80u   /* catalytic contact buffer overflow (events may be missed)      */
 
 /* ---- noise streams (Philox key = seed; counter = (a, b, step, stream)) --- */
 enum EdmStream {
@@ -131,12 +132,14 @@ typedef struct {
   /* cell list (dynamics.py:89-114, 1738-1788) */
   int32_t nx, ny;
   double cell_sx, cell_sy, cutoff_sq;
-  /* replica slices of the engine's global arrays */
+  /* replica slices of the engine's global arrays; a replica owns nx*ny + 1
+   * sort buckets: its cells, then one bucket for non-alive particles */
   int64_t particle_offset, n_particles;
   int64_t cell_offset;
   int64_t grid_cells;    /* total density-grid cells of this replica          */
   /* BD (dynamics.py:323-406, 1837-1864) */
   double max_disp, max_disp_sq;
+  double force_range_sq; /* max over species pairs of the squared force range */
   int32_t use_wca, use_harmonic, n_species, dfield;
   double D_base[EDM_MAX_SPECIES];
   double sigma[EDM_MAX_SPECIES * EDM_MAX_SPECIES];
