@@ -14,18 +14,23 @@
 #include <tuple>
 #include <vector>
 
+#include "edm_error.h"
 #include "edm_phot.cuh"
 
 using namespace edm;
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
 
-int fail(int code, const std::string& msg) {
+int edm::report_error(int code, const std::string& msg) {
   g_last_error = msg;
   return code;
 }
+
+namespace {
+
+int fail(int code, const std::string& msg) { return edm::report_error(code, msg); }
 
 #define CUDA_TRY(expr)                                                                  \
   do {                                                                                  \

@@ -71,6 +71,7 @@ def load_library():
     L.edm_get_cells.argtypes = [vp, i32, vp, vp, i64, i64, vp]
     L.edm_profile_steps.argtypes = [vp, i32, i32, vp, vp]
     L.edm_launches_per_step.argtypes = [vp, i32]
+    L.edm_cell_list_static.argtypes = [vp, i64, C.c_double, C.c_double, i32, i32, vp, vp, vp]
     L.edm_noise_normal_pairs.argtypes = [u64, i64, i32, vp, i64, vp, vp]
     L.edm_noise_uniforms.argtypes = [u64, i64, i32, vp, vp, i64, vp, vp]
     for which, cls in ((0, PR.EdmDynParams), (1, PR.EdmPhotParams), (2, PR.EdmScopeParams), (3, PR.EdmHostState)):

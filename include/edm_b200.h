@@ -317,6 +317,31 @@ int edm_get_cells(EdmEngine* eng, int32_t replica, int32_t* cell_start,
                   int32_t* members, int64_t cap_cells, int64_t cap_members,
                   void* stream);
 
+/* ---- allocation-free cell list ------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory when they call: code that runs inside a pre-sized device memory
+ * pool or arena owned by a host framework, a process whose device memory is
+ * already handed to another allocator, or a tight loop where cudaMalloc (which
+ * may synchronise the device) is not acceptable.
+ *
+ * Builds the reference's cell list (CellList with cell = L/n, cx = int(x/cell)
+ * clamped, key cx*ny + cy) of n caller-owned device positions [n][2]:
+ * cell_start_dev[nx*ny + 1] and members_dev[n] (particle indices of cell c in
+ * members[cell_start[c] .. cell_start[c+1]), ascending).  It allocates
+ * nothing: its scratch is one static device array of
+ * EDM_STATIC_MAX_CELLS-sized counters that every GPU loading this library
+ * holds until the process exits (about 8 MB).  nx*ny beyond
+ * EDM_STATIC_MAX_CELLS is rejected with EDM_EINVAL.  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress), so
+ * make it before any stream capture.  All calls share the one array: calls
+ * that overlap on the GPU race; order them on one stream.  Each call clears
+ * what must start at zero. */
+#define EDM_STATIC_MAX_CELLS (1 << 20)
+int edm_cell_list_static(const double* positions_dev, int64_t n, double Lx,
+                         double Ly, int32_t nx, int32_t ny,
+                         int32_t* cell_start_dev, int32_t* members_dev,
+                         void* stream);
+
 /* Noise of the engine's generator, for injection into the reference:
  * writes n keyed standard normals pairs (2n doubles) / uniforms.  The
  * arrays are device pointers; keys a[i] (particle / photon index). */
