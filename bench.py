@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--flim-replicas", type=int, default=256, help="FLIM acquisition replicas (256^2 px each)")
+    ap.add_argument("--no-flim", action="store_true")
     return ap.parse_args()
 
 
@@ -177,6 +179,15 @@ def oracle_sample(raws, steps: int, threads: int):
     return ps / dt, dt, ps
 
 
+def oracle_sample_sized(raws, threads: int, target_s: float = 10.0):
+    """oracle_sample with the step count calibrated so the timed run takes
+    about target_s seconds (10 calibration steps first, at most 2000 steps)."""
+    _, dt, _ = oracle_sample(raws, 10, threads)
+    steps = int(min(2000, max(10, round(10 * target_s / max(dt, 1e-3)))))
+    v, dt, ps = oracle_sample(raws, steps, threads)
+    return v, dt, ps, steps
+
+
 def reference_arm(args, rank: int, world: int):
     if rank != 0:
         return
@@ -190,21 +201,126 @@ def reference_arm(args, rank: int, world: int):
     for _ in range(max(0, args.warmup)):
         oracle_sample(sample[:2], 1, cores)
     vals = []
+    steps_used = 0
     for _ in range(max(1, args.steps)):
-        v, dt, ps = oracle_sample(sample, 10, cores)
+        v, dt, ps, steps_used = oracle_sample_sized(sample, cores, target_s=10.0)
         vals.append(v)
     value = float(statistics.median(vals))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"batched ensemble, {args.replicas} replicas (sample: 16 median-size replicas x 10 BD "
-                               "steps per timed step)", "replicas": args.replicas},
+        "config": {"workload": f"batched ensemble, {args.replicas} replicas (sample: 16 median-size replicas x "
+                               f"{steps_used} BD steps per timed step, about 10 s)", "replicas": args.replicas},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": "16 median-size replicas x 10 full BD steps (dynamics+photophysics+TCSPC)"},
+                         "sample": f"16 median-size replicas x {steps_used} full BD steps "
+                                   "(dynamics+photophysics+TCSPC), about 10 s per timed step"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if not args.no_flim:
+        fv, fdt, fr = flim_cpu_sample(16, args.seed)
+        line["flim"] = {"metric": "FLIM px/s", "value": fv, "unit": "px/s",
+                        "workload": FLIM_WORKLOAD.format(R=args.flim_replicas),
+                        "cpu_baseline": {"value": fv, "unit": "px/s", "cores": 1, "kind": "port",
+                                         "sample": f"{fr} replicas, float64 numpy restatement + numpy Poisson "
+                                                   f"({fdt:.1f} s); the reference has no batched acquisition"}}
     print(json.dumps(line), flush=True)
+
+
+FLIM_WORKLOAD = ("batched FLIM acquisition: {R} replicas x 256x256 px x 256 bins, 50,000 donors per replica "
+                 "(bound fraction U(0,1)), 31-tap PSF (sigma 100 nm), 1000 photons/px budget")
+FLIM_BYTES_PER_PX = 256 * 4 + 8  # histogram written + the two intensity values read
+
+
+def flim_cpu_sample(n_replicas: int, seed: int, steps: int = 1):
+    """The float64 numpy restatement (oracle/flim_oracle.py) of the acquisition
+    on a bounded sample of replicas: expected histograms + numpy Poisson.
+    Returns FLIM px/s, seconds, replicas."""
+    from flim_microscopy_simulator_with_causal_inference_b200 import flim_acquire as FA
+    from flim_microscopy_simulator_with_causal_inference_b200.config import config_from_dict
+    from oracle import flim_oracle as FO
+    p, _ = FA.build_flim_params(config_from_dict(FA.flim_config()), n_replicas, 50_000, 1000.0, seed)
+    bf = FA.bound_fractions(n_replicas, seed)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for r in range(n_replicas):
+            e = FO.acquire_expected(p, bf, r)
+            FO.poisson_histograms(e["mu"], seed + r)
+    dt = time.perf_counter() - t0
+    return n_replicas * steps * 65536 / dt, dt, n_replicas
+
+
+def flim_bench(args, device: int, rank: int, world: int, stream):
+    """FLIM px/s of the batched acquisition (device-resident and end to end)."""
+    import ctypes
+    import torch
+    from flim_microscopy_simulator_with_causal_inference_b200 import flim_acquire as FA
+    R = args.flim_replicas
+    acq = FA.FlimAcquisition(FA.flim_config(), R, n_emitters=50_000, photon_budget=1000.0,
+                             seed=args.seed + 7919 * rank, device=device)
+    s = int(stream.cuda_stream)
+    for _ in range(max(3, args.warmup)):
+        acq.acquire(stream=s)
+    stream.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3 * args.steps)]
+    with ClockSampler(device) as clk:
+        for k in range(args.steps):
+            ev[3 * k].record(stream)
+            acq.project(stream=s)
+            ev[3 * k + 1].record(stream)
+            acq.histograms(True, stream=s)
+            ev[3 * k + 2].record(stream)
+        stream.synchronize()
+    torch.cuda.synchronize()
+    proj = [ev[3 * k].elapsed_time(ev[3 * k + 1]) for k in range(args.steps)]
+    hist = [ev[3 * k + 1].elapsed_time(ev[3 * k + 2]) for k in range(args.steps)]
+    ms = max_over_ranks(ev[0].elapsed_time(ev[-1]), world, "cuda")
+    px = R * 65536 * world * args.steps
+    value = px / (ms / 1e3)
+    hist_ms = statistics.mean(hist)
+    proj_ms = statistics.mean(proj)
+    peak, peak_kind = peaks()
+    achieved = FLIM_BYTES_PER_PX * R * 65536 / (hist_ms / 1e3) / 1e9
+    gemm_flops = 2 * (2 * 2 * 256 ** 3) * R  # two maps, two 256^3 products each (algorithmic)
+    err = acq.error_word()
+
+    # e2e: host bound fractions in, every histogram out to pinned host memory
+    ring = [torch.empty(65536 * 256, dtype=torch.int32).pin_memory().numpy() for _ in range(4)]
+    bf = FA.bound_fractions(R, args.seed + 1)
+    bf_pinned = torch.from_numpy(bf).pin_memory().numpy()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        acq.set_inputs(bf_pinned, args.seed + 1 + k, stream=s)
+        acq.acquire(stream=s)
+        for r in range(R):
+            buf = ring[r % 4]
+            acq._check(acq.lib.edm_flim_read(acq._h, FA.HIST, r, buf.ctypes.data_as(ctypes.c_void_p), buf.nbytes, s))
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world, "cuda")
+    acq.close()
+    return {
+        "metric": "FLIM px/s", "value": value, "unit": "px/s", "ms_per_step": ms / args.steps,
+        "workload": FLIM_WORKLOAD.format(R=R), "replicas_per_gpu": R, "dtype": "bf16 GEMM / f32 accumulate, f64 bins",
+        "kernel_ms": {"project": proj_ms, "histograms": hist_ms},
+        "roofline": {"bound": "hbm", "kernel": "k_hist", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                     "alg_bytes_per_px": FLIM_BYTES_PER_PX},
+        "tensor": {"kernel": "k_umma_gemm x2 (+ emitter maps)", "alg_tflops": gemm_flops / (proj_ms / 1e3) / 1e12,
+                   "note": "algorithmic 2 x 2*256^3 FLOP per map over the whole projection time"},
+        "e2e": {"value": px / e2e_s, "unit": "px/s", "h2d_bytes_per_step": int(bf.nbytes),
+                "d2h_bytes_per_step": int(R * 65536 * 256 * 4),
+                "note": "per acquisition: bound fractions H2D, acquire, every histogram D2H to pinned host memory"},
+        "gpu_launches": 5 * args.steps, "error_word": err, "clocks": clk.summary(),
+        "l2": "histograms 17 GB per acquisition >> 126 MB L2",
+    }
 
 
 # ---------------------------------------------------------------------------
@@ -331,15 +447,24 @@ def main():
         fp64 = c1.total_membrane * n64 / (f0.elapsed_time(f1) / 1e3)
         del c1
 
+    # ---- batched FLIM acquisition -------------------------------------------
+    flim = None
+    if not args.no_flim:
+        flim = flim_bench(args, device, rank, world, stream)
+
     # ---- CPU baseline (oracle) on a bounded sample ---------------------------
     cpu = None
     if not args.no_cpu_baseline and rank == 0:
         sizes = np.array([sum(r["initial_populations"].values()) for r in raws])
         order = np.argsort(np.abs(sizes - np.median(sizes)))[:16]
         cores = os.cpu_count() or 1
-        v, dt, ps = oracle_sample([raws[i] for i in order], 10, cores)
+        v, dt, ps, nsteps = oracle_sample_sized([raws[i] for i in order], cores, target_s=10.0)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": f"16 median-size replicas x 10 full BD steps ({ps} particle-steps, {dt:.1f} s)"}
+               "sample": f"16 median-size replicas x {nsteps} full BD steps ({ps} particle-steps, {dt:.1f} s)"}
+        if flim is not None:
+            fv, fdt, fr = flim_cpu_sample(16, args.seed)
+            flim["cpu_baseline"] = {"value": fv, "unit": "px/s", "cores": 1, "kind": "port",
+                                    "sample": f"{fr} replicas, float64 numpy restatement + numpy Poisson ({fdt:.1f} s)"}
 
     if rank == 0:
         line = {
@@ -365,6 +490,7 @@ def main():
                                                                  "per-step launches, full BD step"},
             "fp32_over_fp64": None if fp64 is None else value / world / fp64,
             "cpu_baseline": cpu,
+            "flim": flim,
             "gpu_launches": launches,
             "status_word": status,
             "clocks": clk.summary(),

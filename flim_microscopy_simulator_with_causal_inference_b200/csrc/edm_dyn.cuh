@@ -91,32 +91,82 @@ __device__ __forceinline__ bool matches(uint8_t f, const Match& m) {
   return ((m.species_mask >> fl_species(f)) & 1u) && (fl_alive(f) == (m.alive != 0));
 }
 
-// Vectorised flag sweep: 4 slots per thread; body(replica, slot) for matches.
+// Flag sweep with block-local compaction: each block reads the flags of its
+// 4*kBlock slots (4 per thread, one 32-bit load), collects the matching slots
+// in shared memory, then runs body(replica, slot) on them with every lane
+// busy.  Launch with blockDim == kBlock and ceil(n_slots / (4*kBlock)) blocks.
 template <typename Body>
 __device__ __forceinline__ void sweep4(const DevState& st, const Match& m, Body body) {
-  const int64_t s0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
-  if (s0 >= st.n_slots) return;
-  const uchar4 f4 = *reinterpret_cast<const uchar4*>(st.flags + s0);
-  const uint8_t f[4] = {f4.x, f4.y, f4.z, f4.w};
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const int64_t s = s0 + k;
-    if (s < st.n_slots && matches(f[k], m)) body(replica_of(st.rep_first, st.n_rep, s), s);
+  __shared__ int32_t list[4 * kBlock];
+  __shared__ int n_list, r_first;
+  const int64_t b0 = (int64_t)blockIdx.x * blockDim.x * 4;
+  if (threadIdx.x == 0) {
+    n_list = 0;
+    r_first = b0 < st.n_slots ? replica_of(st.rep_first, st.n_rep, b0) : 0;
   }
+  __syncthreads();
+  const int64_t s0 = b0 + (int64_t)threadIdx.x * 4;
+  if (s0 < st.n_slots) {
+    const uchar4 f4 = *reinterpret_cast<const uchar4*>(st.flags + s0);
+    const uint8_t f[4] = {f4.x, f4.y, f4.z, f4.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (s0 + k < st.n_slots && matches(f[k], m)) list[atomicAdd(&n_list, 1)] = (int32_t)(s0 + k);
+    }
+  }
+  __syncthreads();
+  const int n = n_list;
+  for (int q = threadIdx.x; q < n; q += blockDim.x) {
+    const int64_t s = list[q];
+    int r = r_first;
+    while (r + 1 < st.n_rep && st.rep_first[r + 1] <= s) ++r;
+    body(r, s);
+  }
+}
+
+// One atomicAdd per group of lanes adding 1 to the same address; returns
+// the value each lane would have got from its own atomicAdd(addr, 1).
+__device__ __forceinline__ int atomic_inc_aggregated(int32_t* addr) {
+  const unsigned act = __activemask();
+  const unsigned peers = __match_any_sync(act, (unsigned long long)(uintptr_t)addr);
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(peers) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(addr, __popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  return base + __popc(peers & ((1u << lane) - 1u));
 }
 
 // ---- replica geometry --------------------------------------------------------
 struct Geo {
   int nx, ny, px, py;
   double Lx, Ly, sx, sy, cutoff_sq;
-  float sxf, syf;
+  float sxf, syf, inv_ny;
   int64_t cbase, poff;
   int grave;  // bucket of non-alive particles
   __device__ __forceinline__ explicit Geo(const EdmDynParams& p)
       : nx(p.nx), ny(p.ny), px(p.periodic_x), py(p.periodic_y), Lx(p.Lx), Ly(p.Ly),
         sx(p.cell_sx), sy(p.cell_sy), cutoff_sq(p.cutoff_sq), sxf((float)p.cell_sx),
-        syf((float)p.cell_sy), cbase(p.cell_offset), poff(p.particle_offset), grave(p.nx * p.ny) {}
+        syf((float)p.cell_sy), inv_ny(1.0f / (float)p.ny), cbase(p.cell_offset), poff(p.particle_offset),
+        grave(p.nx * p.ny) {}
 };
+
+// Cell key c = cx * ny + cy -> (cx, cy) without an integer division: the
+// float quotient (c + 0.5) / ny is within one of cx for any c < 2^24 and the
+// remainder check corrects it, so the result is exact.
+__device__ __forceinline__ void split_cell(int c, const Geo& g, int& cx, int& cy) {
+  int q = __float2int_rz(((float)c + 0.5f) * g.inv_ny);
+  int r = c - q * g.ny;
+  if (r < 0) {
+    --q;
+    r += g.ny;
+  } else if (r >= g.ny) {
+    ++q;
+    r -= g.ny;
+  }
+  cx = q;
+  cy = r;
+}
 
 // Absolute position of a slot (float64).
 template <bool F64>
@@ -128,8 +178,8 @@ __device__ __forceinline__ void abs_pos(const void* pos, const int32_t* cell, in
     y = v.y;
   } else {
     const float2 v = ((const float2*)pos)[s];
-    const int c = cell[s];
-    const int cx = c / g.ny, cy = c - (c / g.ny) * g.ny;
+    int cx, cy;
+    split_cell(cell[s], g, cx, cy);
     x = __dadd_rn(__dmul_rn((double)cx, g.sx), (double)v.x);
     y = __dadd_rn(__dmul_rn((double)cy, g.sy), (double)v.y);
   }
@@ -154,8 +204,9 @@ __device__ __forceinline__ double min_image_sq(double x1, double y1, double x2, 
 // float32 separation of two cell-relative points (cells ci, cj).
 __device__ __forceinline__ float rel_sq_f32(int ci, float2 oi, int cj, float2 oj, const Geo& g, float& dx,
                                             float& dy) {
-  const int cxi = ci / g.ny, cyi = ci - cxi * g.ny;
-  const int cxj = cj / g.ny, cyj = cj - cxj * g.ny;
+  int cxi, cyi, cxj, cyj;
+  split_cell(ci, g, cxi, cyi);
+  split_cell(cj, g, cxj, cyj);
   int dcx = cxi - cxj, dcy = cyi - cyj;
   if (g.px) {
     if (2 * dcx > g.nx) dcx -= g.nx;
@@ -200,7 +251,8 @@ __device__ __forceinline__ Tile tile_of(const int2* blk) {
 // Visit the 3x3 neighbour cells of cell c (dynamics.py:243-260): f(bucket, ordinal, dcx, dcy).
 template <typename F>
 __device__ __forceinline__ void for_neighbour_cells(const Geo& g, int c, F f) {
-  const int cx = c / g.ny, cy = c - (c / g.ny) * g.ny;
+  int cx, cy;
+  split_cell(c, g, cx, cy);
   for (int dcx = -1; dcx <= 1; ++dcx) {
     int ncx = cx + dcx;
     if (g.px) ncx = ncx < 0 ? ncx + g.nx : (ncx >= g.nx ? ncx - g.nx : ncx);
@@ -342,7 +394,7 @@ __global__ void __launch_bounds__(kBlock) k_scatter(const EdmDynParams* __restri
   const int c = st.cell_post[t.s];
   const uint8_t f = st.flags_old[t.s];
   const int key = fl_alive(f) ? c : p.nx * p.ny;
-  const int d = atomicAdd(&st.cell_cursor[p.cell_offset + key], 1);
+  const int d = atomic_inc_aggregated(&st.cell_cursor[p.cell_offset + key]);
   if constexpr (F64) {
     ((double2*)st.pos_pre)[d] = ((const double2*)st.pos_post)[t.s];
   } else {
@@ -527,7 +579,7 @@ __global__ void __launch_bounds__(kBlock) k_move(const EdmDynParams* __restrict_
       ((float2*)st.pos_post)[s] = ((const float2*)st.pos_pre)[s];
     }
     st.cell_post[s] = c;
-    atomicAdd(&st.cnt_next[g.cbase + g.grave], 1);
+    atomic_inc_aggregated(&st.cnt_next[g.cbase + g.grave]);
     return;
   }
   const int sp = fl_species(f);
@@ -607,7 +659,8 @@ __global__ void __launch_bounds__(kBlock) k_move(const EdmDynParams* __restrict_
       dyt *= scale;
     }
     float2 o = ((const float2*)st.pos_pre)[s];
-    int cx = c / g.ny, cy = c - (c / g.ny) * g.ny;
+    int cx, cy;
+    split_cell(c, g, cx, cy);
     o.x += dxt;
     o.y += dyt;
     // renormalise into [0, cell) and carry the integer cell
@@ -617,9 +670,9 @@ __global__ void __launch_bounds__(kBlock) k_move(const EdmDynParams* __restrict_
     for (int it = 0; it < 64 && o.y < 0.0f; ++it) { o.y += g.syf; --cy; }
     if (o.x >= g.sxf || o.x < 0.0f) o.x = 0.0f;
     if (o.y >= g.syf || o.y < 0.0f) o.y = 0.0f;
-    if (g.px) {
-      cx = cx % g.nx;
-      if (cx < 0) cx += g.nx;
+    if (g.px) {  // |cx| stays within 64 cells of the box: a few wraps at most
+      while (cx >= g.nx) cx -= g.nx;
+      while (cx < 0) cx += g.nx;
     } else if (cx < 0 || cx >= g.nx) {  // reflecting wall, in float64
       double ax = (double)cx * g.sx + (double)o.x;
       if (ax < 0.0) ax = -ax;
@@ -628,8 +681,8 @@ __global__ void __launch_bounds__(kBlock) k_move(const EdmDynParams* __restrict_
       o.x = (float)(ax - (double)cx * g.sx);
     }
     if (g.py) {
-      cy = cy % g.ny;
-      if (cy < 0) cy += g.ny;
+      while (cy >= g.ny) cy -= g.ny;
+      while (cy < 0) cy += g.ny;
     } else if (cy < 0 || cy >= g.ny) {
       double ay = (double)cy * g.sy + (double)o.y;
       if (ay < 0.0) ay = -ay;
@@ -644,7 +697,7 @@ __global__ void __launch_bounds__(kBlock) k_move(const EdmDynParams* __restrict_
     y = (double)cy * g.sy + (double)o.y;
   }
   st.cell_post[s] = newc;
-  atomicAdd(&st.cnt_next[g.cbase + newc], 1);
+  atomic_inc_aggregated(&st.cnt_next[g.cbase + newc]);
   grid_add(p, st.grid_cnt, sp, x, y, 1);
 }
 

@@ -373,6 +373,7 @@ int64_t edm_abi_sizeof(int which) {
     case 1: return (int64_t)sizeof(EdmPhotParams);
     case 2: return (int64_t)sizeof(EdmScopeParams);
     case 3: return (int64_t)sizeof(EdmHostState);
+    case 4: return (int64_t)sizeof(EdmFlimParams);
     default: return -1;
   }
 }

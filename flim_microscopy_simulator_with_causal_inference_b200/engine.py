@@ -72,9 +72,19 @@ def load_library():
     L.edm_profile_steps.argtypes = [vp, i32, i32, vp, vp]
     L.edm_launches_per_step.argtypes = [vp, i32]
     L.edm_cell_list_static.argtypes = [vp, i64, C.c_double, C.c_double, i32, i32, vp, vp, vp]
+    L.edm_flim_create.argtypes = [vp, i32, C.POINTER(vp)]
+    L.edm_flim_destroy.argtypes = [vp]
+    L.edm_flim_set_inputs.argtypes = [vp, vp, u64, vp]
+    L.edm_flim_project.argtypes = [vp, vp]
+    L.edm_flim_histograms.argtypes = [vp, i32, vp]
+    L.edm_flim_acquire.argtypes = [vp, vp]
+    L.edm_flim_device_ptr.argtypes = [vp, i32, C.POINTER(vp), C.POINTER(i64)]
+    L.edm_flim_read.argtypes = [vp, i32, i32, vp, i64, vp]
+    L.edm_flim_get_error.argtypes = [vp, C.POINTER(C.c_uint32)]
     L.edm_noise_normal_pairs.argtypes = [u64, i64, i32, vp, i64, vp, vp]
     L.edm_noise_uniforms.argtypes = [u64, i64, i32, vp, vp, i64, vp, vp]
-    for which, cls in ((0, PR.EdmDynParams), (1, PR.EdmPhotParams), (2, PR.EdmScopeParams), (3, PR.EdmHostState)):
+    for which, cls in ((0, PR.EdmDynParams), (1, PR.EdmPhotParams), (2, PR.EdmScopeParams), (3, PR.EdmHostState),
+                       (4, PR.EdmFlimParams)):
         if L.edm_abi_sizeof(which) != C.sizeof(cls):
             raise ImportError(f"ABI mismatch for {cls.__name__}: C {L.edm_abi_sizeof(which)} vs ctypes {C.sizeof(cls)}")
     _lib = L

@@ -147,6 +147,14 @@ class EdmScopeParams(C.Structure):
     ]
 
 
+class EdmFlimParams(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("n_replicas", C.c_int32), ("n_emitters", C.c_int32),
+                ("n_bins", C.c_int32), ("half_taps", C.c_int32), ("seed", C.c_uint64),
+                ("bin_width_ns", C.c_double), ("sigma_irf_ns", C.c_double), ("sigma_psf_px", C.c_double),
+                ("tau_free_ns", C.c_double), ("tau_bound_ns", C.c_double),
+                ("yield_free", C.c_double), ("yield_bound", C.c_double)]
+
+
 class EdmHostState(C.Structure):
     _fields_ = [("n", C.c_int64), ("positions", C.c_void_p), ("species_id", C.c_void_p),
                 ("is_alive", C.c_void_p), ("bond_partner", C.c_void_p), ("has_dye", C.c_void_p),

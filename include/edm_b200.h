@@ -233,7 +233,8 @@ typedef struct EdmEngine EdmEngine;
 /* ---- versioning / layout checks ----------------------------------------- */
 int edm_abi_version(void);
 /* sizeof of the ABI structs: which = 0 EdmDynParams, 1 EdmPhotParams,
- * 2 EdmScopeParams, 3 EdmHostState; lets a binding verify its mirror. */
+ * 2 EdmScopeParams, 3 EdmHostState, 4 EdmFlimParams; lets a binding verify
+ * its mirror. */
 int64_t edm_abi_sizeof(int which);
 const char* edm_last_error(void);
 
@@ -341,6 +342,79 @@ int edm_cell_list_static(const double* positions_dev, int64_t n, double Lx,
                          double Ly, int32_t nx, int32_t ny,
                          int32_t* cell_start_dev, int32_t* members_dev,
                          void* stream);
+
+/* ---- batched FLIM acquisition from expected intensities ----------------
+ * No reference function: the reference forms FLIM stacks photon by photon
+ * (VirtualMicroscope.process_photons, microscope.py:1069-1157).  This path
+ * takes its pieces from there: the emitter-centric Gaussian PSF with a
+ * (2R+1)^2 window renormalised over in-field pixels (microscope.py:522-631),
+ * TCSPC bins with negative times in bin 0 and late ones lost
+ * (microscope.py:716-803), Gaussian IRF, photon yields and lifetimes of the
+ * per-pulse chain (photophysics.py:218-331, computed on the host).
+ * For each replica: n_emitters donors at keyed uniform pixels, each bound
+ * (FRET) with the replica's bound fraction; intensity maps
+ * I = G . counts . G^T on tcgen05 BF16 GEMMs; then per pixel and bin a
+ * Poisson count of mean I_free h_free[b] yield_free + I_bound h_bound[b]
+ * yield_bound, written as uint32 [replica][x][y][bin]. */
+typedef struct EdmFlimParams {
+  int32_t nx, ny;          /* pixels per side; 256 x 256 only                   */
+  int32_t n_replicas;      /* 1 .. 4096                                         */
+  int32_t n_emitters;      /* per replica                                        */
+  int32_t n_bins;          /* 128 or 256                                         */
+  int32_t half_taps;       /* R: PSF window half-width in pixels (2R+1 taps)    */
+  uint64_t seed;
+  double bin_width_ns, sigma_irf_ns;
+  double sigma_psf_px;     /* PSF sigma in pixels                                */
+  double tau_free_ns, tau_bound_ns;
+  double yield_free, yield_bound; /* expected detected photons per emitter     */
+} EdmFlimParams;
+
+/* Seed of replica r: the acquisition seed mixed with r (also used by hosts
+ * that reproduce the emitter draws). */
+#if defined(__CUDACC__)
+#define EDM_HOST_DEVICE __host__ __device__
+#else
+#define EDM_HOST_DEVICE
+#endif
+static inline EDM_HOST_DEVICE uint64_t edm_flim_replica_seed(uint64_t seed, int32_t r) {
+  return seed ^ (0x9E3779B97F4A7C15ull * (uint64_t)(r + 1));
+}
+
+enum EdmFlimArray {
+  EDM_FLIM_HIST = 0,      /* uint32 [R][nx][ny][n_bins]                        */
+  EDM_FLIM_INTENSITY = 1, /* float  [R][free, bound][nx][ny]                   */
+  EDM_FLIM_COUNTS = 2,    /* int32  [R][free, bound][nx][ny] emitter counts    */
+  EDM_FLIM_TAU = 3,       /* double [R][nx][ny] expected mean arrival time, ns */
+  EDM_FLIM_BINS = 4,      /* double [free, bound][n_bins] bin probabilities    */
+  EDM_FLIM_ERROR = 5      /* uint32 error word (EDM_FLIM_ERR_*)                */
+};
+#define EDM_FLIM_ERR_LOAD_WAIT 0x1u /* a GEMM stage load did not arrive in time  */
+#define EDM_FLIM_ERR_DONE_WAIT 0x2u /* a GEMM accumulator did not complete       */
+#define EDM_FLIM_ERR_COUNT 0x4u     /* > 256 emitters in one pixel (bf16 inexact) */
+
+typedef struct EdmFlim EdmFlim;
+/* Allocates every device array (histograms: R * nx * ny * n_bins * 4 bytes)
+ * and computes the PSF band and bin probabilities. */
+int edm_flim_create(const EdmFlimParams* params, int32_t device, EdmFlim** out);
+int edm_flim_destroy(EdmFlim* flim);
+/* Host bound fractions (n_replicas doubles) and the seed of the next
+ * acquisition; the copy is ordered on `stream`. */
+int edm_flim_set_inputs(EdmFlim* flim, const double* bound_fraction_host,
+                        uint64_t seed, void* stream);
+/* Emitter maps and intensity maps (the two GEMMs). */
+int edm_flim_project(EdmFlim* flim, void* stream);
+/* Poisson histograms from the intensity maps; with_tau also writes the
+ * expected mean arrival time per pixel. */
+int edm_flim_histograms(EdmFlim* flim, int32_t with_tau, void* stream);
+/* project + histograms (with tau). */
+int edm_flim_acquire(EdmFlim* flim, void* stream);
+/* Device pointer and size in bytes of one of the EdmFlimArray arrays. */
+int edm_flim_device_ptr(EdmFlim* flim, int32_t what, void** out, int64_t* bytes);
+/* Copies array `what` (one replica's part when replica >= 0 and the array
+ * is per replica, else all of it) to host memory and waits for `stream`. */
+int edm_flim_read(EdmFlim* flim, int32_t what, int32_t replica,
+                  void* host_out, int64_t bytes, void* stream);
+int edm_flim_get_error(EdmFlim* flim, uint32_t* word);
 
 /* Noise of the engine's generator, for injection into the reference:
  * writes n keyed standard normals pairs (2n doubles) / uniforms.  The
