@@ -111,6 +111,31 @@ __device__ __forceinline__ U2 normal2(uint64_t seed, int64_t step, int stream, u
   return z;
 }
 
+// The same normal pair in float32 for the float32 engine: the candidate
+// draws and the acceptance test are those of normal2 (float64), so both
+// accept the same candidate; only sqrt(-2 ln q / q) is evaluated in float32
+// (relative error ~1e-6, far below the float32 path's position tolerance).
+__device__ __forceinline__ void normal2_f32(uint64_t seed, int64_t step, int stream, uint64_t a, float& z0,
+                                            float& z1) {
+  double x = 0.0, y = 0.0, q = 0.0;
+  uint32_t t = 0;
+  for (; t < 64; ++t) {
+    const U2 u = uniform2(seed, step, stream, a, t);
+    x = __dadd_rn(__dmul_rn(2.0, u.u0), -1.0);
+    y = __dadd_rn(__dmul_rn(2.0, u.u1), -1.0);
+    q = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
+    if (q > 0.0 && q < 1.0) break;
+  }
+  if (t == 64) {
+    z0 = z1 = 0.0f;
+    return;
+  }
+  const float qf = (float)q;
+  const float f = sqrtf(-2.0f * logf(qf) / qf);
+  z0 = (float)x * f;
+  z1 = (float)y * f;
+}
+
 // ---- particle flags: bits 0-6 species, bit 7 alive -------------------------
 __device__ __forceinline__ int fl_species(uint8_t f) { return f & 0x7F; }
 __device__ __forceinline__ bool fl_alive(uint8_t f) { return (f & 0x80) != 0; }

@@ -32,6 +32,7 @@
 namespace edm {
 
 constexpr int kBlock = 256;
+constexpr int kSweepChunk = 128;  // slots per warp in the flag sweeps (4 per lane)
 constexpr int kRecCap = 128;
 constexpr int kBindCap = 512;
 
@@ -67,6 +68,7 @@ struct DevState {
   int32_t* contact_count;
   int64_t contact_cap;
   const int64_t* rep_first;  // [R + 1] first slot of each replica
+  const int32_t* chunk_rep;  // replica of the first slot of each kSweepChunk-slot chunk
   int n_rep;
   int64_t n_slots;
 };
@@ -91,34 +93,36 @@ __device__ __forceinline__ bool matches(uint8_t f, const Match& m) {
   return ((m.species_mask >> fl_species(f)) & 1u) && (fl_alive(f) == (m.alive != 0));
 }
 
-// Flag sweep with block-local compaction: each block reads the flags of its
-// 4*kBlock slots (4 per thread, one 32-bit load), collects the matching slots
-// in shared memory, then runs body(replica, slot) on them with every lane
-// busy.  Launch with blockDim == kBlock and ceil(n_slots / (4*kBlock)) blocks.
+// Flag sweep with warp-local compaction: each warp reads the flags of its
+// kSweepChunk slots (4 per lane, one 32-bit load), gathers the matching
+// slots in its shared-memory list (ballot + popc, no block barrier), then
+// runs body(replica, slot) on them with every lane busy.  Launch with
+// blockDim == kBlock and ceil(n_slots / (4*kBlock)) blocks.
 template <typename Body>
 __device__ __forceinline__ void sweep4(const DevState& st, const Match& m, Body body) {
-  __shared__ int32_t list[4 * kBlock];
-  __shared__ int n_list, r_first;
-  const int64_t b0 = (int64_t)blockIdx.x * blockDim.x * 4;
-  if (threadIdx.x == 0) {
-    n_list = 0;
-    r_first = b0 < st.n_slots ? replica_of(st.rep_first, st.n_rep, b0) : 0;
-  }
-  __syncthreads();
-  const int64_t s0 = b0 + (int64_t)threadIdx.x * 4;
-  if (s0 < st.n_slots) {
-    const uchar4 f4 = *reinterpret_cast<const uchar4*>(st.flags + s0);
-    const uint8_t f[4] = {f4.x, f4.y, f4.z, f4.w};
+  __shared__ int32_t list[kBlock / 32][kSweepChunk];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) * 4;
+  if (w0 >= st.n_slots) return;  // whole warps only
+  const int64_t s0 = w0 + (int64_t)lane * 4;
+  uchar4 f4 = make_uchar4(0, 0, 0, 0);
+  if (s0 < st.n_slots) f4 = *reinterpret_cast<const uchar4*>(st.flags + s0);
+  const uint8_t f[4] = {f4.x, f4.y, f4.z, f4.w};
+  const unsigned below = (1u << lane) - 1u;
+  int n = 0;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (s0 + k < st.n_slots && matches(f[k], m)) list[atomicAdd(&n_list, 1)] = (int32_t)(s0 + k);
-    }
+  for (int k = 0; k < 4; ++k) {
+    const bool hit = s0 + k < st.n_slots && matches(f[k], m);
+    const unsigned bits = __ballot_sync(0xffffffffu, hit);
+    if (hit) list[wid][n + __popc(bits & below)] = (int32_t)(s0 + k);
+    n += __popc(bits);
   }
-  __syncthreads();
-  const int n = n_list;
-  for (int q = threadIdx.x; q < n; q += blockDim.x) {
-    const int64_t s = list[q];
-    int r = r_first;
+  __syncwarp();
+  if (n == 0) return;
+  const int r0 = st.chunk_rep[w0 / kSweepChunk];
+  for (int q = lane; q < n; q += 32) {
+    const int64_t s = list[wid][q];
+    int r = r0;
     while (r + 1 < st.n_rep && st.rep_first[r + 1] <= s) ++r;
     body(r, s);
   }
@@ -201,11 +205,11 @@ __device__ __forceinline__ double min_image_sq(double x1, double y1, double x2, 
   return dx * dx + dy * dy;
 }
 
-// float32 separation of two cell-relative points (cells ci, cj).
-__device__ __forceinline__ float rel_sq_f32(int ci, float2 oi, int cj, float2 oj, const Geo& g, float& dx,
-                                            float& dy) {
-  int cxi, cyi, cxj, cyj;
-  split_cell(ci, g, cxi, cyi);
+// float32 separation of two cell-relative points, i in cell (cxi, cyi), j in
+// cell key cj.
+__device__ __forceinline__ float rel_sq_f32_xy(int cxi, int cyi, float2 oi, int cj, float2 oj, const Geo& g,
+                                               float& dx, float& dy) {
+  int cxj, cyj;
   split_cell(cj, g, cxj, cyj);
   int dcx = cxi - cxj, dcy = cyi - cyj;
   if (g.px) {
@@ -219,6 +223,14 @@ __device__ __forceinline__ float rel_sq_f32(int ci, float2 oi, int cj, float2 oj
   dx = (float)dcx * g.sxf + (oi.x - oj.x);
   dy = (float)dcy * g.syf + (oi.y - oj.y);
   return dx * dx + dy * dy;
+}
+
+// float32 separation of two cell-relative points (cells ci, cj).
+__device__ __forceinline__ float rel_sq_f32(int ci, float2 oi, int cj, float2 oj, const Geo& g, float& dx,
+                                            float& dy) {
+  int cxi, cyi;
+  split_cell(ci, g, cxi, cyi);
+  return rel_sq_f32_xy(cxi, cyi, oi, cj, oj, g, dx, dy);
 }
 
 // Squared separation of slots a and b in the given position array.
@@ -248,20 +260,45 @@ __device__ __forceinline__ Tile tile_of(const int2* blk) {
   return t;
 }
 
-// Visit the 3x3 neighbour cells of cell c (dynamics.py:243-260): f(bucket, ordinal, dcx, dcy).
+// Visit the slots of the 3x3 neighbour cells of cell c: f(slot, ordinal,
+// dcx, dcy), ordinal = (dcx + 1) * 3 + (dcy + 1) as in dynamics.py:243-260.
+// The cells of one neighbour column are consecutive sort buckets, so each
+// column is one slot run (two where the column wraps in y); a slot's dcy
+// follows from its bucket (its pre-move cell).
 template <typename F>
-__device__ __forceinline__ void for_neighbour_cells(const Geo& g, int c, F f) {
+__device__ __forceinline__ void for_neighbour_slots(const Geo& g, const DevState& st, int c, F f) {
   int cx, cy;
   split_cell(c, g, cx, cy);
+  int ya0, yb0, ya1 = 0, yb1 = -1;
+  if (cy >= 1 && cy + 1 < g.ny) {
+    ya0 = cy - 1;
+    yb0 = cy + 1;
+  } else if (!g.py) {
+    ya0 = cy > 0 ? cy - 1 : 0;
+    yb0 = cy + 1 < g.ny ? cy + 1 : g.ny - 1;
+  } else if (cy == 0) {
+    ya0 = 0;
+    yb0 = 1;
+    ya1 = yb1 = g.ny - 1;
+  } else {
+    ya0 = g.ny - 2;
+    yb0 = g.ny - 1;
+    ya1 = yb1 = 0;
+  }
   for (int dcx = -1; dcx <= 1; ++dcx) {
     int ncx = cx + dcx;
     if (g.px) ncx = ncx < 0 ? ncx + g.nx : (ncx >= g.nx ? ncx - g.nx : ncx);
     else if (ncx < 0 || ncx >= g.nx) continue;
-    for (int dcy = -1; dcy <= 1; ++dcy) {
-      int ncy = cy + dcy;
-      if (g.py) ncy = ncy < 0 ? ncy + g.ny : (ncy >= g.ny ? ncy - g.ny : ncy);
-      else if (ncy < 0 || ncy >= g.ny) continue;
-      f(g.cbase + (int64_t)ncx * g.ny + ncy, (dcx + 1) * 3 + (dcy + 1), dcx, dcy);
+    const int col = ncx * g.ny;
+    for (int run = 0; run < 2; ++run) {
+      const int ya = run == 0 ? ya0 : ya1, yb = run == 0 ? yb0 : yb1;
+      if (yb < ya) break;
+      const int j0 = st.cell_start[g.cbase + col + ya], j1 = st.cell_start[g.cbase + col + yb + 1];
+      for (int j = j0; j < j1; ++j) {
+        int dcy = st.cell_pre[j] - col - cy;
+        dcy = dcy > 1 ? dcy - g.ny : (dcy < -1 ? dcy + g.ny : dcy);
+        f(j, (dcx + 1) * 3 + (dcy + 1), dcx, dcy);
+      }
     }
   }
 }
@@ -305,8 +342,28 @@ __device__ __forceinline__ void rebucket(const DevState& st, const Geo& g, int f
 // Sort: exclusive scan of the bucket counts, scatter into slots.
 // =============================================================================
 constexpr int kScanThreads = 512;
-constexpr int kScanItems = 8;
+constexpr int kScanItems = 4;  // one int4 per thread: a warp touches 512 contiguous bytes
 constexpr int kScanTile = kScanThreads * kScanItems;
+
+// The kScanItems counts at [base, base + 4) (zero past n); arrays are
+// 16-byte aligned and base is a multiple of 4.
+__device__ __forceinline__ int4 load4(const int32_t* __restrict__ a, int64_t base, int64_t n) {
+  if (base + 3 < n) return *reinterpret_cast<const int4*>(a + base);
+  int4 v = make_int4(0, 0, 0, 0);
+  if (base < n) v.x = a[base];
+  if (base + 1 < n) v.y = a[base + 1];
+  if (base + 2 < n) v.z = a[base + 2];
+  return v;
+}
+__device__ __forceinline__ void store4(int32_t* __restrict__ a, int64_t base, int64_t n, int4 v) {
+  if (base + 3 < n) {
+    *reinterpret_cast<int4*>(a + base) = v;
+    return;
+  }
+  if (base < n) a[base] = v.x;
+  if (base + 1 < n) a[base + 1] = v.y;
+  if (base + 2 < n) a[base + 2] = v.z;
+}
 
 __device__ __forceinline__ int block_exclusive_scan(int v, int& total) {
   __shared__ int warp_sums[32];
@@ -338,10 +395,8 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int& total) {
 
 __global__ void k_scan_reduce(const int32_t* __restrict__ cnt, int64_t n, int32_t* __restrict__ bsum) {
   const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
-  int v = 0;
-#pragma unroll
-  for (int i = 0; i < kScanItems; ++i)
-    if (base + i < n) v += cnt[base + i];
+  const int4 c = load4(cnt, base, n);
+  const int v = c.x + c.y + c.z + c.w;
   int total;
   block_exclusive_scan(v, total);
   if (threadIdx.x == 0) bsum[blockIdx.x] = total;
@@ -362,26 +417,15 @@ __global__ void k_scan_bsum(int32_t* __restrict__ bsum, int nb) {
 __global__ void k_scan_down(int32_t* __restrict__ cnt, int64_t n, const int32_t* __restrict__ bsum,
                             int32_t* __restrict__ start, int32_t* __restrict__ cursor) {
   const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
-  int vals[kScanItems];
-  int v = 0;
-#pragma unroll
-  for (int i = 0; i < kScanItems; ++i) {
-    vals[i] = base + i < n ? cnt[base + i] : 0;
-    v += vals[i];
-  }
+  const int4 c = load4(cnt, base, n);
   int total;
-  int run = block_exclusive_scan(v, total) + bsum[blockIdx.x];
-#pragma unroll
-  for (int i = 0; i < kScanItems; ++i) {
-    if (base + i < n) {
-      start[base + i] = run;
-      cursor[base + i] = run;
-      cnt[base + i] = 0;
-    }
-    run += vals[i];
-  }
+  const int run = block_exclusive_scan(c.x + c.y + c.z + c.w, total) + bsum[blockIdx.x];
+  const int4 st4 = make_int4(run, run + c.x, run + c.x + c.y, run + c.x + c.y + c.z);
+  store4(start, base, n, st4);
+  store4(cursor, base, n, st4);
+  store4(cnt, base, n, make_int4(0, 0, 0, 0));
   // the thread holding element n-1 writes the sentinel start[n]
-  if (base < n && base + kScanItems >= n) start[n] = run;
+  if (base < n && base + kScanItems >= n) start[n] = run + c.x + c.y + c.z + c.w;
   if (n == 0 && blockIdx.x == 0 && threadIdx.x == 0) start[0] = 0;
 }
 
@@ -427,31 +471,30 @@ __device__ __forceinline__ void for_each_force_term(const EdmDynParams& p, const
   // pairs beyond both the pair-list cutoff and every potential's range carry no force
   const double range_sq = p.force_range_sq < g.cutoff_sq ? p.force_range_sq : g.cutoff_sq;
   const float range_sqf = (float)range_sq * 1.0001f;
-  for_neighbour_cells(g, st.cell_pre[s], [&](int64_t nc, int ordinal, int dcx, int dcy) {
-    const int j0 = st.cell_start[nc], j1 = st.cell_start[nc + 1];
-    for (int j = j0; j < j1; ++j) {
-      if (j == s) continue;
+  for_neighbour_slots(g, st, st.cell_pre[s], [&](int j, int ordinal, int dcx, int dcy) {
+    {
+      if (j == s) return;
       double dx, dy, dsq;
       if constexpr (F64) {
         const double2 v = ((const double2*)st.pos_pre)[j];
         dsq = min_image_sq(xi, yi, v.x, v.y, g, dx, dy);
-        if (!(dsq < range_sq)) continue;
+        if (!(dsq < range_sq)) return;
       } else {
         const float2 oj = ((const float2*)st.pos_pre)[j];
         const float fdx = -(float)dcx * g.sxf + (oi.x - oj.x);
         const float fdy = -(float)dcy * g.syf + (oi.y - oj.y);
         const float fdsq = fdx * fdx + fdy * fdy;
-        if (!(fdsq < range_sqf)) continue;
-        if (!((double)fdsq < g.cutoff_sq)) continue;
+        if (!(fdsq < range_sqf)) return;
+        if (!((double)fdsq < g.cutoff_sq)) return;
         dx = fdx;
         dy = fdy;
         dsq = fdsq;
       }
       const uint8_t fj = st.flags[j];
-      if (!fl_alive(fj)) continue;
+      if (!fl_alive(fj)) return;
       const int spj = fl_species(fj);
       const double sig = p.sigma[sp * EDM_MAX_SPECIES + spj];
-      if (!(sig > 0.0)) continue;
+      if (!(sig > 0.0)) return;
       const int idj = st.ids[j] - (int)g.poff;
       const uint64_t order = idj < id ? (uint64_t)idj
                                       : ((1ull << 60) | ((uint64_t)ordinal << 32) | (uint64_t)(0xFFFFFFFFu - (uint32_t)idj));
@@ -620,10 +663,10 @@ __global__ void __launch_bounds__(kBlock) k_move(const EdmDynParams* __restrict_
   abs_pos<F64>(st.pos_pre, st.cell_pre, s, g, x, y);
   double Di, gDx, gDy;
   dfield(p, sp, x, y, Di, gDx, gDy);
-  const U2 z = normal2(p.seed, step, EDM_S_BD_NORMAL, (uint64_t)id);
   const double dt = p.dt;
   int newc;
   if constexpr (F64) {
+    const U2 z = normal2(p.seed, step, EDM_S_BD_NORMAL, (uint64_t)id);
     const double sn = sqrt(2.0 * Di * dt);
     double dxt = gDx * dt, dyt = gDy * dt;
     dxt += sn * z.u0;
@@ -648,10 +691,12 @@ __global__ void __launch_bounds__(kBlock) k_move(const EdmDynParams* __restrict_
     ((double2*)st.pos_post)[s] = make_double2(x, y);
     newc = cell_index(x, g.sx, g.nx) * g.ny + cell_index(y, g.sy, g.ny);
   } else {
+    float z0, z1;
+    normal2_f32(p.seed, step, EDM_S_BD_NORMAL, (uint64_t)id, z0, z1);
     const float Dif = (float)Di, dtf = (float)dt;
     const float sn = sqrtf(2.0f * Dif * dtf);
-    float dxt = (float)gDx * dtf + sn * (float)z.u0 + Dif * (float)Fx * dtf;
-    float dyt = (float)gDy * dtf + sn * (float)z.u1 + Dif * (float)Fy * dtf;
+    float dxt = (float)gDx * dtf + sn * z0 + Dif * (float)Fx * dtf;
+    float dyt = (float)gDy * dtf + sn * z1 + Dif * (float)Fy * dtf;
     const float dr2 = dxt * dxt + dyt * dyt;
     if ((double)dr2 > p.max_disp_sq) {
       const float scale = (float)p.max_disp / sqrtf(dr2);
@@ -722,22 +767,39 @@ __global__ void __launch_bounds__(kBlock) k_contacts(const EdmDynParams* __restr
   sweep4(st, m, [&](int r, int64_t s) {
     const EdmDynParams& p = P[r];
     const Geo g(p);
-    for_neighbour_cells(g, st.cell_pre[s], [&](int64_t nc, int, int, int) {
-      const int j0 = st.cell_start[nc], j1 = st.cell_start[nc + 1];
-      for (int j = j0; j < j1; ++j) {
-        if (j == s) continue;
-        const uint8_t fj = st.flags[j];
-        if (!fl_alive(fj) || !((partner_mask >> fl_species(fj)) & 1u)) continue;
-        if (!(sep_sq<F64>(st.pos_pre, st.cell_pre, s, j, g) < g.cutoff_sq)) continue;
-        if (sep_sq<F64>(st.pos_post, st.cell_post, s, j, g) > contact_sq) continue;
-        const int k = atomicAdd(&nbuf, 1);
-        if (k < kContactSmem) {
-          buf[k] = make_int2((int)s, j);
-        } else {  // shared buffer full: append directly
-          const int q = atomicAdd(st.contact_count, 1);
-          if (q < st.contact_cap) st.contacts[q] = make_int2((int)s, j);
-          else set_status(st.status, EDM_STATUS_BIND_CAP);
-        }
+    // this particle's pre- and post-move points (float32: offsets + post cell)
+    float2 oi_pre = make_float2(0.f, 0.f), oi_post = make_float2(0.f, 0.f);
+    int cxs = 0, cys = 0;
+    if constexpr (!F64) {
+      oi_pre = ((const float2*)st.pos_pre)[s];
+      oi_post = ((const float2*)st.pos_post)[s];
+      split_cell(st.cell_post[s], g, cxs, cys);
+    }
+    for_neighbour_slots(g, st, st.cell_pre[s], [&](int j, int, int dcx, int dcy) {
+      if (j == s) return;
+      const uint8_t fj = st.flags[j];
+      if (!fl_alive(fj) || !((partner_mask >> fl_species(fj)) & 1u)) return;
+      if constexpr (F64) {
+        if (!(sep_sq<F64>(st.pos_pre, st.cell_pre, s, j, g) < g.cutoff_sq)) return;
+        if (sep_sq<F64>(st.pos_post, st.cell_post, s, j, g) > contact_sq) return;
+      } else {
+        // pre-move: j sits in the neighbour cell at (dcx, dcy)
+        const float2 oj = ((const float2*)st.pos_pre)[j];
+        const float fdx = -(float)dcx * g.sxf + (oi_pre.x - oj.x);
+        const float fdy = -(float)dcy * g.syf + (oi_pre.y - oj.y);
+        if (!((double)(fdx * fdx + fdy * fdy) < g.cutoff_sq)) return;
+        float dx, dy;
+        if ((double)rel_sq_f32_xy(cxs, cys, oi_post, st.cell_post[j], ((const float2*)st.pos_post)[j], g, dx, dy) >
+            contact_sq)
+          return;
+      }
+      const int k = atomicAdd(&nbuf, 1);
+      if (k < kContactSmem) {
+        buf[k] = make_int2((int)s, j);
+      } else {  // shared buffer full: append directly
+        const int q = atomicAdd(st.contact_count, 1);
+        if (q < st.contact_cap) st.contacts[q] = make_int2((int)s, j);
+        else set_status(st.status, EDM_STATUS_BIND_CAP);
       }
     });
   });
@@ -920,14 +982,13 @@ __global__ void __launch_bounds__(kBlock) k_bind_candidates(const EdmDynParams* 
     const int id = st.ids[s] - (int)g.poff;
     if (st.bond[g.poff + id] >= 0) return;
     const int64_t step = *st.d_step;
-    for_neighbour_cells(g, st.cell_pre[s], [&](int64_t nc, int ordinal, int, int) {
-      const int j0 = st.cell_start[nc], j1 = st.cell_start[nc + 1];
-      for (int j = j0; j < j1; ++j) {
+    for_neighbour_slots(g, st, st.cell_pre[s], [&](int j, int ordinal, int, int) {
+      {
         const int idj = st.ids[j] - (int)g.poff;
-        if (idj <= id) continue;
+        if (idj <= id) return;
         const uint8_t fj = st.flags[j];
-        if (!fl_alive(fj)) continue;
-        if (st.bond[g.poff + idj] >= 0) continue;
+        if (!fl_alive(fj)) return;
+        if (st.bond[g.poff + idj] >= 0) return;
         const int spj = fl_species(fj);
         int a, bb;
         if (spi == B.ra && spj == B.rb) {
@@ -937,12 +998,12 @@ __global__ void __launch_bounds__(kBlock) k_bind_candidates(const EdmDynParams* 
           a = idj;
           bb = id;
         } else {
-          continue;
+          return;
         }
-        if (!(sep_sq<F64>(st.pos_pre, st.cell_pre, s, j, g) < g.cutoff_sq)) continue;
-        if (sep_sq<F64>(st.pos_post, st.cell_post, s, j, g) > B.contact_sq) continue;
+        if (!(sep_sq<F64>(st.pos_pre, st.cell_pre, s, j, g) < g.cutoff_sq)) return;
+        if (sep_sq<F64>(st.pos_post, st.cell_post, s, j, g) > B.contact_sq) return;
         const double u = uniform1(p.seed, step, EDM_S_BIND + 2 * b, (uint64_t)id, (uint64_t)idj);
-        if (!(u < B.prob_bind)) continue;
+        if (!(u < B.prob_bind)) return;
         const int k = atomicAdd(&st.bind_count[r], 1);
         if (k < kBindCap) {
           st.bind_key[(int64_t)r * kBindCap + k] =

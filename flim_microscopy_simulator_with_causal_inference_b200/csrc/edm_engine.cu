@@ -118,6 +118,7 @@ struct EdmEngine {
   uint32_t enzyme_mask = 0, partner_mask = 0;
   double contact_sq_max = 0.0;
   int64_t* rep_first = nullptr;
+  int32_t* chunk_rep = nullptr;  // replica of the first slot of each 128-slot chunk
   std::vector<int32_t> emit_host;  // emitter list last uploaded
   std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;
   std::vector<void*> allocs;
@@ -153,6 +154,7 @@ struct EdmEngine {
     s.contact_count = contact_count;
     s.contact_cap = contact_cap;
     s.rep_first = rep_first;
+    s.chunk_rep = chunk_rep;
     s.n_rep = R;
     s.n_slots = N;
     return s;
@@ -525,6 +527,15 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
     std::vector<int64_t> rf(pfirst);
     rf.push_back(np);
     CUDA_TRY(cudaMemcpy(E->rep_first, rf.data(), sizeof(int64_t) * rf.size(), cudaMemcpyHostToDevice));
+    const int64_t nchunks = (np + kSweepChunk - 1) / kSweepChunk;
+    std::vector<int32_t> cr((size_t)std::max<int64_t>(1, nchunks), 0);
+    int r = 0;
+    for (int64_t c = 0; c < nchunks; ++c) {
+      while (r + 1 < n_replicas && rf[r + 1] <= c * kSweepChunk) ++r;
+      cr[(size_t)c] = r;
+    }
+    ALLOC(E->chunk_rep, cr.size());
+    CUDA_TRY(cudaMemcpy(E->chunk_rep, cr.data(), sizeof(int32_t) * cr.size(), cudaMemcpyHostToDevice));
   }
   std::vector<int2> pt = tiles(pfirst, pcount);
   E->npblk = (int)pt.size();

@@ -13,12 +13,14 @@
 //      for emitters at pixel centres.  It runs as two tcgen05 BF16 GEMMs with
 //      FP32 accumulation in tensor memory; G and the intermediate product are
 //      split into BF16 hi + lo parts so the projection keeps ~17 bits;
-//   3. histogram writer: the Poisson mean of pixel p, bin b is
+//   3. histogram writer: the count of pixel p, bin b is Poisson with mean
 //      I_free[p] h_free[b] yield_free + I_bound[p] h_bound[b] yield_bound,
 //      h the bin probabilities of an exponential decay convolved with the
 //      Gaussian IRF, negative times folded into bin 0 and times past the last
 //      bin lost (the TCSPC rule of microscope.py:716-803), in float64.  The
-//      expected mean arrival time of each pixel is accumulated in float64.
+//      counts are drawn as Poisson in-window totals per component followed
+//      by alias-table photons.  The expected mean arrival time of each pixel
+//      follows in float64 from its two intensities and the bin sums.
 // Photon yields and lifetimes are host inputs (the reference's per-pulse
 // chain, photophysics.py:218-331).  This path has no reference counterpart:
 // the reference only has the photon-by-photon microscope (edm_phot.cuh).
@@ -26,6 +28,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -253,14 +256,65 @@ __device__ double exgauss_sf(double t, double tau, double s) {
   return 0.5 * erfc(a * r2) + exp(-t / tau + 0.5 * (s / tau) * (s / tau)) * 0.5 * erfc(-g * r2);
 }
 
-__global__ void k_bins(EdmFlimParams p, double* h /*[2][n_bins]*/) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= p.n_bins) return;
+// h[c][b] (float64), the sums S_c = sum_b h[c][b] yield_c (expected in-window
+// photons per unit intensity) and T_c = sum_b t_b h[c][b] yield_c with t_b the
+// bin centre, so that a pixel's expected mean arrival time is
+// (A T_free + B T_bound) / (A S_free + B S_bound), and the alias tables of
+// h[c][.] / sum h[c][.].  One block of 256 threads.
+__global__ void k_bins(EdmFlimParams p, double* h /*[2][n_bins]*/,
+                       double* sums /*[T_free, S_free, T_bound, S_bound]*/, int2* alias /*[2][n_bins]*/) {
+  __shared__ double ts[256], ss[256], q[256];
+  __shared__ int small[256], large[256];
+  const int b = threadIdx.x;
   const double w = p.bin_width_ns, s = p.sigma_irf_ns;
   for (int c = 0; c < 2; ++c) {
     const double tau = c == 0 ? p.tau_free_ns : p.tau_bound_ns;
-    const double lo = b == 0 ? 1.0 : exgauss_sf(b * w, tau, s);  // bin 0 takes every negative time
-    h[c * p.n_bins + b] = lo - exgauss_sf((b + 1) * w, tau, s);
+    const double y = c == 0 ? p.yield_free : p.yield_bound;
+    double v = 0.0;
+    if (b < p.n_bins) {
+      const double lo = b == 0 ? 1.0 : exgauss_sf(b * w, tau, s);  // bin 0 takes every negative time
+      v = lo - exgauss_sf((b + 1) * w, tau, s);
+      h[c * p.n_bins + b] = v;
+    }
+    ts[b] = (b + 0.5) * w * v * y;
+    ss[b] = v * y;
+    __syncthreads();
+    if (b == 0) {
+      double T = 0.0, S = 0.0;
+      for (int i = 0; i < p.n_bins; ++i) {
+        T += ts[i];
+        S += ss[i];
+      }
+      sums[2 * c] = T;
+      sums[2 * c + 1] = S;
+      // Alias table of the in-window bin distribution ss[i] / S (Vose's
+      // method, M. D. Vose, IEEE Trans. Softw. Eng. 17 (1991) 972-975):
+      // cell i keeps bin i with probability thr / 2^24, else gives `alias`.
+      const int n = p.n_bins;
+      int ns = 0, nl = 0;
+      for (int i = 0; i < n; ++i) {
+        q[i] = S > 0.0 ? ss[i] / S * n : 1.0;
+        if (q[i] < 1.0) small[ns++] = i;
+        else large[nl++] = i;
+      }
+      int2* tab = alias + c * n;
+      while (ns > 0 && nl > 0) {
+        const int l = small[--ns], g = large[--nl];
+        tab[l] = make_int2((int)fmin(16777216.0, rint(q[l] * 16777216.0)), g);
+        q[g] = (q[g] + q[l]) - 1.0;
+        if (q[g] < 1.0) small[ns++] = g;
+        else large[nl++] = g;
+      }
+      while (nl > 0) {
+        const int g = large[--nl];
+        tab[g] = make_int2(16777216, g);
+      }
+      while (ns > 0) {  // leftovers of rounding: probability one
+        const int l = small[--ns];
+        tab[l] = make_int2(16777216, l);
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -319,94 +373,178 @@ __global__ void k_band(EdmFlimParams p, __nv_bfloat16* g1, __nv_bfloat16* a2) {
 // ----------------------------------------------------------------------------
 // histogram writer: one warp per pixel, lane l owns bins b0 + l + 32 k
 // ----------------------------------------------------------------------------
-__device__ __forceinline__ float u24(uint32_t w) { return ((float)(w >> 8) + 0.5f) * (1.0f / 16777216.0f); }
+// SplitMix64 output function (G. Steele, D. Lea, C. Flood, "Fast splittable
+// pseudorandom number generators", OOPSLA 2014): a bijective 64-bit mixer.
+__device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// Per-lane uniform stream: xoshiro128** (D. Blackman, S. Vigna, "Scrambled
+// linear pseudorandom number generators", ACM TOMS 47 (2021)) seeded, as its
+// authors recommend, with SplitMix64 outputs of a key unique to (acquisition
+// seed, replica, pixel, lane), so every lane of every pixel has its own
+// reproducible stream.
+struct LaneRng {
+  uint32_t s0, s1, s2, s3;
+  __device__ __forceinline__ LaneRng(uint64_t seed, uint32_t r, uint32_t px, uint32_t lane) {
+    // distinct keys give distinct SplitMix64 inputs: odd and even multiples
+    // of the (odd) increment, one pair per key
+    const uint64_t key = ((uint64_t)r << 32) | ((uint64_t)px << 8) | lane;
+    const uint64_t z0 = seed + 0x9E3779B97F4A7C15ull * (2 * key + 1);
+    const uint64_t a = splitmix64(z0), b = splitmix64(z0 + 0x9E3779B97F4A7C15ull);
+    s0 = (uint32_t)a;
+    s1 = (uint32_t)(a >> 32);
+    s2 = (uint32_t)b;
+    s3 = (uint32_t)(b >> 32) | ((a | b) == 0ull ? 1u : 0u);  // the all-zero state is the one fixed point
+  }
+  __device__ __forceinline__ uint32_t next() {
+    const uint32_t out = __funnelshift_l(s1 * 5u, s1 * 5u, 7) * 9u;
+    const uint32_t t = s1 << 9;
+    s2 ^= s0;
+    s3 ^= s1;
+    s1 ^= s2;
+    s0 ^= s3;
+    s2 ^= t;
+    s3 = __funnelshift_l(s3, s3, 11);
+    return out;
+  }
+  // uniform in (0, 1) with 24 bits
+  __device__ __forceinline__ float uniform() { return ((float)(next() >> 8) + 0.5f) * (1.0f / 16777216.0f); }
+};
+
+// Lane 0's stream seen by the whole warp (warp-uniform draws).
+struct WarpRng {
+  LaneRng& lane_rng;
+  __device__ __forceinline__ uint32_t next() { return __shfl_sync(0xffffffffu, lane_rng.next(), 0); }
+  __device__ __forceinline__ float uniform() { return ((float)(next() >> 8) + 0.5f) * (1.0f / 16777216.0f); }
+};
 
 // Poisson(mu) for mu < 10 by sequential inversion of the CDF with one
 // uniform; the search stops at mu + 12 sqrt(mu) + 12, where the FP32 CDF no
 // longer resolves the tail mass left.
 __device__ __forceinline__ uint32_t poisson_small(float mu, float u) {
   if (mu <= 0.0f) return 0u;
-  const uint32_t kmax = (uint32_t)(mu + 12.0f * sqrtf(mu) + 12.0f);
-  float pk = __expf(-mu), F = pk;
-  uint32_t k = 0;
+  const float kmax = floorf(mu + 12.0f * sqrtf(mu) + 12.0f);
+  float pk = __expf(-mu), F = pk, k = 0.0f;
   while (u > F && k < kmax) {
-    ++k;
-    pk *= __fdividef(mu, (float)k);
+    k += 1.0f;
+    pk *= __fdividef(mu, k);
     F += pk;
   }
-  return k;
+  return (uint32_t)k;
 }
 
 // Poisson(mu) for mu >= 10: transformed rejection with squeeze (PTRS,
-// W. Hoermann, Insurance: Mathematics and Economics 12 (1993) 39-45).  Each
-// attempt takes two 32-bit uniforms from its own Philox block.
-__device__ __forceinline__ uint32_t poisson_ptrs(float mu, uint64_t seed, uint32_t c0, uint32_t bin, uint32_t c2) {
+// W. Hoermann, Insurance: Mathematics and Economics 12 (1993) 39-45), two
+// uniforms per attempt from the lane's stream.
+template <typename Rng>
+__device__ __forceinline__ uint32_t poisson_ptrs(float mu, Rng& rng) {
   const float smu = sqrtf(mu);
   const float b = 0.931f + 2.53f * smu;
   const float a = -0.059f + 0.02483f * b;
-  const float inv_alpha = 1.1239f + 1.1328f / (b - 3.4f);
-  const float vr = 0.9277f - 3.6224f / (b - 2.0f);
+  const float inv_alpha = 1.1239f + __fdividef(1.1328f, b - 3.4f);
+  const float vr = 0.9277f - __fdividef(3.6224f, b - 2.0f);
   const float log_mu = __logf(mu);
-  for (uint32_t attempt = 0; attempt < 64u; ++attempt) {
-    uint32_t w0 = c0, w1 = bin | (attempt << 16), w2 = c2, w3 = 203u << 16;
-    edm::philox10(w0, w1, w2, w3, (uint32_t)seed, (uint32_t)(seed >> 32));
-    const float U = ((float)(w0 >> 8) + 0.5f) * (1.0f / 16777216.0f) - 0.5f;
-    const float V = ((float)(w1 >> 8) + 0.5f) * (1.0f / 16777216.0f);
+  for (int attempt = 0; attempt < 64; ++attempt) {
+    const float U = rng.uniform() - 0.5f;
+    const float V = rng.uniform();
     const float us = 0.5f - fabsf(U);
-    const float kf = floorf((2.0f * a / us + b) * U + mu + 0.43f);
+    const float kf = floorf((__fdividef(2.0f * a, us) + b) * U + mu + 0.43f);
     if (us >= 0.07f && V <= vr) return (uint32_t)kf;
     if (kf < 0.0f || (us < 0.013f && V > us)) continue;
-    const float lhs = __logf(V) + __logf(inv_alpha) - __logf(a / (us * us) + b);
+    const float lhs = __logf(V) + __logf(inv_alpha) - __logf(__fdividef(a, us * us) + b);
     const float rhs = -mu + kf * log_mu - lgammaf(kf + 1.0f);
     if (lhs <= rhs) return (uint32_t)kf;
   }
   return (uint32_t)(mu + 0.5f);  // 64 rejections in a row: not reached in practice
 }
 
-__global__ void __launch_bounds__(256) k_hist(EdmFlimParams p, const float* I /*[R][2][256*256]*/,
-                                              const double* h, uint32_t* hist,
-                                              double* tau_expected /*[R][256*256], may be null*/) {
-  __shared__ float hf[256], hb[256];
-  __shared__ double tmid[256];
-  for (int b = threadIdx.x; b < p.n_bins; b += blockDim.x) {
-    hf[b] = (float)(h[b] * p.yield_free);
-    hb[b] = (float)(h[p.n_bins + b] * p.yield_bound);
-    tmid[b] = (b + 0.5) * p.bin_width_ns;
-  }
+// Poisson(mu) of any mean: inversion below 10, PTRS above.
+template <typename Rng>
+__device__ __forceinline__ uint32_t poisson(float mu, Rng& rng) {
+  return mu < 10.0f ? poisson_small(mu, rng.uniform()) : poisson_ptrs(mu, rng);
+}
+
+// One warp per pixel (grid-stride).  The counts n_b ~ Poisson(mu_b),
+// mu_b = A h_free[b] y_free + B h_bound[b] y_bound, are drawn through the
+// identity "Poisson total, then independent categorical photons": per
+// component c the in-window total N_c ~ Poisson(A_c S_c) (drawn identically
+// by all lanes from lane 0's stream), then each of the
+// N_free + N_bound photons picks its bin from the component's alias table
+// with one 32-bit word of its lane's stream.  Photons are counted in
+// kSub shared-memory copies of the warp's histogram (lane % kSub), four per
+// lane per round so table loads and atomics overlap; the copies are summed
+// into 512-byte coalesced stores.
+constexpr int kSub = 1;
+
+__global__ void __launch_bounds__(256, 4) k_hist(EdmFlimParams p, const float* __restrict__ I /*[R][2][256*256]*/,
+                                                 const int2* __restrict__ alias, const double* __restrict__ sums,
+                                                 uint32_t* __restrict__ hist, double* __restrict__ tau_expected) {
+  __shared__ int2 tab[2][256];
+  __shared__ __align__(16) uint32_t wh[8][kSub][256];
+  const int nb = p.n_bins;
+  for (int i = threadIdx.x; i < 2 * nb; i += blockDim.x) tab[i / nb][i % nb] = alias[i];
   __syncthreads();
+  const double Tf = sums[0], Sf = sums[1], Tb = sums[2], Sb = sums[3];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const size_t npx = (size_t)kDim * kDim;
-  const size_t gpx = (size_t)blockIdx.x * (blockDim.x >> 5) + warp;  // pixel over all replicas
-  if (gpx >= npx * (size_t)p.n_replicas) return;
-  const uint32_t r = (uint32_t)(gpx / npx);
-  const uint32_t px = (uint32_t)(gpx - (size_t)r * npx);
-  const float i_free = I[((size_t)r * 2 + 0) * npx + px];
-  const float i_bound = I[((size_t)r * 2 + 1) * npx + px];
-  const uint64_t seed = edm_flim_replica_seed(p.seed, (int32_t)r);
-  uint32_t* out = hist + gpx * (size_t)p.n_bins;
-  double num = 0.0, den = 0.0;
-  for (int b0 = 0; b0 < p.n_bins; b0 += 128) {
-    uint32_t w0 = px, w1 = (uint32_t)(b0 + lane), w2 = r, w3 = 202u << 16;
-    edm::philox10(w0, w1, w2, w3, (uint32_t)seed, (uint32_t)(seed >> 32));
-    const uint32_t words[4] = {w0, w1, w2, w3};
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int b = b0 + lane + 32 * k;
-      const float mu = i_free * hf[b] + i_bound * hb[b];
-      const uint32_t n =
-          mu < 10.0f ? poisson_small(mu, u24(words[k])) : poisson_ptrs(mu, seed, px, (uint32_t)b, r);
-      out[b] = n;
-      num += tmid[b] * (double)mu;
-      den += (double)mu;
+  const int shift = nb == 256 ? 24 : 25;  // top bits of a word pick the cell
+  uint32_t* h = wh[warp][lane % kSub];
+  const uint32_t npx = (uint32_t)kDim * kDim;
+  const size_t total = (size_t)npx * (size_t)p.n_replicas;
+  for (size_t gpx = (size_t)blockIdx.x * 8 + warp; gpx < total; gpx += (size_t)gridDim.x * 8) {
+    const uint32_t r = (uint32_t)(gpx / npx);
+    const uint32_t px = (uint32_t)(gpx - (size_t)r * npx);
+    const float A = I[((size_t)r * 2 + 0) * npx + px];
+    const float B = I[((size_t)r * 2 + 1) * npx + px];
+    const uint64_t seed = edm_flim_replica_seed(p.seed, (int32_t)r);
+    LaneRng rng(seed, r, px, (uint32_t)lane);
+    WarpRng pixel_rng{rng};  // the totals: lane 0's first draws, in every lane
+    const int n_free = (int)poisson(fmaxf(0.0f, A) * (float)Sf, pixel_rng);
+    const int n_all = n_free + (int)poisson(fmaxf(0.0f, B) * (float)Sb, pixel_rng);
+    {
+      uint4* z = (uint4*)wh[warp];
+      for (int i = lane; i < kSub * nb / 4; i += 32) z[i] = make_uint4(0u, 0u, 0u, 0u);
     }
-  }
-  if (tau_expected) {
+    __syncwarp();
+    // photons lane, lane + 32, ...: four per round
+    int i = lane;
+    for (; i + 96 < n_all; i += 128) {
+      uint32_t w[4];
+      int2 e[4];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      num += __shfl_xor_sync(0xffffffffu, num, o);
-      den += __shfl_xor_sync(0xffffffffu, den, o);
+      for (int k = 0; k < 4; ++k) w[k] = rng.next();
+#pragma unroll
+      for (int k = 0; k < 4; ++k) e[k] = tab[i + 32 * k < n_free ? 0 : 1][w[k] >> shift];
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        atomicAdd(&h[(int)(w[k] & 0xFFFFFFu) < e[k].x ? (int)(w[k] >> shift) : e[k].y], 1u);
     }
-    if (lane == 0) tau_expected[gpx] = den > 0.0 ? num / den : 0.0;
+    for (; i < n_all; i += 32) {
+      const uint32_t w = rng.next();
+      const int2 e = tab[i < n_free ? 0 : 1][w >> shift];
+      atomicAdd(&h[(int)(w & 0xFFFFFFu) < e.x ? (int)(w >> shift) : e.y], 1u);
+    }
+    __syncwarp();
+    uint4* out = (uint4*)(hist + gpx * (size_t)nb);
+    for (int q = lane; q < nb / 4; q += 32) {
+      uint4 v = ((const uint4*)wh[warp][0])[q];
+#pragma unroll
+      for (int c = 1; c < kSub; ++c) {
+        const uint4 u = ((const uint4*)wh[warp][c])[q];
+        v.x += u.x;
+        v.y += u.y;
+        v.z += u.z;
+        v.w += u.w;
+      }
+      out[q] = v;
+    }
+    __syncwarp();
+    if (tau_expected != nullptr && lane == 0) {
+      const double den = (double)A * Sf + (double)B * Sb;
+      tau_expected[gpx] = den > 0.0 ? ((double)A * Tf + (double)B * Tb) / den : 0.0;
+    }
   }
 }
 
@@ -445,10 +583,12 @@ struct EdmFlim {
   int32_t* counts = nullptr;
   __nv_bfloat16 *maps = nullptr, *g1 = nullptr, *a2 = nullptr, *b2 = nullptr;
   float* I = nullptr;
-  double *h = nullptr, *tau = nullptr;
+  double *h = nullptr, *tau = nullptr, *sums = nullptr;
+  int2* alias = nullptr;
   uint32_t* hist = nullptr;
   uint32_t* err = nullptr;
   CUtensorMap mA1, mB1, mA2, mB2;
+  int hist_blocks = 148;  // resident k_hist blocks on this device (grid of the grid-stride loop)
   std::vector<void*> allocs;
   ~EdmFlim() {
     for (void* a : allocs) cudaFree(a);
@@ -505,6 +645,8 @@ int edm_flim_create(const EdmFlimParams* params, int32_t device, EdmFlim** out) 
   FA(F->b2, R * 2 * kDim * kK2);
   FA(F->I, R * 2 * npx);
   FA(F->h, 2 * (size_t)params->n_bins);
+  FA(F->sums, 4);
+  FA(F->alias, 2 * (size_t)params->n_bins);
   FA(F->tau, R * npx);
   FA(F->hist, R * npx * params->n_bins);
   FA(F->err, 1);
@@ -518,7 +660,13 @@ int edm_flim_create(const EdmFlimParams* params, int32_t device, EdmFlim** out) 
   }
   cudaError_t e = cudaFuncSetAttribute(k_umma_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
   if (e == cudaSuccess) {
-    k_bins<<<(params->n_bins + 127) / 128, 128>>>(*params, F->h);
+    int sms = 0, per_sm = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hist, 256, 0);
+    if (e == cudaSuccess) F->hist_blocks = std::max(1, sms * std::max(1, per_sm));
+  }
+  if (e == cudaSuccess) {
+    k_bins<<<1, 256>>>(*params, F->h, F->sums, F->alias);
     k_band<<<kDim, kDim>>>(*params, F->g1, F->a2);
     e = cudaGetLastError();
   }
@@ -580,8 +728,8 @@ int edm_flim_histograms(EdmFlim* F, int32_t with_tau, void* stream) {
   FL_TRY(cudaSetDevice(F->device));
   const EdmFlimParams& p = F->p;
   const size_t total_px = (size_t)p.n_replicas * kDim * kDim;
-  const unsigned blocks = (unsigned)((total_px + 7) / 8);
-  k_hist<<<blocks, 256, 0, (cudaStream_t)stream>>>(p, F->I, F->h, F->hist, with_tau ? F->tau : nullptr);
+  const unsigned blocks = (unsigned)std::min<size_t>((total_px + 7) / 8, (size_t)F->hist_blocks);
+  k_hist<<<blocks, 256, 0, (cudaStream_t)stream>>>(p, F->I, F->alias, F->sums, F->hist, with_tau ? F->tau : nullptr);
   FL_TRY(cudaGetLastError());
   return EDM_OK;
 }

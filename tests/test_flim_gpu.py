@@ -84,8 +84,9 @@ def test_histogram_bin_totals(acq, ref):
 
 @pytest.mark.parametrize("branch", ["inversion", "rejection"])
 def test_poisson_dispersion_per_sampler_branch(acq, ref, branch):
-    """mu < 10 uses CDF inversion, mu >= 10 the transformed rejection; both
-    must give mean mu and variance mu."""
+    """Bins of small (< 10) and large means: counts must have mean mu and
+    variance mu in both (the per-component totals use inversion below a
+    mean of 10 and transformed rejection above)."""
     num = den = 0.0
     n_cells = 0
     chi = 0.0
@@ -127,3 +128,16 @@ def test_acquisition_is_deterministic(acq):
     a.acquire()
     other = a.read(FA.HIST, replica=2)
     assert not np.array_equal(other, acq["hist"][2])
+
+
+def test_pixel_totals_are_poisson(acq, ref):
+    """Per-pixel photon totals (the per-component Poisson totals summed):
+    mean and variance equal to the float64 expected total."""
+    for r in range(R):
+        lam = ref[r]["mu"].sum(axis=-1)
+        n = acq["hist"][r].astype(np.float64).sum(axis=-1)
+        m = lam > 1.0
+        d = n[m] - lam[m]
+        assert abs(d.sum()) / math.sqrt(lam[m].sum()) < 6.0
+        disp = float(((d ** 2) / lam[m]).mean())
+        assert abs(disp - 1.0) < 6.0 * math.sqrt(3.0 / m.sum()), (r, disp)
