@@ -65,8 +65,8 @@ struct DevState {
   int32_t* bind_ab;      // [R][kBindCap][2] local ids (a = reactant A role, b = B role)
   // catalytic contacts of the step: (enzyme slot, substrate-capable slot)
   int2* contacts;
-  int32_t* contact_count;
-  int64_t contact_cap;
+  int32_t* contact_count;  // [EDM_MAX_CAT]
+  int64_t contact_cap;      // per catalytic reaction
   const int64_t* rep_first;  // [R + 1] first slot of each replica
   const int32_t* chunk_rep;  // replica of the first slot of each kSweepChunk-slot chunk
   int n_rep;
@@ -753,20 +753,34 @@ __global__ void __launch_bounds__(kBlock) k_move(const EdmDynParams* __restrict_
 // Catalytic contacts (pairs of the reference's pre-move pair list, dynamics.py
 // :219-278, in post-move contact): enzyme-capable alive particles sweep their
 // neighbour cells once per step, after the binding passes.  During the
-// catalytic passes enzymes keep their species and nobody moves or dies, so
-// every pass of the step reads this list instead of sweeping again.
+// catalytic passes enzymes keep their species and nobody moves or dies, so a
+// pair (enzyme s, partner j) is filed once, in the list of every catalytic
+// reaction c whose enzyme is s's species, when j's species can be c's
+// substrate by the time pass c runs (its substrate, or a species earlier
+// passes convert into it) and the pair is within c's contact radius.  Pass c
+// then reads only its own list.
 constexpr int kContactSmem = 2048;
+
+struct CatLists {
+  uint32_t capable[EDM_MAX_CAT];          // species that can be substrate of c at pass c
+  uint32_t reactions_of[EDM_MAX_SPECIES];  // reactions whose enzyme is the species
+  uint32_t partners_of[EDM_MAX_SPECIES];   // union of capable[c] over those reactions
+  int n_cat;
+};
 
 template <bool F64>
 __global__ void __launch_bounds__(kBlock) k_contacts(const EdmDynParams* __restrict__ P, DevState st, Match m,
-                                                     uint32_t partner_mask, double contact_sq) {
+                                                     CatLists L) {
   __shared__ int2 buf[kContactSmem];
-  __shared__ int nbuf, base;
-  if (threadIdx.x == 0) nbuf = 0;
+  __shared__ int nbuf[EDM_MAX_CAT], base[EDM_MAX_CAT];
+  const int per = L.n_cat > 0 ? kContactSmem / L.n_cat : kContactSmem;  // staging slots per reaction
+  if (threadIdx.x < EDM_MAX_CAT) nbuf[threadIdx.x] = 0;
   __syncthreads();
   sweep4(st, m, [&](int r, int64_t s) {
     const EdmDynParams& p = P[r];
     const Geo g(p);
+    const int sps = fl_species(st.flags[s]);
+    const uint32_t rmask = L.reactions_of[sps], pmask = L.partners_of[sps];
     // this particle's pre- and post-move points (float32: offsets + post cell)
     float2 oi_pre = make_float2(0.f, 0.f), oi_post = make_float2(0.f, 0.f);
     int cxs = 0, cys = 0;
@@ -778,10 +792,12 @@ __global__ void __launch_bounds__(kBlock) k_contacts(const EdmDynParams* __restr
     for_neighbour_slots(g, st, st.cell_pre[s], [&](int j, int, int dcx, int dcy) {
       if (j == s) return;
       const uint8_t fj = st.flags[j];
-      if (!fl_alive(fj) || !((partner_mask >> fl_species(fj)) & 1u)) return;
+      const int spj = fl_species(fj);
+      if (!fl_alive(fj) || !((pmask >> spj) & 1u)) return;
+      double d2;
       if constexpr (F64) {
         if (!(sep_sq<F64>(st.pos_pre, st.cell_pre, s, j, g) < g.cutoff_sq)) return;
-        if (sep_sq<F64>(st.pos_post, st.cell_post, s, j, g) > contact_sq) return;
+        d2 = sep_sq<F64>(st.pos_post, st.cell_post, s, j, g);
       } else {
         // pre-move: j sits in the neighbour cell at (dcx, dcy)
         const float2 oj = ((const float2*)st.pos_pre)[j];
@@ -789,47 +805,56 @@ __global__ void __launch_bounds__(kBlock) k_contacts(const EdmDynParams* __restr
         const float fdy = -(float)dcy * g.syf + (oi_pre.y - oj.y);
         if (!((double)(fdx * fdx + fdy * fdy) < g.cutoff_sq)) return;
         float dx, dy;
-        if ((double)rel_sq_f32_xy(cxs, cys, oi_post, st.cell_post[j], ((const float2*)st.pos_post)[j], g, dx, dy) >
-            contact_sq)
-          return;
+        d2 = (double)rel_sq_f32_xy(cxs, cys, oi_post, st.cell_post[j], ((const float2*)st.pos_post)[j], g, dx, dy);
       }
-      const int k = atomicAdd(&nbuf, 1);
-      if (k < kContactSmem) {
-        buf[k] = make_int2((int)s, j);
-      } else {  // shared buffer full: append directly
-        const int q = atomicAdd(st.contact_count, 1);
-        if (q < st.contact_cap) st.contacts[q] = make_int2((int)s, j);
-        else set_status(st.status, EDM_STATUS_BIND_CAP);
+      for (uint32_t bits = rmask; bits; bits &= bits - 1) {
+        const int c = __ffs(bits) - 1;
+        if (!((L.capable[c] >> spj) & 1u) || d2 > p.cat[c].contact_sq) continue;
+        const int k = atomicAdd(&nbuf[c], 1);
+        if (k < per) {
+          buf[c * per + k] = make_int2((int)s, j);
+        } else {  // staging full: append directly
+          const int q = atomicAdd(&st.contact_count[c], 1);
+          if (q < st.contact_cap) st.contacts[(int64_t)c * st.contact_cap + q] = make_int2((int)s, j);
+          else set_status(st.status, EDM_STATUS_CONTACT_CAP);
+        }
       }
     });
   });
   __syncthreads();
-  const int n = nbuf < kContactSmem ? nbuf : kContactSmem;
-  if (threadIdx.x == 0) base = n > 0 ? atomicAdd(st.contact_count, n) : 0;
+  if (threadIdx.x < L.n_cat) {
+    const int n = nbuf[threadIdx.x] < per ? nbuf[threadIdx.x] : per;
+    base[threadIdx.x] = n > 0 ? atomicAdd(&st.contact_count[threadIdx.x], n) : 0;
+  }
   __syncthreads();
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    const int64_t q = (int64_t)base + k;
-    if (q < st.contact_cap) st.contacts[q] = buf[k];
-    else set_status(st.status, EDM_STATUS_BIND_CAP);
+  for (int c = 0; c < L.n_cat; ++c) {
+    const int n = nbuf[c] < per ? nbuf[c] : per;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      const int64_t q = (int64_t)base[c] + k;
+      if (q < st.contact_cap) st.contacts[(int64_t)c * st.contact_cap + q] = buf[c * per + k];
+      else set_status(st.status, EDM_STATUS_CONTACT_CAP);
+    }
   }
 }
 
-// Catalytic pass c (dynamics.py:825-983) over the step's contacts: the set of
+// Catalytic pass c (dynamics.py:825-983) over its contact list: the set of
 // substrates with at least one accepted (enzyme, substrate) pair converts.
+// Every listed pair is alive, has the pass's enzyme and is within its contact
+// radius; only the partner's current species is left to test.
 template <bool F64>
 __global__ void __launch_bounds__(kBlock) k_catalytic(const EdmDynParams* __restrict__ P, DevState st, int cidx) {
-  const int n = *st.contact_count;
+  const int n = st.contact_count[cidx];
   const int lim = (int64_t)n < st.contact_cap ? n : (int)st.contact_cap;
+  const int2* list = st.contacts + (int64_t)cidx * st.contact_cap;
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < lim; q += (int64_t)gridDim.x * blockDim.x) {
-    const int2 es = st.contacts[q];
-    const uint8_t fe = st.flags[es.x];
+    const int2 es = list[q];
     const uint8_t fs = st.flags[es.y];
-    const int r = replica_of(st.rep_first, st.n_rep, es.x);
+    int r = st.chunk_rep[es.x / kSweepChunk];
+    while (r + 1 < st.n_rep && st.rep_first[r + 1] <= es.x) ++r;
     const EdmDynParams& p = P[r];
     const EdmCat& C = p.cat[cidx];
-    if (!fl_alive(fe) || !fl_alive(fs) || fl_species(fe) != C.enzyme || fl_species(fs) != C.substrate) continue;
+    if (!fl_alive(fs) || fl_species(fs) != C.substrate) continue;
     const Geo g(p);
-    if (sep_sq<F64>(st.pos_post, st.cell_post, es.x, es.y, g) > C.contact_sq) continue;
     const int ide = st.ids[es.x] - (int)g.poff, ids = st.ids[es.y] - (int)g.poff;
     const uint32_t lo = ide < ids ? ide : ids, hi = ide < ids ? ids : ide;
     const double u = uniform1(p.seed, *st.d_step, EDM_S_CAT + cidx, lo, hi);

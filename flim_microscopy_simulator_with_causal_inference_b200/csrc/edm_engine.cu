@@ -115,8 +115,8 @@ struct EdmEngine {
   int2* contacts = nullptr;
   int32_t* contact_count = nullptr;
   int64_t contact_cap = 0;
-  uint32_t enzyme_mask = 0, partner_mask = 0;
-  double contact_sq_max = 0.0;
+  uint32_t enzyme_mask = 0;
+  CatLists cat_lists{};
   int64_t* rep_first = nullptr;
   int32_t* chunk_rep = nullptr;  // replica of the first slot of each 128-slot chunk
   std::vector<int32_t> emit_host;  // emitter list last uploaded
@@ -231,36 +231,55 @@ struct EdmEngine {
       writes({B.ra, B.rb, B.product});
     }
     if (p.n_cat > 0) {
-      enzyme_mask = partner_mask = 0;
-      contact_sq_max = 0.0;
+      enzyme_mask = 0;
+      uint32_t touched = 0;
+      cat_lists = CatLists{};
+      cat_lists.n_cat = p.n_cat;
       for (int c = 0; c < p.n_cat; ++c) {
         enzyme_mask |= 1u << p.cat[c].enzyme;
-        partner_mask |= (1u << p.cat[c].substrate) | (1u << p.cat[c].product);
+        touched |= (1u << p.cat[c].substrate) | (1u << p.cat[c].product);
+        // species that earlier passes of the step can turn into this substrate
+        uint32_t capable = 1u << p.cat[c].substrate;
+        for (int c2 = c - 1; c2 >= 0; --c2)
+          if ((capable >> p.cat[c2].product) & 1u) capable |= 1u << p.cat[c2].substrate;
+        cat_lists.capable[c] = capable;
+        cat_lists.reactions_of[p.cat[c].enzyme] |= 1u << c;
       }
-      for (int r = 0; r < R; ++r)
-        for (int c = 0; c < hdp[r].n_cat; ++c)
-          if (hdp[r].cat[c].contact_sq > contact_sq_max) contact_sq_max = hdp[r].cat[c].contact_sq;
-      if (enzyme_mask & partner_mask) return fail(EDM_EUNSUP, "an enzyme species is also a catalytic substrate/product");
+      for (int c = 0; c < p.n_cat; ++c) cat_lists.partners_of[p.cat[c].enzyme] |= cat_lists.capable[c];
+      if (enzyme_mask & touched) return fail(EDM_EUNSUP, "an enzyme species is also a catalytic substrate/product");
       Match m;
       m.species_mask = enzyme_mask;
       m.alive = 1;
       passes.push_back({P_CONTACTS, 0, m});
     }
+    // A pass whose probability is zero in every replica changes nothing (its
+    // keyed draws feed no other pass), so it is not scheduled.
+    auto any_positive = [&](auto prob_of) {
+      for (int r = 0; r < R; ++r)
+        if (prob_of(hdp[r]) > 0.0) return true;
+      return false;
+    };
     for (int c = 0; c < p.n_cat; ++c) {
+      if (!any_positive([&](const EdmDynParams& q) { return q.cat[c].prob; })) continue;
       reads({p.cat[c].rule});
       passes.push_back({P_CAT, c, none});
       writes({p.cat[c].substrate, p.cat[c].product});
     }
     for (int e = 0; e < p.n_exch; ++e) {
-      reads({p.exch[e].rule_on, p.exch[e].rule_on2});
-      passes.push_back({P_REC_CAND, e, match({p.exch[e].species}, 0)});
-      passes.push_back({P_REC_APPLY, e, none});
-      writes({p.exch[e].species});
-      reads({p.exch[e].rule_off});
-      passes.push_back({P_DETACH, e, match({p.exch[e].species}, 1)});
-      writes({p.exch[e].species});
+      if (any_positive([&](const EdmDynParams& q) { return q.exch[e].prob_on; })) {
+        reads({p.exch[e].rule_on, p.exch[e].rule_on2});
+        passes.push_back({P_REC_CAND, e, match({p.exch[e].species}, 0)});
+        passes.push_back({P_REC_APPLY, e, none});
+        writes({p.exch[e].species});
+      }
+      if (any_positive([&](const EdmDynParams& q) { return q.exch[e].prob_off; })) {
+        reads({p.exch[e].rule_off});
+        passes.push_back({P_DETACH, e, match({p.exch[e].species}, 1)});
+        writes({p.exch[e].species});
+      }
     }
     for (int v = 0; v < p.n_conv; ++v) {
+      if (!any_positive([&](const EdmDynParams& q) { return q.conv[v].prob; })) continue;
       reads({p.conv[v].rule});
       passes.push_back({P_CONV, v, match({p.conv[v].from}, 1)});
       writes({p.conv[v].from, p.conv[v].to});
@@ -302,8 +321,8 @@ struct EdmEngine {
         case P_BIND_APPLY: k_bind_apply<F64><<<rb, 128, 0, s>>>(dp, R, st, ps.index); break;
         case P_DISSOC: k_dissociate<F64><<<sgrid, kBlock, 0, s>>>(dp, st, ps.match, ps.index); break;
         case P_CONTACTS:
-          cudaMemsetAsync(contact_count, 0, sizeof(int32_t), s);
-          k_contacts<F64><<<sgrid, kBlock, 0, s>>>(dp, st, ps.match, partner_mask, contact_sq_max);
+          cudaMemsetAsync(contact_count, 0, sizeof(int32_t) * EDM_MAX_CAT, s);
+          k_contacts<F64><<<sgrid, kBlock, 0, s>>>(dp, st, ps.match, cat_lists);
           break;
         case P_CAT: k_catalytic<F64><<<cgrid, kBlock, 0, s>>>(dp, st, ps.index); break;
         case P_REC_CAND: k_recruit_candidates<F64><<<sgrid, kBlock, 0, s>>>(dp, st, ps.match, ps.index); break;
@@ -519,9 +538,9 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
     delete E;
     return rc;
   }
-  E->contact_cap = std::max<int64_t>(4 * np, 1 << 20);
-  ALLOC(E->contacts, (size_t)E->contact_cap);
-  ALLOC(E->contact_count, 1);
+  E->contact_cap = std::max<int64_t>(4 * np, 1 << 20);  // per catalytic reaction
+  ALLOC(E->contacts, (size_t)E->contact_cap * std::max(1, E->hdp[0].n_cat));
+  ALLOC(E->contact_count, EDM_MAX_CAT);
   ALLOC(E->rep_first, (size_t)n_replicas + 1);
   {
     std::vector<int64_t> rf(pfirst);
