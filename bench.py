@@ -286,6 +286,10 @@ def flim_bench(args, device: int, rank: int, world: int, stream):
     peak, peak_kind = peaks()
     achieved = FLIM_BYTES_PER_PX * R * 65536 / (hist_ms / 1e3) / 1e9
     gemm_flops = 2 * (2 * 2 * 256 ** 3) * R  # two maps, two 256^3 products each (algorithmic)
+    traffic = None
+    tr_file = ROOT / "profiles" / "traffic.json"
+    if tr_file.exists() and R == 256:  # the committed figure is for 256 replicas
+        traffic = json.loads(tr_file.read_text()).get("hist")
     err = acq.error_word()
 
     # e2e: host bound fractions in, every histogram out to pinned host memory
@@ -311,8 +315,8 @@ def flim_bench(args, device: int, rank: int, world: int, stream):
         "workload": FLIM_WORKLOAD.format(R=R), "replicas_per_gpu": R, "dtype": "bf16 GEMM / f32 accumulate, f64 bins",
         "kernel_ms": {"project": proj_ms, "histograms": hist_ms},
         "roofline": {"bound": "hbm", "kernel": "k_hist", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                     "alg_bytes_per_px": FLIM_BYTES_PER_PX},
+                     "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "alg_bytes_per_px": FLIM_BYTES_PER_PX, "alg_bytes": FLIM_BYTES_PER_PX * R * 65536},
         "tensor": {"kernel": "k_umma_gemm x2 (+ emitter maps)", "alg_tflops": gemm_flops / (proj_ms / 1e3) / 1e12,
                    "note": "algorithmic 2 x 2*256^3 FLOP per map over the whole projection time"},
         "e2e": {"value": px / e2e_s, "unit": "px/s", "h2d_bytes_per_step": int(bf.nbytes),
@@ -427,7 +431,7 @@ def main():
     achieved = alg[dom] * N / (groups[dom] / 1e3) / 1e9
     traffic = None
     tr_file = ROOT / "profiles" / "traffic.json"
-    if tr_file.exists():
+    if tr_file.exists() and args.replicas == 512 and world == 1:  # the committed figures are for this workload
         traffic = json.loads(tr_file.read_text()).get(dom)
 
     # ---- plain float64 path: one 13,000-particle system, per-step launches ---
@@ -483,7 +487,7 @@ def main():
                             "D2H; bytes are per BD step"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "alg_bytes_per_particle": alg[dom], "kernel_ms": groups[dom]},
+                         "alg_bytes_per_particle": alg[dom], "alg_bytes": alg[dom] * N, "kernel_ms": groups[dom]},
             "kernel_ms_per_step": groups,
             "fp64_plain": None if fp64 is None else {"value": fp64, "unit": UNIT,
                                                      "workload": "13,000-particle system with sine D(x), float64, "

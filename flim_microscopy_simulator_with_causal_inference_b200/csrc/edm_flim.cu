@@ -492,10 +492,13 @@ __global__ void __launch_bounds__(256, 4) k_hist(EdmFlimParams p, const float* _
   const int shift = nb == 256 ? 24 : 25;  // top bits of a word pick the cell
   uint32_t* h = wh[warp][lane % kSub];
   const uint32_t npx = (uint32_t)kDim * kDim;
-  const size_t total = (size_t)npx * (size_t)p.n_replicas;
-  for (size_t gpx = (size_t)blockIdx.x * 8 + warp; gpx < total; gpx += (size_t)gridDim.x * 8) {
-    const uint32_t r = (uint32_t)(gpx / npx);
-    const uint32_t px = (uint32_t)(gpx - (size_t)r * npx);
+  const uint32_t total = npx * (uint32_t)p.n_replicas;
+  // pixel index over all replicas: at most 4096 x 2^16 = 2^28, so 32 bits
+  // hold it and the replica / pixel split is a shift and a mask
+  static_assert(kDim * kDim == 1 << 16, "pixel split assumes 2^16 pixels per replica");
+  for (uint32_t gpx = blockIdx.x * 8u + (uint32_t)warp; gpx < total; gpx += gridDim.x * 8u) {
+    const uint32_t r = gpx >> 16;
+    const uint32_t px = gpx & 0xFFFFu;
     const float A = I[((size_t)r * 2 + 0) * npx + px];
     const float B = I[((size_t)r * 2 + 1) * npx + px];
     const uint64_t seed = edm_flim_replica_seed(p.seed, (int32_t)r);
@@ -527,7 +530,7 @@ __global__ void __launch_bounds__(256, 4) k_hist(EdmFlimParams p, const float* _
       atomicAdd(&h[(int)(w & 0xFFFFFFu) < e.x ? (int)(w >> shift) : e.y], 1u);
     }
     __syncwarp();
-    uint4* out = (uint4*)(hist + gpx * (size_t)nb);
+    uint4* out = (uint4*)(hist + (size_t)gpx * (size_t)nb);
     for (int q = lane; q < nb / 4; q += 32) {
       uint4 v = ((const uint4*)wh[warp][0])[q];
 #pragma unroll
