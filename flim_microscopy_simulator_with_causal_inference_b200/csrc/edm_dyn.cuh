@@ -266,26 +266,23 @@ __device__ __forceinline__ Tile tile_of(const int2* blk) {
 // column is one slot run (two where the column wraps in y); a slot's dcy
 // follows from its bucket (its pre-move cell).
 template <typename F>
-__device__ __forceinline__ void for_neighbour_slots(const Geo& g, const DevState& st, int c, F f) {
+__device__ __forceinline__ void for_neighbour_slots_box(const Geo& g, const DevState& st, int c, int dxlo, int dxhi,
+                                                        int dylo, int dyhi, F f) {
   int cx, cy;
   split_cell(c, g, cx, cy);
-  int ya0, yb0, ya1 = 0, yb1 = -1;
-  if (cy >= 1 && cy + 1 < g.ny) {
-    ya0 = cy - 1;
-    yb0 = cy + 1;
-  } else if (!g.py) {
-    ya0 = cy > 0 ? cy - 1 : 0;
-    yb0 = cy + 1 < g.ny ? cy + 1 : g.ny - 1;
-  } else if (cy == 0) {
+  // rows cy+dylo .. cy+dyhi (dylo <= 0 <= dyhi) as one or two runs
+  int ya0 = cy + dylo, yb0 = cy + dyhi, ya1 = 0, yb1 = -1;
+  if (!g.py) {
+    ya0 = ya0 < 0 ? 0 : ya0;
+    yb0 = yb0 >= g.ny ? g.ny - 1 : yb0;
+  } else if (ya0 < 0) {
     ya0 = 0;
-    yb0 = 1;
     ya1 = yb1 = g.ny - 1;
-  } else {
-    ya0 = g.ny - 2;
+  } else if (yb0 >= g.ny) {
     yb0 = g.ny - 1;
     ya1 = yb1 = 0;
   }
-  for (int dcx = -1; dcx <= 1; ++dcx) {
+  for (int dcx = dxlo; dcx <= dxhi; ++dcx) {
     int ncx = cx + dcx;
     if (g.px) ncx = ncx < 0 ? ncx + g.nx : (ncx >= g.nx ? ncx - g.nx : ncx);
     else if (ncx < 0 || ncx >= g.nx) continue;
@@ -301,6 +298,11 @@ __device__ __forceinline__ void for_neighbour_slots(const Geo& g, const DevState
       }
     }
   }
+}
+
+template <typename F>
+__device__ __forceinline__ void for_neighbour_slots(const Geo& g, const DevState& st, int c, F f) {
+  for_neighbour_slots_box(g, st, c, -1, 1, -1, 1, f);
 }
 
 // ---- density grids -----------------------------------------------------------
@@ -471,7 +473,25 @@ __device__ __forceinline__ void for_each_force_term(const EdmDynParams& p, const
   // pairs beyond both the pair-list cutoff and every potential's range carry no force
   const double range_sq = p.force_range_sq < g.cutoff_sq ? p.force_range_sq : g.cutoff_sq;
   const float range_sqf = (float)range_sq * 1.0001f;
-  for_neighbour_slots(g, st, st.cell_pre[s], [&](int j, int ordinal, int dcx, int dcy) {
+  // Only neighbour cells within that range of the particle can hold a force
+  // partner (a partner in a skipped column or row is farther than its offset
+  // to the cell side, itself beyond the range), so the sweep skips the others.
+  // Range <= cutoff <= cell side keeps every partner inside the 3x3 block.
+  const int c_pre = st.cell_pre[s];
+  double ox, oy;
+  if constexpr (F64) {
+    int cx, cy;
+    split_cell(c_pre, g, cx, cy);
+    ox = xi - (double)cx * g.sx;
+    oy = yi - (double)cy * g.sy;
+  } else {
+    ox = (double)oi.x;
+    oy = (double)oi.y;
+  }
+  const double reach = sqrt(range_sq) * 1.0001 + 1e-9;
+  const int dxlo = ox < reach ? -1 : 0, dxhi = ox > g.sx - reach ? 1 : 0;
+  const int dylo = oy < reach ? -1 : 0, dyhi = oy > g.sy - reach ? 1 : 0;
+  for_neighbour_slots_box(g, st, c_pre, dxlo, dxhi, dylo, dyhi, [&](int j, int ordinal, int dcx, int dcy) {
     {
       if (j == s) return;
       double dx, dy, dsq;
