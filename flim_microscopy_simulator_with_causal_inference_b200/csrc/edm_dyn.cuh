@@ -862,7 +862,7 @@ __global__ void __launch_bounds__(kBlock) k_contacts(const EdmDynParams* __restr
 // Every listed pair is alive, has the pass's enzyme and is within its contact
 // radius; only the partner's current species is left to test.
 template <bool F64>
-__global__ void __launch_bounds__(kBlock) k_catalytic(const EdmDynParams* __restrict__ P, DevState st, int cidx) {
+__global__ void __launch_bounds__(kBlock, 8) k_catalytic(const EdmDynParams* __restrict__ P, DevState st, int cidx) {
   const int n = st.contact_count[cidx];
   const int lim = (int64_t)n < st.contact_cap ? n : (int)st.contact_cap;
   const int2* list = st.contacts + (int64_t)cidx * st.contact_cap;
@@ -894,7 +894,7 @@ __global__ void __launch_bounds__(kBlock) k_catalytic(const EdmDynParams* __rest
 // Recruitment candidates of exchange e (dynamics.py:1229-1458): dormant
 // particles of the species whose keyed draw accepts at the keyed position.
 template <bool F64>
-__global__ void __launch_bounds__(kBlock) k_recruit_candidates(const EdmDynParams* __restrict__ P, DevState st,
+__global__ void __launch_bounds__(kBlock, 8) k_recruit_candidates(const EdmDynParams* __restrict__ P, DevState st,
                                                                Match m, int e) {
   sweep4(st, m, [&](int r, int64_t s) {
     const EdmDynParams& p = P[r];
@@ -972,7 +972,7 @@ __global__ void k_recruit_apply(const EdmDynParams* __restrict__ P, int n_rep, D
 
 // Detachment of exchange e (dynamics.py:1461-1555).
 template <bool F64>
-__global__ void __launch_bounds__(kBlock) k_detach(const EdmDynParams* __restrict__ P, DevState st, Match m, int e) {
+__global__ void __launch_bounds__(kBlock, 8) k_detach(const EdmDynParams* __restrict__ P, DevState st, Match m, int e) {
   sweep4(st, m, [&](int r, int64_t s) {
     const EdmDynParams& p = P[r];
     const EdmExch& X = p.exch[e];
@@ -994,7 +994,7 @@ __global__ void __launch_bounds__(kBlock) k_detach(const EdmDynParams* __restric
 
 // Unimolecular conversion v (dynamics.py:1565-1657).
 template <bool F64>
-__global__ void __launch_bounds__(kBlock) k_convert(const EdmDynParams* __restrict__ P, DevState st, Match m, int v) {
+__global__ void __launch_bounds__(kBlock, 8) k_convert(const EdmDynParams* __restrict__ P, DevState st, Match m, int v) {
   sweep4(st, m, [&](int r, int64_t s) {
     const EdmDynParams& p = P[r];
     const EdmConv& V = p.conv[v];

@@ -120,6 +120,7 @@ struct EdmEngine {
   int64_t* rep_first = nullptr;
   int32_t* chunk_rep = nullptr;  // replica of the first slot of each 128-slot chunk
   std::vector<int32_t> emit_host;  // emitter list last uploaded
+  std::vector<uint8_t> has_dye_host;  // has_dye of the last edm_set_state
   std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;
   std::vector<void*> allocs;
 
@@ -375,7 +376,16 @@ struct EdmEngine {
     else enqueue_scope_t<false>(s);
   }
 
+  // overlapped frame readout (edm_frame_out_begin / _wait)
+  uint32_t* flim_snap = nullptr;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_snap = nullptr, ev_read = nullptr;
+  bool read_pending = false;
+
   ~EdmEngine() {
+    if (ev_snap) cudaEventDestroy(ev_snap);
+    if (ev_read) cudaEventDestroy(ev_read);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     for (void* p : allocs) cudaFree(p);
   }
@@ -658,6 +668,11 @@ __global__ void k_get_state(const EdmDynParams* __restrict__ P, const int2* __re
   bond_local[id] = b >= 0 ? (int32_t)(b - p.particle_offset) : -1;
 }
 
+__global__ void k_narrow_i8(const int32_t* __restrict__ in, int8_t* __restrict__ out, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (int8_t)in[i];
+}
+
 __global__ void k_bond_to_global(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk, int32_t* bond) {
   const Tile t = tile_of(blk);
   const EdmDynParams& p = P[t.r];
@@ -682,9 +697,9 @@ int edm_set_state(EdmEngine* E, const EdmHostState* st, void* stream) {
   CUDA_TRY(cudaMemcpyAsync(E->st_alive, st->is_alive, N, cudaMemcpyHostToDevice, s));
   CUDA_TRY(cudaMemcpyAsync(E->bond, st->bond_partner, sizeof(int32_t) * N, cudaMemcpyHostToDevice, s));
   CUDA_TRY(cudaMemcpyAsync(E->has_dye, st->has_dye, N, cudaMemcpyHostToDevice, s));
-  std::vector<int8_t> dye8(N);
-  for (int64_t i = 0; i < N; ++i) dye8[i] = (int8_t)st->dye_type_id[i];
-  CUDA_TRY(cudaMemcpyAsync(E->dye, dye8.data(), N, cudaMemcpyHostToDevice, s));
+  // dye types arrive as int32 and are narrowed on the device (st_bond is free here)
+  CUDA_TRY(cudaMemcpyAsync(E->st_bond, st->dye_type_id, sizeof(int32_t) * N, cudaMemcpyHostToDevice, s));
+  if (N > 0) k_narrow_i8<<<148 * 8, 256, 0, s>>>(E->st_bond, E->dye, N);
   CUDA_TRY(cudaMemcpyAsync(E->ctmc, st->ctmc_state, N, cudaMemcpyHostToDevice, s));
   CUDA_TRY(cudaMemcpyAsync(E->bleached, st->is_bleached, N, cudaMemcpyHostToDevice, s));
   CUDA_TRY(cudaMemsetAsync(E->cnt, 0, sizeof(int32_t) * (E->n_cells > 0 ? E->n_cells : 1), s));
@@ -699,8 +714,16 @@ int edm_set_state(EdmEngine* E, const EdmHostState* st, void* stream) {
                                                      E->cnt);
     k_bond_to_global<<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, E->bond);
   }
-  // emitters: particles carrying a dye, in particle order per replica
+  // emitters: particles carrying a dye, in particle order per replica.  When
+  // has_dye equals the last upload the emitter list, its tiles and the
+  // captured graphs stay, and nothing here waits for the stream.
+  if (E->has_phot && E->has_dye_host.size() == (size_t)N &&
+      std::memcmp(E->has_dye_host.data(), st->has_dye, (size_t)N) == 0) {
+    CUDA_TRY(cudaGetLastError());
+    return EDM_OK;
+  }
   if (E->has_phot) {
+    E->has_dye_host.assign(st->has_dye, st->has_dye + N);
     std::vector<int32_t> eid;
     eid.reserve(N);
     int64_t off = 0;
@@ -976,6 +999,40 @@ int edm_get_flim(EdmEngine* E, int32_t replica, uint32_t* host_out, int64_t n_el
 int edm_reset_flim(EdmEngine* E, void* stream) {
   if (!E || !E->has_scope) return fail(EDM_EINVAL, "edm_reset_flim: engine has no microscope");
   CUDA_TRY(cudaMemsetAsync(E->flim, 0, sizeof(uint32_t) * E->n_flim, (cudaStream_t)stream));
+  return EDM_OK;
+}
+
+int64_t edm_flim_elems(EdmEngine* E) { return (E && E->has_scope) ? E->n_flim : 0; }
+
+int edm_frame_out_begin(EdmEngine* E, uint32_t* host_out, int64_t n_elems, void* stream) {
+  if (!E || !E->has_scope || !host_out) return fail(EDM_EINVAL, "edm_frame_out_begin: bad argument");
+  if (n_elems < E->n_flim) return fail(EDM_EINVAL, "edm_frame_out_begin: host buffer too small");
+  CUDA_TRY(cudaSetDevice(E->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!E->flim_snap) {
+    int rc;
+    if ((rc = E->alloc(&E->flim_snap, (size_t)E->n_flim)) != EDM_OK) return rc;
+    CUDA_TRY(cudaStreamCreateWithFlags(&E->copy_stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&E->ev_snap, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&E->ev_read, cudaEventDisableTiming));
+  }
+  const size_t bytes = sizeof(uint32_t) * (size_t)E->n_flim;
+  if (E->read_pending) CUDA_TRY(cudaStreamWaitEvent(s, E->ev_read, 0));  // snapshot free again
+  CUDA_TRY(cudaMemcpyAsync(E->flim_snap, E->flim, bytes, cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(cudaMemsetAsync(E->flim, 0, bytes, s));
+  CUDA_TRY(cudaEventRecord(E->ev_snap, s));
+  CUDA_TRY(cudaStreamWaitEvent(E->copy_stream, E->ev_snap, 0));
+  CUDA_TRY(cudaMemcpyAsync(host_out, E->flim_snap, bytes, cudaMemcpyDeviceToHost, E->copy_stream));
+  CUDA_TRY(cudaEventRecord(E->ev_read, E->copy_stream));
+  E->read_pending = true;
+  return EDM_OK;
+}
+
+int edm_frame_out_wait(EdmEngine* E) {
+  if (!E) return fail(EDM_EINVAL, "edm_frame_out_wait: null engine");
+  if (!E->read_pending) return EDM_OK;
+  CUDA_TRY(cudaSetDevice(E->device));
+  CUDA_TRY(cudaEventSynchronize(E->ev_read));
   return EDM_OK;
 }
 

@@ -72,6 +72,10 @@ def load_library():
     L.edm_profile_steps.argtypes = [vp, i32, i32, vp, vp]
     L.edm_launches_per_step.argtypes = [vp, i32]
     L.edm_cell_list_static.argtypes = [vp, i64, C.c_double, C.c_double, i32, i32, vp, vp, vp]
+    L.edm_flim_elems.argtypes = [vp]
+    L.edm_flim_elems.restype = i64
+    L.edm_frame_out_begin.argtypes = [vp, vp, i64, vp]
+    L.edm_frame_out_wait.argtypes = [vp]
     L.edm_flim_create.argtypes = [vp, i32, C.POINTER(vp)]
     L.edm_flim_destroy.argtypes = [vp]
     L.edm_flim_set_inputs.argtypes = [vp, vp, u64, vp]
@@ -157,11 +161,20 @@ class Engine:
                              _ptr(arrs["bleached"]))
         _check(self.L.edm_set_state(self.handle, C.byref(hs), _stream_handle(stream)), "edm_set_state")
 
-    def get_state(self, stream=None) -> dict:
+    STATE_FIELDS = (("positions", np.float64, 2), ("species", np.int32, 1), ("alive", np.uint8, 1),
+                    ("bond", np.int32, 1), ("ctmc", np.int8, 1), ("bleached", np.uint8, 1),
+                    ("has_dye", np.uint8, 1))
+
+    def get_state(self, stream=None, out: Optional[dict] = None) -> dict:
+        """The particle state in id order.  `out` may hold preallocated
+        (e.g. pinned) arrays of STATE_FIELDS' dtypes and shapes to fill."""
         N = self.N
-        out = dict(positions=np.empty((N, 2)), species=np.empty(N, np.int32), alive=np.empty(N, np.uint8),
-                   bond=np.empty(N, np.int32), ctmc=np.empty(N, np.int8), bleached=np.empty(N, np.uint8),
-                   has_dye=np.empty(N, np.uint8))
+        if out is None:
+            out = {k: np.empty((N, w) if w > 1 else N, dtype=dt) for k, dt, w in self.STATE_FIELDS}
+        for k, dt, w in self.STATE_FIELDS:
+            a = out[k]
+            if a.dtype != dt or a.shape != ((N, w) if w > 1 else (N,)) or not a.flags.c_contiguous:
+                raise ValueError(f"get_state: out['{k}'] must be a contiguous {np.dtype(dt).name} array of N rows")
         hs = PR.EdmHostState(N, _ptr(out["positions"]), _ptr(out["species"]), _ptr(out["alive"]), _ptr(out["bond"]),
                              _ptr(out["has_dye"]), None, _ptr(out["ctmc"]), _ptr(out["bleached"]))
         _check(self.L.edm_get_state(self.handle, C.byref(hs), _stream_handle(stream)), "edm_get_state")
@@ -206,6 +219,23 @@ class Engine:
 
     def launches_per_step(self, with_photons: bool = True) -> int:
         return _check(self.L.edm_launches_per_step(self.handle, int(bool(with_photons))), "edm_launches_per_step")
+
+    def flim_elems(self) -> int:
+        """uint32 elements of all replicas' FLIM stacks (edm_flim_elems)."""
+        return int(self.L.edm_flim_elems(self.handle))
+
+    def frame_out_begin(self, host_out: np.ndarray, stream=None) -> None:
+        """Snapshot and clear the finalized stacks on `stream`, then read the
+        snapshot into `host_out` (pinned uint32, flim_elems() long) on the
+        engine's copy stream, overlapping what `stream` does next."""
+        if host_out.dtype != np.uint32 or not host_out.flags.c_contiguous:
+            raise ValueError("host_out must be a contiguous uint32 array")
+        _check(self.L.edm_frame_out_begin(self.handle, _ptr(host_out), host_out.size, _stream_handle(stream)),
+               "edm_frame_out_begin")
+
+    def frame_out_wait(self) -> None:
+        """Block until the last frame_out_begin read has landed in host memory."""
+        _check(self.L.edm_frame_out_wait(self.handle), "edm_frame_out_wait")
 
     def finalize(self, frame_index: int, stream=None):
         _check(self.L.edm_scope_finalize(self.handle, int(frame_index), _stream_handle(stream)), "edm_scope_finalize")

@@ -252,7 +252,11 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot,
                int32_t device, EdmEngine** out);
 int edm_destroy(EdmEngine* eng);
 
-/* Host <-> device particle state, id order (ParticleState arrays). */
+/* Host <-> device particle state, id order (ParticleState arrays).  The
+ * copies are ordered on `stream`; when the host arrays are pinned they are
+ * read asynchronously, so keep them unchanged until the stream has passed
+ * this call.  edm_get_state returns after the state has landed in host
+ * memory. */
 int edm_set_state(EdmEngine* eng, const EdmHostState* st, void* stream);
 int edm_get_state(EdmEngine* eng, EdmHostState* st, void* stream);
 int edm_set_step(EdmEngine* eng, int64_t step_index);
@@ -296,6 +300,24 @@ int edm_scope_finalize(EdmEngine* eng, int64_t frame_index, void* stream);
 int edm_get_flim(EdmEngine* eng, int32_t replica, uint32_t* host_out,
                  int64_t n_elems, void* stream);
 int edm_reset_flim(EdmEngine* eng, void* stream);
+
+/* Overlapped frame readout, for frame loops that read every stack.
+ * edm_frame_out_begin copies the finalized stacks of all replicas into an
+ * engine-owned snapshot on `stream` and clears the live stacks (what
+ * edm_reset_flim does). Then, on a copy stream of the engine's own, it
+ * starts reading the snapshot into host_out, so the read overlaps the work
+ * `stream` does next. host_out holds edm_flim_elems() uint32 values,
+ * replicas in order, each [n_ch][nx][ny][n_bins] as edm_get_flim returns
+ * it; it should be pinned (page-locked) for the copy to be asynchronous.
+ * A new begin first waits, on `stream`, for the previous read to leave the
+ * snapshot. edm_frame_out_wait blocks until the last read has landed in
+ * host memory. The first begin allocates the snapshot (n_flim * 4 bytes).
+ * The read occupies the device-to-host link for n_flim * 4 bytes: issue the
+ * frame's other reads (edm_get_state) before it, or they queue behind it. */
+int64_t edm_flim_elems(EdmEngine* eng);
+int edm_frame_out_begin(EdmEngine* eng, uint32_t* host_out, int64_t n_elems,
+                        void* stream);
+int edm_frame_out_wait(EdmEngine* eng);
 
 /* Counters [n_replicas][EDM_NCOUNTERS] and the sticky status word. */
 int edm_get_counters(EdmEngine* eng, int64_t* out, void* stream);

@@ -1,0 +1,42 @@
+"""Overlapped frame readout (edm_frame_out_begin / edm_frame_out_wait): on
+two frames in a row, the snapshot read into host memory equals the stacks
+edm_get_flim returns replica by replica, and the live stacks start the next
+frame cleared."""
+import numpy as np
+import pytest
+import torch
+
+from flim_microscopy_simulator_with_causal_inference_b200 import workloads as W
+from flim_microscopy_simulator_with_causal_inference_b200.batch import Ensemble
+
+pytestmark = pytest.mark.gpu
+
+
+def test_frame_out_equals_per_replica_reads_on_two_frames():
+    raws = W.ensemble_replicas(4, seed=11, n_min=600, n_max=1500)
+    ens = Ensemble(raws, precision=32, photons=True, device=0)
+    eng = ens.engine
+    n = eng.flim_elems()
+    sizes = [int(np.prod(eng.flim(r).shape)) for r in range(ens.R)]
+    assert n == sum(sizes)
+    host = torch.empty(n, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+    s = torch.cuda.Stream()
+    for frame in range(2):
+        eng.pipeline_steps(50, True, 50, stream=s)
+        eng.finalize(frame, stream=s)
+        s.synchronize()
+        expect = np.concatenate([eng.flim(r).ravel() for r in range(ens.R)])
+        assert expect.sum() > 0
+        host[:] = 7
+        eng.frame_out_begin(host, stream=s)
+        eng.frame_out_wait()
+        np.testing.assert_array_equal(host, expect)
+        s.synchronize()
+        assert all(eng.flim(r).sum() == 0 for r in range(ens.R))
+
+
+def test_frame_out_rejects_a_short_buffer():
+    ens = Ensemble(W.ensemble_replicas(2, seed=3, n_min=600, n_max=800), precision=32, photons=True, device=0)
+    short = np.zeros(ens.engine.flim_elems() - 1, dtype=np.uint32)
+    with pytest.raises(RuntimeError, match="too small"):
+        ens.engine.frame_out_begin(short)
