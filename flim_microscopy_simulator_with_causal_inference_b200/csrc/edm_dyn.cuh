@@ -439,8 +439,10 @@ __global__ void __launch_bounds__(kBlock) k_scatter(const EdmDynParams* __restri
   if (t.s >= p.particle_offset + p.n_particles) return;
   const int c = st.cell_post[t.s];
   const uint8_t f = st.flags_old[t.s];
-  const int key = fl_alive(f) ? c : p.nx * p.ny;
-  const int d = atomic_inc_aggregated(&st.cell_cursor[p.cell_offset + key]);
+  // alive particles mostly have a cell to themselves: a plain atomic; the
+  // non-alive ones all share their replica's last bucket: aggregated per warp
+  const int d = fl_alive(f) ? atomicAdd(&st.cell_cursor[p.cell_offset + c], 1)
+                            : atomic_inc_aggregated(&st.cell_cursor[p.cell_offset + p.nx * p.ny]);
   if constexpr (F64) {
     ((double2*)st.pos_pre)[d] = ((const double2*)st.pos_post)[t.s];
   } else {
@@ -762,7 +764,7 @@ __global__ void __launch_bounds__(kBlock) k_move(const EdmDynParams* __restrict_
     y = (double)cy * g.sy + (double)o.y;
   }
   st.cell_post[s] = newc;
-  atomic_inc_aggregated(&st.cnt_next[g.cbase + newc]);
+  atomicAdd(&st.cnt_next[g.cbase + newc], 1);  // result unused: a fire-and-forget reduction
   grid_add(p, st.grid_cnt, sp, x, y, 1);
 }
 
