@@ -69,6 +69,10 @@ struct DevState {
   int64_t contact_cap;      // per catalytic reaction
   const int64_t* rep_first;  // [R + 1] first slot of each replica
   const int32_t* chunk_rep;  // replica of the first slot of each kSweepChunk-slot chunk
+  // slots that left their sort bucket's neighbourhood after the sort this step
+  // (recruited, or placed by dissociation): per replica at particle_offset
+  int32_t* moved;
+  int32_t* moved_count;  // [R]
   int n_rep;
   int64_t n_slots;
 };
@@ -331,6 +335,12 @@ __device__ __forceinline__ void grid_change(const EdmDynParams& p, int32_t* delt
                                             int sp_new, bool alive_new, double x, double y) {
   if (alive_old) grid_add(p, delta, sp_old, x, y, -1);
   if (alive_new) grid_add(p, delta, sp_new, x, y, +1);
+}
+
+// Record a slot placed away from its sort bucket after this step's sort.
+__device__ __forceinline__ void note_moved(const DevState& st, int r, const EdmDynParams& p, int64_t slot) {
+  const int k = atomicAdd(&st.moved_count[r], 1);
+  if (k < p.n_particles) st.moved[p.particle_offset + k] = (int32_t)slot;
 }
 
 // Next step's bucket counts when a particle changes bucket.
@@ -967,6 +977,7 @@ __global__ void k_recruit_apply(const EdmDynParams* __restrict__ P, int n_rep, D
     st.cell_post[slot] = newc;
     rebucket(st, g, g.grave, newc);
     st.flags[slot] = fl_make(X.species, true);
+    note_moved(st, r, p, slot);
     grid_add(p, st.grid_delta, X.species, x, y, 1);
   }
   atomic_add_i64(&st.counters[(int64_t)r * EDM_NCOUNTERS + EDM_C_RECRUITED], take);
@@ -1143,6 +1154,7 @@ __global__ void __launch_bounds__(kBlock) k_dissociate(const EdmDynParams* __res
     }
     rebucket(st, g, fl_alive(fj) ? st.cell_post[sj] : g.grave, newc);
     st.cell_post[sj] = newc;
+    note_moved(st, r, p, sj);
     st.bond[g.poff + id] = -1;
     st.bond[partner] = -1;
     grid_change(p, st.grid_delta, B.product, true, B.ra, true, x, y);

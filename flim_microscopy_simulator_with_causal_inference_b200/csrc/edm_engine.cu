@@ -119,8 +119,10 @@ struct EdmEngine {
   CatLists cat_lists{};
   int64_t* rep_first = nullptr;
   int32_t* chunk_rep = nullptr;  // replica of the first slot of each 128-slot chunk
+  int32_t *moved = nullptr, *moved_count = nullptr;
   std::vector<int32_t> emit_host;  // emitter list last uploaded
   std::vector<uint8_t> has_dye_host;  // has_dye of the last edm_set_state
+  bool cells_valid = false;  // the cell list matches the state (a dynamics step ran since set_state)
   std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;
   std::vector<void*> allocs;
 
@@ -156,6 +158,8 @@ struct EdmEngine {
     s.contact_cap = contact_cap;
     s.rep_first = rep_first;
     s.chunk_rep = chunk_rep;
+    s.moved = moved;
+    s.moved_count = moved_count;
     s.n_rep = R;
     s.n_slots = N;
     return s;
@@ -309,6 +313,7 @@ struct EdmEngine {
       cudaMemsetAsync(grid_cnt, 0, sizeof(int32_t) * n_grid, s);
       cudaMemsetAsync(grid_delta, 0, sizeof(int32_t) * n_grid, s);
     }
+    cudaMemsetAsync(moved_count, 0, sizeof(int32_t) * R, s);
     mark(2, s);
     k_move<F64><<<npblk, kBlock, 0, s>>>(dp, pblk, st);
     mark(3, s);
@@ -334,6 +339,7 @@ struct EdmEngine {
       }
     }
     k_step_inc<<<1, 1, 0, s>>>(d_step);
+    cells_valid = true;
     mark(4, s);
   }
 
@@ -352,7 +358,7 @@ struct EdmEngine {
   void enqueue_photons_t(cudaStream_t s) {
     DevState st = dev_state();
     PhotState ph = phot_state();
-    if (neblk > 0) k_phot_count<F64><<<neblk, kBlock, 0, s>>>(dp, pp, eblk, st, ph);
+    if (neblk > 0) k_phot_count<F64><<<neblk, kBlock, 0, s>>>(dp, pp, eblk, st, ph, cells_valid ? 1 : 0);
     k_phot_scan<<<R, 256, 0, s>>>(pp, ph, counters, status);
     if (neblk > 0) k_phot_write<<<neblk, kBlock, 0, s>>>(dp, pp, eblk, ph, counters);
     k_phot_advance<<<1, 1, 0, s>>>(d_pstep, d_batch_key);
@@ -551,6 +557,8 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
   E->contact_cap = std::max<int64_t>(4 * np, 1 << 20);  // per catalytic reaction
   ALLOC(E->contacts, (size_t)E->contact_cap * std::max(1, E->hdp[0].n_cat));
   ALLOC(E->contact_count, EDM_MAX_CAT);
+  ALLOC(E->moved, np);
+  ALLOC(E->moved_count, (size_t)n_replicas);
   ALLOC(E->rep_first, (size_t)n_replicas + 1);
   {
     std::vector<int64_t> rf(pfirst);
@@ -688,6 +696,7 @@ extern "C" {
 
 int edm_set_state(EdmEngine* E, const EdmHostState* st, void* stream) {
   if (!E || !st || st->n != E->N) return fail(EDM_EINVAL, "edm_set_state: size mismatch");
+  E->cells_valid = false;
   cudaStream_t s = (cudaStream_t)stream;
   CUDA_TRY(cudaSetDevice(E->device));
   const int64_t N = E->N;

@@ -71,7 +71,8 @@ __device__ __forceinline__ int64_t poisson_lcg(double mean, double u_seed, doubl
 template <bool F64>
 __global__ void __launch_bounds__(kBlock) k_phot_count(const EdmDynParams* __restrict__ DP,
                                                        const EdmPhotParams* __restrict__ PP,
-                                                       const int2* __restrict__ eblk, DevState st, PhotState ph) {
+                                                       const int2* __restrict__ eblk, DevState st, PhotState ph,
+                                                       int cells_valid) {
   const Tile t = tile_of(eblk);
   const EdmPhotParams& pp = PP[t.r];
   const EdmDynParams& p = DP[t.r];
@@ -113,14 +114,21 @@ __global__ void __launch_bounds__(kBlock) k_phot_count(const EdmDynParams* __res
         }
       }
     } else {
+      // Any alive target within the radius, post-move (the reference's
+      // all-pairs search, photophysics.py:591-683).  After a dynamics step
+      // it goes through that step's cell list: a target within radius R now
+      // was within R + 2 max_disp before the move, so the pre-move cells
+      // within that reach of the donor's pre-move cell hold every candidate
+      // that moved by Brownian steps; the step's list of particles placed
+      // after the sort holds the rest.  Same per-pair test, same answer.  Before any dynamics step since the
+      // state was set, the cell list does not exist and every particle of
+      // the replica is tested.
       const Geo g(p);
       double xi, yi;
       abs_pos<F64>(st.pos_post, st.cell_post, slot, g, xi, yi);
-      bool found = false;
-      for (int64_t j = p.particle_offset; j < p.particle_offset + p.n_particles && !found; ++j) {
-        if (j == slot) continue;
+      auto near = [&](int64_t j) {
         const uint8_t fj = st.flags[j];
-        if (!fl_alive(fj) || fl_species(fj) != F.target_species) continue;
+        if (j == slot || !fl_alive(fj) || fl_species(fj) != F.target_species) return false;
         double xj, yj;
         abs_pos<F64>(st.pos_post, st.cell_post, j, g, xj, yj);
         double dx = xj - xi, dy = yj - yi;
@@ -132,8 +140,37 @@ __global__ void __launch_bounds__(kBlock) k_phot_count(const EdmDynParams* __res
           if (dy > g.Ly / 2.0) dy -= g.Ly;
           else if (dy < -g.Ly / 2.0) dy += g.Ly;
         }
-        if (dx * dx + dy * dy < F.prox_radius_sq) found = true;
+        return dx * dx + dy * dy < F.prox_radius_sq;
+      };
+      bool found = false;
+      if (!cells_valid) {
+        for (int64_t j = p.particle_offset; j < p.particle_offset + p.n_particles && !found; ++j) found = near(j);
+        cls = found ? F.cls_high : F.cls_low;
+        acc = -1;
+        continue;
       }
+      const double reach = sqrt(F.prox_radius_sq) + 2.0 * p.max_disp;
+      const int kx = (int)ceil(reach / g.sx), ky = (int)ceil(reach / g.sy);
+      int cx, cy;
+      split_cell(st.cell_pre[slot], g, cx, cy);
+      // a window as wide as the grid visits every column / row once
+      const int x0 = 2 * kx + 1 >= g.nx ? 0 : cx - kx, x1 = 2 * kx + 1 >= g.nx ? g.nx - 1 : cx + kx;
+      const int y0 = 2 * ky + 1 >= g.ny ? 0 : cy - ky, y1 = 2 * ky + 1 >= g.ny ? g.ny - 1 : cy + ky;
+      for (int ux = x0; ux <= x1 && !found; ++ux) {
+        int ncx = ux;
+        if (g.px) ncx = ncx < 0 ? ncx + g.nx : (ncx >= g.nx ? ncx - g.nx : ncx);
+        else if (ncx < 0 || ncx >= g.nx) continue;
+        for (int uy = y0; uy <= y1 && !found; ++uy) {
+          int ncy = uy;
+          if (g.py) ncy = ncy < 0 ? ncy + g.ny : (ncy >= g.ny ? ncy - g.ny : ncy);
+          else if (ncy < 0 || ncy >= g.ny) continue;
+          const int64_t nc = g.cbase + (int64_t)ncx * g.ny + ncy;
+          for (int j = st.cell_start[nc], je = st.cell_start[nc + 1]; j < je && !found; ++j) found = near(j);
+        }
+      }
+      // particles placed after the sort (recruitment, dissociation) are not in the cell list
+      const int nm = min(st.moved_count[t.r], (int)p.n_particles);
+      for (int k = 0; k < nm && !found; ++k) found = near(st.moved[p.particle_offset + k]);
       cls = found ? F.cls_high : F.cls_low;
       acc = -1;
     }

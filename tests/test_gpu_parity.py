@@ -57,7 +57,7 @@ def test_fp64_cell_lists_match_oracle():
         assert gsets == cell_sets_oracle(P.orc, P.dp.nx, P.dp.ny)
 
 
-@pytest.mark.parametrize("case", ["rich_small", "binding_regions"])
+@pytest.mark.parametrize("case", ["rich_small", "binding_regions", "proximity_small"])
 def test_fp64_pipeline_photons_and_tcspc_match_oracle(case):
     P = Pair(cases.get(case), precision=64)
     total = 0
@@ -129,3 +129,15 @@ def test_determinism_two_runs_bitwise():
         assert np.array_equal(runs[0][0][k], runs[1][0][k]), k
     assert np.array_equal(runs[0][1], runs[1][1])
     assert np.array_equal(runs[0][2], runs[1][2])
+
+
+def test_fp64_proximity_photons_before_any_dynamics_step():
+    """Proximity FRET right after the state is set (no cell list yet): the
+    all-pairs search gives the oracle's photons."""
+    P = Pair(cases.get("proximity_small"), precision=64)
+    P.eng.photon_step()
+    ob = P.orc.photon_step()
+    pid, tt, ch, fr = P.eng.photons(0)
+    assert pid.size > 0
+    assert np.array_equal(pid, ob[0]) and np.array_equal(ch, ob[2]) and np.array_equal(fr, ob[3])
+    np.testing.assert_allclose(tt, ob[1], rtol=1e-14, atol=0)
