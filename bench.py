@@ -276,6 +276,21 @@ def flim_bench(args, device: int, rank: int, world: int, stream):
             ev[3 * k + 2].record(stream)
         stream.synchronize()
     torch.cuda.synchronize()
+    # lifetime readouts (mean arrival time + phasor) of all histograms: one streaming pass
+    from flim_microscopy_simulator_with_causal_inference_b200 import readouts as RD
+    hist_ptr, _ = acq.device_ptr(FA.HIST)
+    ro_out = torch.empty((6, R * 65536), dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        RD.lifetimes_device(hist_ptr, R * 65536, 256, 25e-9, out=ro_out, stream=s)
+    rev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps)]
+    for k in range(args.steps):
+        rev[2 * k].record(stream)
+        RD.lifetimes_device(hist_ptr, R * 65536, 256, 25e-9, out=ro_out, stream=s)
+        rev[2 * k + 1].record(stream)
+    stream.synchronize()
+    ro_ms = statistics.mean(rev[2 * k].elapsed_time(rev[2 * k + 1]) for k in range(args.steps))
+    ro_bytes = R * 65536 * (256 * 4 + 6 * 8)
+    del ro_out
     proj = [ev[3 * k].elapsed_time(ev[3 * k + 1]) for k in range(args.steps)]
     hist = [ev[3 * k + 1].elapsed_time(ev[3 * k + 2]) for k in range(args.steps)]
     ms = max_over_ranks(ev[0].elapsed_time(ev[-1]), world, "cuda")
@@ -322,6 +337,11 @@ def flim_bench(args, device: int, rank: int, world: int, stream):
         "e2e": {"value": px / e2e_s, "unit": "px/s", "h2d_bytes_per_step": int(bf.nbytes),
                 "d2h_bytes_per_step": int(R * 65536 * 256 * 4),
                 "note": "per acquisition: bound fractions H2D, acquire, every histogram D2H to pinned host memory"},
+        "readout": {"kernel": "k_readout (mean arrival time + phasor of every pixel)", "ms": ro_ms,
+                    "px_per_s": R * 65536 / (ro_ms / 1e3),
+                    "roofline": {"bound": "hbm", "achieved": ro_bytes / (ro_ms / 1e3) / 1e9, "peak": peak,
+                                 "unit": "GB/s", "frac": ro_bytes / (ro_ms / 1e3) / 1e9 / peak,
+                                 "alg_bytes_per_px": 256 * 4 + 6 * 8}},
         "gpu_launches": 5 * args.steps, "error_word": err, "clocks": clk.summary(),
         "l2": "histograms 17 GB per acquisition >> 126 MB L2",
     }

@@ -1013,6 +1013,16 @@ int edm_reset_flim(EdmEngine* E, void* stream) {
 
 int64_t edm_flim_elems(EdmEngine* E) { return (E && E->has_scope) ? E->n_flim : 0; }
 
+int edm_flim_stack_ptr(EdmEngine* E, int32_t replica, void** ptr, int64_t* n_px, int32_t* n_bins) {
+  if (!E || !E->has_scope || !ptr || replica < 0 || replica >= E->R)
+    return fail(EDM_EINVAL, "edm_flim_stack_ptr: bad argument");
+  const EdmScopeParams& p = E->hsp[replica];
+  *ptr = E->flim + p.flim_offset;
+  if (n_px) *n_px = (int64_t)p.n_channels * p.nx * p.ny;
+  if (n_bins) *n_bins = p.n_bins;
+  return EDM_OK;
+}
+
 int edm_frame_out_begin(EdmEngine* E, uint32_t* host_out, int64_t n_elems, void* stream) {
   if (!E || !E->has_scope || !host_out) return fail(EDM_EINVAL, "edm_frame_out_begin: bad argument");
   if (n_elems < E->n_flim) return fail(EDM_EINVAL, "edm_frame_out_begin: host buffer too small");

@@ -72,6 +72,8 @@ def load_library():
     L.edm_profile_steps.argtypes = [vp, i32, i32, vp, vp]
     L.edm_launches_per_step.argtypes = [vp, i32]
     L.edm_cell_list_static.argtypes = [vp, i64, C.c_double, C.c_double, i32, i32, vp, vp, vp]
+    L.edm_readout_lifetimes.argtypes = [vp, i64, i32, C.c_double, i32, i32, i32, vp, vp]
+    L.edm_flim_stack_ptr.argtypes = [vp, i32, C.POINTER(vp), C.POINTER(i64), C.POINTER(i32)]
     L.edm_flim_elems.argtypes = [vp]
     L.edm_flim_elems.restype = i64
     L.edm_frame_out_begin.argtypes = [vp, vp, i64, vp]

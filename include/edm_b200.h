@@ -438,6 +438,23 @@ int edm_flim_read(EdmFlim* flim, int32_t what, int32_t replica,
                   void* host_out, int64_t bytes, void* stream);
 int edm_flim_get_error(EdmFlim* flim, uint32_t* word);
 
+/* ---- lifetime readouts of TCSPC stacks (analysis.py:87-150, 497-566) ----
+ * For a device stack [n_px][n_bins] of uint32 counts (an engine stack from
+ * edm_flim_stack_ptr, or EDM_FLIM_HIST of an acquisition), writes float64
+ * out_dev[6][n_px]: intensity, mean arrival time (ns; NaN below
+ * min_counts_mean), phasor g and s of the given harmonic (0 below
+ * min_counts_phasor), phase and modulation lifetimes (ns; NaN where the
+ * reference leaves them NaN).  n_bins: a multiple of 4, at most 256; the
+ * stack 16-byte aligned. */
+int edm_readout_lifetimes(const uint32_t* stack_dev, int64_t n_px, int32_t n_bins,
+                          double time_range_s, int32_t harmonic,
+                          int32_t min_counts_mean, int32_t min_counts_phasor,
+                          double* out_dev, void* stream);
+/* Device address of replica `replica`'s stack [n_ch][nx][ny][n_bins] and its
+ * pixel count n_ch * nx * ny. */
+int edm_flim_stack_ptr(EdmEngine* eng, int32_t replica, void** ptr,
+                       int64_t* n_px, int32_t* n_bins);
+
 /* Noise of the engine's generator, for injection into the reference:
  * writes n keyed standard normals pairs (2n doubles) / uniforms.  The
  * arrays are device pointers; keys a[i] (particle / photon index). */

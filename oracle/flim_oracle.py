@@ -15,7 +15,9 @@ reference formula it is built from:
 * bin_probs       -- P(bin b) of t = Exp(tau) + N(0, sigma_irf^2) binned by
   b = int(max(t, 0) / width), b >= n_bins lost (microscope.py:716-803);
 * tau_expected    -- the mean-arrival-time readout (analysis.py:87-150) of
-  the expected histogram.
+  the expected histogram;
+* readouts        -- mean_arrival_time and phasor_transform (analysis.py:87-150,
+  497-566) of count stacks.
 """
 from __future__ import annotations
 
@@ -102,3 +104,35 @@ def poisson_histograms(mu: np.ndarray, seed: int) -> np.ndarray:
     """A CPU sample of the histograms (numpy's Poisson generator): the timed
     baseline of the acquisition, not a bit-level model of the GPU draws."""
     return np.random.default_rng(seed).poisson(mu).astype(np.uint32)
+
+
+def readouts(stack: np.ndarray, time_range_s: float, harmonic: int = 1, min_counts_mean: int = 10,
+             min_counts_phasor: int = 20) -> dict:
+    """mean_arrival_time (ed_mrdt/analysis.py:87-150) and phasor_transform
+    (:497-566) of a [..., n_bins] count stack, restated in float64 numpy."""
+    data = stack.astype(np.float64)
+    n_bins = data.shape[-1]
+    t_ns = (np.arange(n_bins) + 0.5) * ((time_range_s / n_bins) * 1e9)
+    intensity = data.sum(axis=-1)
+    weighted = np.tensordot(data, t_ns, axes=([-1], [0]))
+    tau = np.full_like(intensity, np.nan)
+    m = intensity >= min_counts_mean
+    tau[m] = weighted[m] / intensity[m]
+    omega = 2.0 * np.pi * harmonic / time_range_s
+    phi = 2.0 * np.pi * harmonic * (np.arange(n_bins) + 0.5) / n_bins
+    g_num = np.tensordot(data, np.cos(phi), axes=([-1], [0]))
+    s_num = np.tensordot(data, np.sin(phi), axes=([-1], [0]))
+    mask = intensity >= min_counts_phasor
+    g = np.zeros_like(intensity)
+    s = np.zeros_like(intensity)
+    g[mask] = g_num[mask] / intensity[mask]
+    s[mask] = s_num[mask] / intensity[mask]
+    omega_ns = omega * 1e-9
+    tau_phi = np.full_like(g, np.nan)
+    tau_mod = np.full_like(g, np.nan)
+    valid = mask & (g > 1e-10)
+    tau_phi[valid] = (s[valid] / g[valid]) / omega_ns
+    m_sq = g ** 2 + s ** 2
+    mod_valid = valid & (m_sq > 1e-10) & (m_sq < 1.0 - 1e-10)
+    tau_mod[mod_valid] = np.sqrt(1.0 / m_sq[mod_valid] - 1.0) / omega_ns
+    return dict(intensity=intensity, tau_mean_ns=tau, g=g, s=s, tau_phi_ns=tau_phi, tau_mod_ns=tau_mod)

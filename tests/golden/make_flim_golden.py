@@ -18,7 +18,9 @@ it is built from, on the acquisition's own configuration:
   K times the weights to within one photon;
 * TCSPC: the reference's accumulate (microscope.py:716-803) for N
   mono-exponential arrivals t = -tau ln(u) (photophysics.py:440) at the free
-  and FRET-bound lifetimes, seeded.
+  and FRET-bound lifetimes, seeded;
+* readouts: the reference's mean_arrival_time and phasor_transform
+  (analysis.py:87-150, 497-566) on a seeded count stack.
 """
 from __future__ import annotations
 
@@ -92,6 +94,25 @@ def generate() -> dict:
         tc.accumulate(z, z, t, np.zeros(N_TCSPC, np.int8), N_TCSPC, np.random.default_rng(s2))
         out[f"tcspc_{name}"] = tc.flim_stack[0, 0, 0].copy()
     out["tcspc_n"] = N_TCSPC
+
+    # lifetime readouts (analysis.py:87-150, 497-566) of a seeded count stack
+    # [2 ch][12][12][256]: exponential decays of mixed lifetimes and brightness,
+    # some pixels below the readouts' count thresholds
+    from ed_mrdt.analysis import mean_arrival_time, phasor_transform
+    rng = np.random.default_rng(5)
+    t = (np.arange(256) + 0.5) * 25.0 / 256
+    tau = rng.uniform(0.8, 4.0, size=(2, 12, 12, 1))
+    bright = rng.choice([0.0, 0.05, 3.0, 40.0], size=(2, 12, 12, 1))
+    stack = rng.poisson(bright * np.exp(-t / tau)).astype(np.uint32)
+    out["readout_stack"] = stack
+    for ch in range(2):
+        tau_map, inten = mean_arrival_time(stack, time_range=25e-9, channel=ch, min_counts=10)
+        out[f"readout_tau_ch{ch}"] = tau_map
+        out[f"readout_intensity_ch{ch}"] = inten
+        for h in (1, 2):
+            ph = phasor_transform(stack, time_range=25e-9, channel=ch, harmonic=h, min_counts=20)
+            for k in ("g", "s", "tau_phi", "tau_mod"):
+                out[f"readout_{k}_ch{ch}_h{h}"] = getattr(ph, k)
     return out
 
 

@@ -116,3 +116,16 @@ def test_mean_arrival_time_readout_matches_the_formula():
     t = (np.arange(256) + 0.5) * (25.0 / 256)
     assert math.isnan(tau[0, 0]) and inten[0, 0] == 0
     assert tau[1, 1] == pytest.approx((stack[1, 1] * t).sum() / stack[1, 1].sum(), rel=1e-14)
+
+
+@pytest.mark.parametrize("ch", [0, 1])
+@pytest.mark.parametrize("h", [1, 2])
+def test_readouts_equal_the_reference_analysis_functions(gold, ch, h):
+    stack = gold["readout_stack"][ch]
+    r = FO.readouts(stack, 25e-9, harmonic=h, min_counts_mean=10, min_counts_phasor=20)
+    np.testing.assert_allclose(r["intensity"], gold[f"readout_intensity_ch{ch}"], rtol=0, atol=0)
+    np.testing.assert_allclose(r["tau_mean_ns"], gold[f"readout_tau_ch{ch}"], rtol=1e-14, equal_nan=True)
+    for k, name in (("g", "g"), ("s", "s"), ("tau_phi_ns", "tau_phi"), ("tau_mod_ns", "tau_mod")):
+        np.testing.assert_allclose(r[k], gold[f"readout_{name}_ch{ch}_h{h}"], rtol=1e-13, atol=1e-15,
+                                   equal_nan=True, err_msg=k)
+    assert np.isnan(r["tau_mean_ns"]).any() and (~np.isnan(r["tau_mean_ns"])).any()
