@@ -616,7 +616,7 @@ class SimulationPipeline:
         c = eng.counters()[0]
         res = SimulationResult(self.config, frames, time.perf_counter() - t_all, 0.0, tot_em, tot_det,
                                int(c[PR.C_BINDINGS]), int(c[PR.C_DISSOC]), int(np.sum(self._state.is_bleached)),
-                               sub)
+                               self._subframe_result(sub) if sub is not None else None)
         self._dynamics._pull_counters(sys)
         self._progress(self.n_frames - 1, self.n_frames, f"DONE. {res.summary()}")
         return res
@@ -649,7 +649,36 @@ class SimulationPipeline:
             for k, name in ((PR.C_CATALYTIC, "n_catalytic"), (PR.C_RECRUITED, "n_recruited"),
                             (PR.C_DETACHED, "n_detached"), (PR.C_CONVERTED, "n_converted")):
                 sub[name][i] = c[k] - prev[k]
+            sub["mean_fret_E"][i] = self._mean_fret_E(int(sub["n_complexes"][i]))
             for si, sp in enumerate(self.config.species):
                 sub["species"][sp.name][i] = np.sum((st.species_id == si) & st.is_alive)
             sub["i"] = i + 1
             prev = c
+
+    def _mean_fret_E(self, n_bound: int) -> float:
+        """Mean FRET efficiency over the alive unbleached donors (pipeline.py:587-619):
+        per-donor E from k_FRET in proximity mode, E(r/R0) for bound donors in
+        bond mode."""
+        if not self.config.fret_pairs:
+            return 0.0
+        st = self._state
+        fp = self.config.fret_pairs[0]
+        donors = st.has_dye & st.is_alive & ~st.is_bleached & (st.dye_type_id == 0)
+        n_don = int(np.sum(donors))
+        if n_don == 0:
+            return 0.0
+        if getattr(fp, "fret_mode", "bond") == "proximity":
+            self._photon_sim.update_fret_rates()
+            k = self._photon_sim._k_fret[donors]
+            tau_d = self._photon_sim._tau_all[0]
+            return float(np.mean(k * tau_d / (1.0 + k * tau_d)))
+        e_const = 1.0 / (1.0 + (fp.intra_complex_distance / fp.R0) ** 6)
+        return e_const * n_bound / n_don
+
+    def _subframe_result(self, sub) -> SubFrameData:
+        return SubFrameData(
+            n_complexes=sub["n_complexes"], n_bindings=sub["n_bindings"], n_dissociations=sub["n_dissociations"],
+            n_bleached=sub["n_bleached"], total_photons=sub["total_photons"], mean_fret_E=sub["mean_fret_E"],
+            dt_s=self._dynamics.dt, steps_per_frame=self.n_bd_per_frame, species_counts=sub["species"],
+            n_catalytic=sub["n_catalytic"], n_recruited=sub["n_recruited"], n_detached=sub["n_detached"],
+            n_converted=sub["n_converted"])
