@@ -414,13 +414,6 @@ struct LaneRng {
   __device__ __forceinline__ float uniform() { return ((float)(next() >> 8) + 0.5f) * (1.0f / 16777216.0f); }
 };
 
-// Lane 0's stream seen by the whole warp (warp-uniform draws).
-struct WarpRng {
-  LaneRng& lane_rng;
-  __device__ __forceinline__ uint32_t next() { return __shfl_sync(0xffffffffu, lane_rng.next(), 0); }
-  __device__ __forceinline__ float uniform() { return ((float)(next() >> 8) + 0.5f) * (1.0f / 16777216.0f); }
-};
-
 // Poisson(mu) for mu < 10 by sequential inversion of the CDF with one
 // uniform; the search stops at mu + 12 sqrt(mu) + 12, where the FP32 CDF no
 // longer resolves the tail mass left.
@@ -467,86 +460,90 @@ __device__ __forceinline__ uint32_t poisson(float mu, Rng& rng) {
   return mu < 10.0f ? poisson_small(mu, rng.uniform()) : poisson_ptrs(mu, rng);
 }
 
-// One warp per pixel (grid-stride).  The counts n_b ~ Poisson(mu_b),
-// mu_b = A h_free[b] y_free + B h_bound[b] y_bound, are drawn through the
-// identity "Poisson total, then independent categorical photons": per
-// component c the in-window total N_c ~ Poisson(A_c S_c) (drawn identically
-// by all lanes from lane 0's stream), then each of the
-// N_free + N_bound photons picks its bin from the component's alias table
-// with one 32-bit word of its lane's stream.  Photons are counted in
-// kSub shared-memory copies of the warp's histogram (lane % kSub), four per
-// lane per round so table loads and atomics overlap; the copies are summed
-// into 512-byte coalesced stores.
-constexpr int kSub = 1;
-
+// A warp takes 32 consecutive pixels at a time (grid-stride).  The counts
+// n_b ~ Poisson(mu_b), mu_b = A h_free[b] y_free + B h_bound[b] y_bound, are
+// drawn through the identity "Poisson total, then independent categorical
+// photons":
+//   1. lane l draws, for pixel l of the group, the in-window totals
+//      N_c ~ Poisson(A_c S_c) of both components (stream (pixel, 32)) and
+//      writes its expected mean arrival time;
+//   2. pixel by pixel, the warp places the pixel's N_free + N_bound photons:
+//      each picks its bin from its component's alias table with one 32-bit
+//      word of its lane's stream (stream (pixel, lane)), four per lane per
+//      round so table loads and shared-memory atomics overlap, and the
+//      pixel's histogram leaves in 512-byte coalesced stores.
 __global__ void __launch_bounds__(256, 4) k_hist(EdmFlimParams p, const float* __restrict__ I /*[R][2][256*256]*/,
                                                  const int2* __restrict__ alias, const double* __restrict__ sums,
                                                  uint32_t* __restrict__ hist, double* __restrict__ tau_expected) {
   __shared__ int2 tab[2][256];
-  __shared__ __align__(16) uint32_t wh[8][kSub][256];
+  __shared__ __align__(16) uint32_t wh[8][256];
   const int nb = p.n_bins;
   for (int i = threadIdx.x; i < 2 * nb; i += blockDim.x) tab[i / nb][i % nb] = alias[i];
   __syncthreads();
   const double Tf = sums[0], Sf = sums[1], Tb = sums[2], Sb = sums[3];
+  const unsigned FULL = 0xffffffffu;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int shift = nb == 256 ? 24 : 25;  // top bits of a word pick the cell
-  uint32_t* h = wh[warp][lane % kSub];
+  uint32_t* h = wh[warp];
   const uint32_t npx = (uint32_t)kDim * kDim;
   const uint32_t total = npx * (uint32_t)p.n_replicas;
   // pixel index over all replicas: at most 4096 x 2^16 = 2^28, so 32 bits
-  // hold it and the replica / pixel split is a shift and a mask
+  // hold it and the replica / pixel split is a shift and a mask; a group of
+  // 32 aligned pixels never straddles two replicas
   static_assert(kDim * kDim == 1 << 16, "pixel split assumes 2^16 pixels per replica");
-  for (uint32_t gpx = blockIdx.x * 8u + (uint32_t)warp; gpx < total; gpx += gridDim.x * 8u) {
-    const uint32_t r = gpx >> 16;
-    const uint32_t px = gpx & 0xFFFFu;
-    const float A = I[((size_t)r * 2 + 0) * npx + px];
-    const float B = I[((size_t)r * 2 + 1) * npx + px];
+  for (uint32_t g0 = (blockIdx.x * 8u + (uint32_t)warp) * 32u; g0 < total; g0 += gridDim.x * 8u * 32u) {
+    const uint32_t r = g0 >> 16;
     const uint64_t seed = edm_flim_replica_seed(p.seed, (int32_t)r);
-    LaneRng rng(seed, r, px, (uint32_t)lane);
-    WarpRng pixel_rng{rng};  // the totals: lane 0's first draws, in every lane
-    const int n_free = (int)poisson(fmaxf(0.0f, A) * (float)Sf, pixel_rng);
-    const int n_all = n_free + (int)poisson(fmaxf(0.0f, B) * (float)Sb, pixel_rng);
+    // ---- 1. this lane's pixel of the group: totals and expected lifetime
+    int n_free = 0, n_all = 0;
     {
-      uint4* z = (uint4*)wh[warp];
-      for (int i = lane; i < kSub * nb / 4; i += 32) z[i] = make_uint4(0u, 0u, 0u, 0u);
-    }
-    __syncwarp();
-    // photons lane, lane + 32, ...: four per round
-    int i = lane;
-    for (; i + 96 < n_all; i += 128) {
-      uint32_t w[4];
-      int2 e[4];
-#pragma unroll
-      for (int k = 0; k < 4; ++k) w[k] = rng.next();
-#pragma unroll
-      for (int k = 0; k < 4; ++k) e[k] = tab[i + 32 * k < n_free ? 0 : 1][w[k] >> shift];
-#pragma unroll
-      for (int k = 0; k < 4; ++k)
-        atomicAdd(&h[(int)(w[k] & 0xFFFFFFu) < e[k].x ? (int)(w[k] >> shift) : e[k].y], 1u);
-    }
-    for (; i < n_all; i += 32) {
-      const uint32_t w = rng.next();
-      const int2 e = tab[i < n_free ? 0 : 1][w >> shift];
-      atomicAdd(&h[(int)(w & 0xFFFFFFu) < e.x ? (int)(w >> shift) : e.y], 1u);
-    }
-    __syncwarp();
-    uint4* out = (uint4*)(hist + (size_t)gpx * (size_t)nb);
-    for (int q = lane; q < nb / 4; q += 32) {
-      uint4 v = ((const uint4*)wh[warp][0])[q];
-#pragma unroll
-      for (int c = 1; c < kSub; ++c) {
-        const uint4 u = ((const uint4*)wh[warp][c])[q];
-        v.x += u.x;
-        v.y += u.y;
-        v.z += u.z;
-        v.w += u.w;
+      const uint32_t gl = g0 + (uint32_t)lane;
+      if (gl < total) {
+        const uint32_t px = gl & 0xFFFFu;
+        const float A = I[((size_t)r * 2 + 0) * npx + px];
+        const float B = I[((size_t)r * 2 + 1) * npx + px];
+        LaneRng trng(seed, r, px, 32u);
+        n_free = (int)poisson(fmaxf(0.0f, A) * (float)Sf, trng);
+        n_all = n_free + (int)poisson(fmaxf(0.0f, B) * (float)Sb, trng);
+        if (tau_expected != nullptr) {
+          const double den = (double)A * Sf + (double)B * Sb;
+          tau_expected[gl] = den > 0.0 ? ((double)A * Tf + (double)B * Tb) / den : 0.0;
+        }
       }
-      out[q] = v;
     }
-    __syncwarp();
-    if (tau_expected != nullptr && lane == 0) {
-      const double den = (double)A * Sf + (double)B * Sb;
-      tau_expected[gpx] = den > 0.0 ? ((double)A * Tf + (double)B * Tb) / den : 0.0;
+    // ---- 2. the photons of each pixel of the group
+    const int np = total - g0 < 32u ? (int)(total - g0) : 32;
+    for (int q = 0; q < np; ++q) {
+      const uint32_t gpx = g0 + (uint32_t)q;
+      const uint32_t px = gpx & 0xFFFFu;
+      const int nf = __shfl_sync(FULL, n_free, q), na = __shfl_sync(FULL, n_all, q);
+      {
+        uint4* z = (uint4*)h;
+        for (int i = lane; i < nb / 4; i += 32) z[i] = make_uint4(0u, 0u, 0u, 0u);
+      }
+      __syncwarp();
+      LaneRng rng(seed, r, px, (uint32_t)lane);
+      int i = lane;
+      for (; i + 96 < na; i += 128) {
+        uint32_t w[4];
+        int2 e[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) w[k] = rng.next();
+#pragma unroll
+        for (int k = 0; k < 4; ++k) e[k] = tab[i + 32 * k < nf ? 0 : 1][w[k] >> shift];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          atomicAdd(&h[(int)(w[k] & 0xFFFFFFu) < e[k].x ? (int)(w[k] >> shift) : e[k].y], 1u);
+      }
+      for (; i < na; i += 32) {
+        const uint32_t w = rng.next();
+        const int2 e = tab[i < nf ? 0 : 1][w >> shift];
+        atomicAdd(&h[(int)(w & 0xFFFFFFu) < e.x ? (int)(w >> shift) : e.y], 1u);
+      }
+      __syncwarp();
+      uint4* out = (uint4*)(hist + (size_t)gpx * (size_t)nb);
+      for (int i2 = lane; i2 < nb / 4; i2 += 32) out[i2] = ((const uint4*)h)[i2];
+      __syncwarp();
     }
   }
 }
