@@ -301,10 +301,11 @@ def flim_bench(args, device: int, rank: int, world: int, stream):
     peak, peak_kind = peaks()
     achieved = FLIM_BYTES_PER_PX * R * 65536 / (hist_ms / 1e3) / 1e9
     gemm_flops = 2 * (2 * 2 * 256 ** 3) * R  # two maps, two 256^3 products each (algorithmic)
-    traffic = None
+    traffic = ro_traffic = None
     tr_file = ROOT / "profiles" / "traffic.json"
-    if tr_file.exists() and R == 256:  # the committed figure is for 256 replicas
-        traffic = json.loads(tr_file.read_text()).get("hist")
+    if tr_file.exists() and R == 256:  # the committed figures are for 256 replicas
+        tr = json.loads(tr_file.read_text())
+        traffic, ro_traffic = tr.get("hist"), tr.get("readout")
     err = acq.error_word()
 
     # e2e: host bound fractions in, every histogram out to pinned host memory
@@ -341,7 +342,7 @@ def flim_bench(args, device: int, rank: int, world: int, stream):
                     "px_per_s": R * 65536 / (ro_ms / 1e3),
                     "roofline": {"bound": "hbm", "achieved": ro_bytes / (ro_ms / 1e3) / 1e9, "peak": peak,
                                  "unit": "GB/s", "frac": ro_bytes / (ro_ms / 1e3) / 1e9 / peak,
-                                 "alg_bytes_per_px": 256 * 4 + 6 * 8}},
+                                 "traffic": ro_traffic, "alg_bytes_per_px": 256 * 4 + 6 * 8}},
         "gpu_launches": 5 * args.steps, "error_word": err, "clocks": clk.summary(),
         "l2": "histograms 17 GB per acquisition >> 126 MB L2",
     }
