@@ -53,6 +53,7 @@ struct DevState {
   int32_t* grid_cnt;     // density-grid counts (snapshot of the current pass)
   int32_t* grid_delta;   // pending changes of the current pass
   const double* hill;
+  const double* rule_max;  // [R][EDM_MAX_RULES] upper bound of each rule's Hill factor
   int64_t* counters;     // [R][EDM_NCOUNTERS]
   uint32_t* status;
   const int64_t* d_step;
@@ -73,6 +74,11 @@ struct DevState {
   // (recruited, or placed by dissociation): per replica at particle_offset
   int32_t* moved;
   int32_t* moved_count;  // [R]
+  // particles whose keyed draws pass some per-particle pass's bound this step:
+  // (slot, bit mask of those passes); pl_index[slot] = its entry
+  int2* pl;
+  int32_t* pl_count;
+  int32_t* pl_index;
   int n_rep;
   int64_t n_slots;
 };
@@ -87,14 +93,13 @@ __device__ __forceinline__ int replica_of(const int64_t* __restrict__ rep_first,
   return lo;
 }
 
-// Particles a per-particle pass visits: species in `species_mask` and alive
-// (alive = 1) or not alive (alive = 0).
+// Particles a per-particle pass visits: the species set mask[1] of alive
+// particles and mask[0] of particles that are not alive.
 struct Match {
-  uint32_t species_mask;
-  int alive;
+  uint32_t mask[2];
 };
 __device__ __forceinline__ bool matches(uint8_t f, const Match& m) {
-  return ((m.species_mask >> fl_species(f)) & 1u) && (fl_alive(f) == (m.alive != 0));
+  return ((fl_alive(f) ? m.mask[1] : m.mask[0]) >> fl_species(f)) & 1u;
 }
 
 // Flag sweep with warp-local compaction: each warp reads the flags of its
@@ -328,6 +333,16 @@ __device__ __forceinline__ double rule_factor(const EdmDynParams& p, int rule, c
   const EdmRule& R = p.rule[rule];
   const int k = st.grid_cnt[grid_cell_of(p.grid[R.grid], x, y)];
   return hill_of(R, st.hill, k, st.status);
+}
+
+// An upper bound of prob * rule_factor(rule) [* rule_factor(rule2)] for the
+// replica (rule -1: no factor).  Rounded products are monotone in their
+// factors, so a keyed draw u with u >= the bound is rejected whatever the
+// grid counts; the passes test it before they fetch positions and counts.
+__device__ __forceinline__ double prob_bound(const DevState& st, int r, double prob, int rule, int rule2 = -1) {
+  if (rule >= 0) prob = prob * st.rule_max[(int64_t)r * EDM_MAX_RULES + rule];
+  if (rule2 >= 0) prob = prob * st.rule_max[(int64_t)r * EDM_MAX_RULES + rule2];
+  return prob;
 }
 
 // Grid bookkeeping of a particle changing (species, alive) at one position.
@@ -890,6 +905,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_catalytic(const EdmDynParams* __r
     const int ide = st.ids[es.x] - (int)g.poff, ids = st.ids[es.y] - (int)g.poff;
     const uint32_t lo = ide < ids ? ide : ids, hi = ide < ids ? ids : ide;
     const double u = uniform1(p.seed, *st.d_step, EDM_S_CAT + cidx, lo, hi);
+    if (!(u < prob_bound(st, r, C.prob, C.rule))) continue;
     double xs, ys;
     abs_pos<F64>(st.pos_post, st.cell_post, es.y, g, xs, ys);
     double peff = C.prob;
@@ -903,41 +919,76 @@ __global__ void __launch_bounds__(kBlock, 8) k_catalytic(const EdmDynParams* __r
   }
 }
 
-// Recruitment candidates of exchange e (dynamics.py:1229-1458): dormant
-// particles of the species whose keyed draw accepts at the keyed position.
-template <bool F64>
-__global__ void __launch_bounds__(kBlock, 8) k_recruit_candidates(const EdmDynParams* __restrict__ P, DevState st,
-                                                               Match m, int e) {
-  sweep4(st, m, [&](int r, int64_t s) {
+// ---- per-particle passes: recruitment candidates, detachments, conversions ----
+// Each decides for one particle from its flags, its keyed draw u, and (only
+// when u is below the pass's probability bound, prob_bound) its position and
+// the grid counts.  A step draws every particle's u once, for every such pass
+// the particle can still reach, in one sweep placed before the first of them
+// (k_pass_draws); the few particles with some u below its bound go to a list,
+// and the passes visit only that list.  A particle that is not listed for a
+// pass would be rejected by it, so skipping it changes nothing.
+constexpr int kMaxPP = 32;
+enum GroupPass : int8_t { kGroupRecruit = 0, kGroupDetach = 1, kGroupConvert = 2 };
+struct DrawPlan {
+  Match any;                             // states that reach some pass
+  uint32_t reach[2][EDM_MAX_SPECIES];    // passes reachable from (alive, species)
+  int8_t kind[kMaxPP];                   // GroupPass of each per-particle pass
+  int8_t index[kMaxPP];                  // its exchange or conversion
+  int n;
+};
+
+// Whether the keyed draw of per-particle pass (kind, idx) for local id `id`
+// lies below the pass's probability bound (otherwise the pass rejects).
+__device__ __forceinline__ bool pass_may_accept(const EdmDynParams& p, const DevState& st, int r, int id, int kind,
+                                                int idx, int64_t step) {
+  if (kind == kGroupRecruit) {
+    const EdmExch& X = p.exch[idx];
+    const double u = uniform1(p.seed, step, EDM_S_EX_ACCEPT + 4 * idx, (uint64_t)id, 0);
+    return u < prob_bound(st, r, X.prob_on, X.rule_on, X.rule_on >= 0 ? X.rule_on2 : -1);
+  }
+  if (kind == kGroupDetach) {
+    const EdmExch& X = p.exch[idx];
+    const double u = uniform1(p.seed, step, EDM_S_EX_DETACH + 4 * idx, (uint64_t)id, 0);
+    return u < prob_bound(st, r, X.prob_off, X.rule_off);
+  }
+  const EdmConv& V = p.conv[idx];
+  const double u = uniform1(p.seed, step, EDM_S_CONV + idx, (uint64_t)id, 0);
+  return u < prob_bound(st, r, V.prob, V.rule);
+}
+
+__global__ void __launch_bounds__(kBlock, 8) k_pass_draws(const EdmDynParams* __restrict__ P, DevState st,
+                                                       DrawPlan D) {
+  __shared__ DrawPlan sd;
+  if (threadIdx.x == 0) sd = D;
+  __syncthreads();
+  sweep4(st, sd.any, [&](int r, int64_t s) {
     const EdmDynParams& p = P[r];
-    const EdmExch& X = p.exch[e];
+    const uint8_t f = st.flags[s];
+    const int sp = fl_species(f);
+    uint32_t todo = sp < EDM_MAX_SPECIES ? sd.reach[fl_alive(f) ? 1 : 0][sp] : 0u;
     const int id = st.ids[s] - (int)p.particle_offset;
     const int64_t step = *st.d_step;
-    const double ua = uniform1(p.seed, step, EDM_S_EX_ACCEPT + 4 * e, (uint64_t)id, 0);
-    const U2 up = uniform2(p.seed, step, EDM_S_EX_POS + 4 * e, (uint64_t)id, 0);
-    const double cx = up.u0 * p.Lx, cy = up.u1 * p.Ly;
-    double peff = X.prob_on;
-    if (X.rule_on >= 0 && X.rule_on2 >= 0) {
-      peff = X.prob_on * rule_factor(p, X.rule_on, st, cx, cy) * rule_factor(p, X.rule_on2, st, cx, cy);
-    } else if (X.rule_on >= 0) {
-      peff = X.prob_on * rule_factor(p, X.rule_on, st, cx, cy);
+    uint32_t bits = 0;
+    for (; todo; todo &= todo - 1) {
+      const int k = __ffs(todo) - 1;
+      if (pass_may_accept(p, st, r, id, sd.kind[k], sd.index[k], step)) bits |= 1u << k;
     }
-    if (ua < peff) {
-      const int k = atomicAdd(&st.rec_count[r], 1);
-      if (k < kRecCap) {
-        st.rec_id[(int64_t)r * kRecCap + k] = id;
-        st.rec_xy[((int64_t)r * kRecCap + k) * 2] = cx;
-        st.rec_xy[((int64_t)r * kRecCap + k) * 2 + 1] = cy;
-      } else {
-        set_status(st.status, EDM_STATUS_RECRUIT_CAP);
-      }
+    if (bits) {
+      const int q = atomicAdd(st.pl_count, 1);
+      st.pl[q] = make_int2((int)s, (int)bits);
+      st.pl_index[s] = q;
     }
   });
 }
 
 // Apply the first max_recruits accepted candidates in particle order.
+// A recruited particle is alive from here on, so the passes after this one
+// that it can reach (`after`) get its draws now, in its list entry (the
+// entry exists: the particle was listed for this exchange's candidates);
+// `keep` holds the bits of the passes before.
 template <bool F64>
-__global__ void k_recruit_apply(const EdmDynParams* __restrict__ P, int n_rep, DevState st, int e) {
+__global__ void k_recruit_apply(const EdmDynParams* __restrict__ P, int n_rep, DevState st, int e, DrawPlan D,
+                                uint32_t after, uint32_t keep) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n_rep) return;
   const EdmDynParams& p = P[r];
@@ -979,51 +1030,143 @@ __global__ void k_recruit_apply(const EdmDynParams* __restrict__ P, int n_rep, D
     st.flags[slot] = fl_make(X.species, true);
     note_moved(st, r, p, slot);
     grid_add(p, st.grid_delta, X.species, x, y, 1);
+    if (after) {
+      const int64_t step = *st.d_step;
+      uint32_t bits = 0;
+      for (uint32_t todo = after; todo; todo &= todo - 1) {
+        const int k = __ffs(todo) - 1;
+        if (pass_may_accept(p, st, r, ids[a], D.kind[k], D.index[k], step)) bits |= 1u << k;
+      }
+      const int q = st.pl_index[slot];
+      if (q >= 0 && q < *st.pl_count && st.pl[q].x == (int)slot) st.pl[q].y = (int)(((uint32_t)st.pl[q].y & keep) | bits);
+      else set_status(st.status, EDM_STATUS_RECRUIT_CAP);
+    }
   }
   atomic_add_i64(&st.counters[(int64_t)r * EDM_NCOUNTERS + EDM_C_RECRUITED], take);
 }
 
-// Detachment of exchange e (dynamics.py:1461-1555).
-template <bool F64>
-__global__ void __launch_bounds__(kBlock, 8) k_detach(const EdmDynParams* __restrict__ P, DevState st, Match m, int e) {
-  sweep4(st, m, [&](int r, int64_t s) {
-    const EdmDynParams& p = P[r];
-    const EdmExch& X = p.exch[e];
-    const Geo g(p);
-    const int id = st.ids[s] - (int)g.poff;
-    double x, y;
-    abs_pos<F64>(st.pos_post, st.cell_post, s, g, x, y);
-    double peff = X.prob_off;
-    if (X.rule_off >= 0) peff = X.prob_off * rule_factor(p, X.rule_off, st, x, y);
-    const double u = uniform1(p.seed, *st.d_step, EDM_S_EX_DETACH + 4 * e, (uint64_t)id, 0);
-    if (u < peff) {
-      st.flags[s] = fl_make(X.species, false);
-      rebucket(st, g, st.cell_post[s], g.grave);
-      atomic_add_i64(&st.counters[(int64_t)r * EDM_NCOUNTERS + EDM_C_DETACHED], 1);
-      grid_add(p, st.grid_delta, X.species, x, y, -1);
+// Recruitment candidate of exchange e (dynamics.py:1229-1458): a dormant
+// particle of the species whose keyed draw accepts at the keyed position.
+__device__ __forceinline__ void recruit_candidate(const EdmDynParams& p, const DevState& st, int r, int id, int e) {
+  const EdmExch& X = p.exch[e];
+  const int64_t step = *st.d_step;
+  const double ua = uniform1(p.seed, step, EDM_S_EX_ACCEPT + 4 * e, (uint64_t)id, 0);
+  if (!(ua < prob_bound(st, r, X.prob_on, X.rule_on, X.rule_on >= 0 ? X.rule_on2 : -1))) return;
+  const U2 up = uniform2(p.seed, step, EDM_S_EX_POS + 4 * e, (uint64_t)id, 0);
+  const double cx = up.u0 * p.Lx, cy = up.u1 * p.Ly;
+  double peff = X.prob_on;
+  if (X.rule_on >= 0 && X.rule_on2 >= 0) {
+    peff = X.prob_on * rule_factor(p, X.rule_on, st, cx, cy) * rule_factor(p, X.rule_on2, st, cx, cy);
+  } else if (X.rule_on >= 0) {
+    peff = X.prob_on * rule_factor(p, X.rule_on, st, cx, cy);
+  }
+  if (ua < peff) {
+    const int k = atomicAdd(&st.rec_count[r], 1);
+    if (k < kRecCap) {
+      st.rec_id[(int64_t)r * kRecCap + k] = id;
+      st.rec_xy[((int64_t)r * kRecCap + k) * 2] = cx;
+      st.rec_xy[((int64_t)r * kRecCap + k) * 2 + 1] = cy;
+    } else {
+      set_status(st.status, EDM_STATUS_RECRUIT_CAP);
     }
-  });
+  }
 }
 
-// Unimolecular conversion v (dynamics.py:1565-1657).
+// Position of slot s after the move, fetched once for the passes that need it.
 template <bool F64>
-__global__ void __launch_bounds__(kBlock, 8) k_convert(const EdmDynParams* __restrict__ P, DevState st, Match m, int v) {
-  sweep4(st, m, [&](int r, int64_t s) {
+struct LazyPos {
+  bool have = false;
+  double x = 0.0, y = 0.0;
+  __device__ __forceinline__ void get(const DevState& st, int64_t s, const Geo& g) {
+    if (!have) abs_pos<F64>(st.pos_post, st.cell_post, s, g, x, y);
+    have = true;
+  }
+};
+
+// Detachment of exchange e (dynamics.py:1461-1555) of the alive particle in
+// slot s; returns its flags afterwards.
+template <bool F64>
+__device__ __forceinline__ uint8_t detach_one(const EdmDynParams& p, const Geo& g, const DevState& st, int r,
+                                              int64_t s, int id, LazyPos<F64>& pos, int e, uint8_t f) {
+  const EdmExch& X = p.exch[e];
+  const double u = uniform1(p.seed, *st.d_step, EDM_S_EX_DETACH + 4 * e, (uint64_t)id, 0);
+  if (!(u < prob_bound(st, r, X.prob_off, X.rule_off))) return f;
+  pos.get(st, s, g);
+  double peff = X.prob_off;
+  if (X.rule_off >= 0) peff = X.prob_off * rule_factor(p, X.rule_off, st, pos.x, pos.y);
+  if (u < peff) {
+    f = fl_make(X.species, false);
+    st.flags[s] = f;
+    rebucket(st, g, st.cell_post[s], g.grave);
+    atomic_add_i64(&st.counters[(int64_t)r * EDM_NCOUNTERS + EDM_C_DETACHED], 1);
+    grid_add(p, st.grid_delta, X.species, pos.x, pos.y, -1);
+  }
+  return f;
+}
+
+// Unimolecular conversion v (dynamics.py:1565-1657) of the alive particle in
+// slot s; returns its flags afterwards.
+template <bool F64>
+__device__ __forceinline__ uint8_t convert_one(const EdmDynParams& p, const Geo& g, const DevState& st, int r,
+                                               int64_t s, int id, LazyPos<F64>& pos, int v, uint8_t f) {
+  const EdmConv& V = p.conv[v];
+  const double u = uniform1(p.seed, *st.d_step, EDM_S_CONV + v, (uint64_t)id, 0);
+  if (!(u < prob_bound(st, r, V.prob, V.rule))) return f;
+  pos.get(st, s, g);
+  double peff = V.prob;
+  if (V.rule >= 0) peff = V.prob * rule_factor(p, V.rule, st, pos.x, pos.y);
+  if (u < peff) {
+    f = fl_make(V.to, true);
+    st.flags[s] = f;
+    atomic_add_i64(&st.counters[(int64_t)r * EDM_NCOUNTERS + EDM_C_CONVERTED], 1);
+    grid_change(p, st.grid_delta, V.from, true, V.to, true, pos.x, pos.y);
+  }
+  return f;
+}
+
+// A run of consecutive per-particle passes over the listed particles.  Each
+// of these passes decides for a particle from its own flags, position and
+// keyed draws and from the grid counts, which no pass of the run changes
+// (their grid changes go to the delta grid), and a particle's flags change
+// only in its own passes.  So taking every listed particle through the run's
+// passes in order gives the result of the passes one after another.
+constexpr int kMaxGroup = 16;
+struct PassGroup {
+  Match m[kMaxGroup];      // particles each pass visits
+  int8_t kind[kMaxGroup];  // GroupPass
+  int8_t index[kMaxGroup]; // exchange or conversion index
+  int8_t pp[kMaxGroup];    // the pass's bit in the list entries
+  uint32_t bits;           // union of the passes' bits
+  int n;
+};
+
+template <bool F64>
+__global__ void __launch_bounds__(kBlock) k_particle_passes(const EdmDynParams* __restrict__ P, DevState st,
+                                                            PassGroup G) {
+  __shared__ PassGroup sg;
+  if (threadIdx.x == 0) sg = G;
+  __syncthreads();
+  const int n = *st.pl_count;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const int2 e = st.pl[q];
+    const uint32_t bits = (uint32_t)e.y;
+    if (!(bits & sg.bits)) continue;
+    const int64_t s = e.x;
+    int r = st.chunk_rep[s / kSweepChunk];
+    while (r + 1 < st.n_rep && st.rep_first[r + 1] <= s) ++r;
     const EdmDynParams& p = P[r];
-    const EdmConv& V = p.conv[v];
     const Geo g(p);
     const int id = st.ids[s] - (int)g.poff;
-    double x, y;
-    abs_pos<F64>(st.pos_post, st.cell_post, s, g, x, y);
-    double peff = V.prob;
-    if (V.rule >= 0) peff = V.prob * rule_factor(p, V.rule, st, x, y);
-    const double u = uniform1(p.seed, *st.d_step, EDM_S_CONV + v, (uint64_t)id, 0);
-    if (u < peff) {
-      st.flags[s] = fl_make(V.to, true);
-      atomic_add_i64(&st.counters[(int64_t)r * EDM_NCOUNTERS + EDM_C_CONVERTED], 1);
-      grid_change(p, st.grid_delta, V.from, true, V.to, true, x, y);
+    uint8_t f = st.flags[s];
+    LazyPos<F64> pos;  // these passes move no particle
+    for (int k = 0; k < sg.n; ++k) {
+      if (!((bits >> sg.pp[k]) & 1u) || !matches(f, sg.m[k])) continue;
+      const int kind = sg.kind[k], idx = sg.index[k];
+      if (kind == kGroupRecruit) recruit_candidate(p, st, r, id, idx);
+      else if (kind == kGroupDetach) f = detach_one<F64>(p, g, st, r, s, id, pos, idx, f);
+      else f = convert_one<F64>(p, g, st, r, s, id, pos, idx, f);
     }
-  });
+  }
 }
 
 // Binding candidates of reaction b (dynamics.py:528-606): pairs (i < j)

@@ -38,7 +38,8 @@ int fail(int code, const std::string& msg) { return edm::report_error(code, msg)
     if (_e != cudaSuccess) return fail(EDM_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
   } while (0)
 
-enum PassKind { P_BIND_CAND, P_BIND_APPLY, P_DISSOC, P_CONTACTS, P_CAT, P_REC_CAND, P_REC_APPLY, P_DETACH, P_CONV, P_MERGE };
+enum PassKind { P_BIND_CAND, P_BIND_APPLY, P_DISSOC, P_CONTACTS, P_CAT, P_REC_CAND, P_REC_APPLY, P_DETACH, P_CONV, P_MERGE,
+                P_GROUP, P_DRAWS };
 struct Pass {
   PassKind kind;
   int index;
@@ -77,6 +78,7 @@ struct EdmEngine {
   EdmPhotParams* pp = nullptr;
   EdmScopeParams* sp = nullptr;
   double* hill = nullptr;
+  double* rule_max = nullptr;  // [R][EDM_MAX_RULES]
   int2 *pblk = nullptr, *eblk = nullptr, *phblk = nullptr, *pxblk = nullptr;
   int npblk = 0, neblk = 0, nphblk = 0, npxblk = 0;
   void* pos_pre = nullptr;
@@ -112,6 +114,9 @@ struct EdmEngine {
   uint8_t *st_alive = nullptr, *st_bl = nullptr;
   int8_t* st_ctmc = nullptr;
   std::vector<Pass> passes;
+  std::vector<PassGroup> groups;  // runs of per-particle passes (P_GROUP index)
+  DrawPlan draw{};                // the draw sweep of the per-particle passes
+  uint32_t rec_after[EDM_MAX_EXCH] = {}, rec_keep[EDM_MAX_EXCH] = {};  // per recruitment apply
   int2* contacts = nullptr;
   int32_t* contact_count = nullptr;
   int64_t contact_cap = 0;
@@ -120,6 +125,8 @@ struct EdmEngine {
   int64_t* rep_first = nullptr;
   int32_t* chunk_rep = nullptr;  // replica of the first slot of each 128-slot chunk
   int32_t *moved = nullptr, *moved_count = nullptr;
+  int2* pl = nullptr;  // listed particles of the per-particle passes: (slot, pass bits)
+  int32_t *pl_count = nullptr, *pl_index = nullptr;
   std::vector<int32_t> emit_host;  // emitter list last uploaded
   std::vector<uint8_t> has_dye_host;  // has_dye of the last edm_set_state
   bool cells_valid = false;  // the cell list matches the state (a dynamics step ran since set_state)
@@ -144,6 +151,7 @@ struct EdmEngine {
     s.grid_cnt = grid_cnt;
     s.grid_delta = grid_delta;
     s.hill = hill;
+    s.rule_max = rule_max;
     s.counters = counters;
     s.status = status;
     s.d_step = d_step;
@@ -160,6 +168,9 @@ struct EdmEngine {
     s.chunk_rep = chunk_rep;
     s.moved = moved;
     s.moved_count = moved_count;
+    s.pl = pl;
+    s.pl_count = pl_count;
+    s.pl_index = pl_index;
     s.n_rep = R;
     s.n_slots = N;
     return s;
@@ -209,10 +220,8 @@ struct EdmEngine {
       return gs;
     };
     auto match = [](std::vector<int> species, int alive) {
-      Match m;
-      m.species_mask = 0;
-      for (int s : species) m.species_mask |= 1u << s;
-      m.alive = alive;
+      Match m{};
+      for (int s : species) m.mask[alive ? 1 : 0] |= 1u << s;
       return m;
     };
     const Match none = match({}, 1);
@@ -252,10 +261,7 @@ struct EdmEngine {
       }
       for (int c = 0; c < p.n_cat; ++c) cat_lists.partners_of[p.cat[c].enzyme] |= cat_lists.capable[c];
       if (enzyme_mask & touched) return fail(EDM_EUNSUP, "an enzyme species is also a catalytic substrate/product");
-      Match m;
-      m.species_mask = enzyme_mask;
-      m.alive = 1;
-      passes.push_back({P_CONTACTS, 0, m});
+      passes.push_back({P_CONTACTS, 0, Match{{0u, enzyme_mask}}});
     }
     // A pass whose probability is zero in every replica changes nothing (its
     // keyed draws feed no other pass), so it is not scheduled.
@@ -289,11 +295,98 @@ struct EdmEngine {
       passes.push_back({P_CONV, v, match({p.conv[v].from}, 1)});
       writes({p.conv[v].from, p.conv[v].to});
     }
+    return fuse_particle_passes();
+  }
+
+  // The per-particle passes (recruitment candidates, detachments,
+  // conversions) get one draw sweep (k_pass_draws) before the first of them;
+  // runs of consecutive ones become list passes (k_particle_passes).  The
+  // sweep draws, for each particle, the passes it can reach from its state:
+  // a detachment turns alive X into dormant X and a conversion alive `from`
+  // into alive `to`; a recruitment apply draws the later passes of the
+  // particles it recruits itself.
+  int fuse_particle_passes() {
+    auto per_particle = [](PassKind k) { return k == P_REC_CAND || k == P_DETACH || k == P_CONV; };
+    const EdmDynParams& p = hdp[0];
+    std::vector<int> pp_of(passes.size(), -1);
+    int n_pp = 0;
+    size_t first = passes.size();
+    for (size_t i = 0; i < passes.size(); ++i)
+      if (per_particle(passes[i].kind)) {
+        if (first == passes.size()) first = i;
+        pp_of[i] = n_pp++;
+      }
+    groups.clear();
+    draw = DrawPlan{};
+    if (n_pp == 0) return EDM_OK;
+    if (n_pp > kMaxPP) return fail(EDM_EUNSUP, "more than 32 recruitment/detachment/conversion passes");
+    draw.n = n_pp;
+    for (size_t i = 0; i < passes.size(); ++i) {
+      if (pp_of[i] < 0) continue;
+      const PassKind k = passes[i].kind;
+      draw.kind[pp_of[i]] = k == P_REC_CAND ? kGroupRecruit : (k == P_DETACH ? kGroupDetach : kGroupConvert);
+      draw.index[pp_of[i]] = (int8_t)passes[i].index;
+    }
+    auto state = [](int sp, int alive) { return 1u << (alive * EDM_MAX_SPECIES + sp); };
+    // per-particle passes from position `from` on that a particle in one of the states R can reach
+    auto reach_from = [&](size_t from, uint32_t R) {
+      uint32_t mask = 0;
+      for (size_t i = from; i < passes.size(); ++i) {
+        if (pp_of[i] < 0) continue;
+        const Pass& ps = passes[i];
+        const uint32_t M = (ps.match.mask[1] << EDM_MAX_SPECIES) | (ps.match.mask[0] & ((1u << EDM_MAX_SPECIES) - 1));
+        if (!(R & M)) continue;
+        mask |= 1u << pp_of[i];
+        if (ps.kind == P_DETACH) {
+          const int x = p.exch[ps.index].species;
+          if (R & state(x, 1)) R |= state(x, 0);
+        } else if (ps.kind == P_CONV) {
+          const EdmConv& V = p.conv[ps.index];
+          if (R & state(V.from, 1)) R |= state(V.to, 1);
+        }
+      }
+      return mask;
+    };
+    for (int alive = 0; alive < 2; ++alive)
+      for (int sp = 0; sp < p.n_species; ++sp) {
+        draw.reach[alive][sp] = reach_from(first, state(sp, alive));
+        if (draw.reach[alive][sp]) draw.any.mask[alive] |= 1u << sp;
+      }
+    std::vector<Pass> fused;
+    int pp_before = 0;
+    for (size_t i = 0; i < passes.size();) {
+      if (i == first) fused.push_back({P_DRAWS, 0, draw.any});
+      if (!per_particle(passes[i].kind)) {
+        if (passes[i].kind == P_REC_APPLY) {
+          const int e = passes[i].index;
+          rec_after[e] = reach_from(i + 1, state(p.exch[e].species, 1));
+          rec_keep[e] = pp_before >= 32 ? ~0u : (1u << pp_before) - 1u;
+        }
+        fused.push_back(passes[i++]);
+        continue;
+      }
+      PassGroup G{};
+      while (i < passes.size() && per_particle(passes[i].kind) && G.n < kMaxGroup) {
+        const int k = pp_of[i];
+        G.kind[G.n] = draw.kind[k];
+        G.index[G.n] = draw.index[k];
+        G.pp[G.n] = (int8_t)k;
+        G.m[G.n] = passes[i].match;
+        G.bits |= 1u << k;
+        ++G.n;
+        ++pp_before;
+        ++i;
+      }
+      groups.push_back(G);
+      fused.push_back({P_GROUP, (int)groups.size() - 1, Match{}});
+    }
+    passes.swap(fused);
     return EDM_OK;
   }
 
-  // optional CUDA events between kernel groups (profiling only)
+  // optional CUDA events between kernel groups and between reaction passes (profiling only)
   cudaEvent_t* prof = nullptr;
+  cudaEvent_t* pass_prof = nullptr;
   void mark(int k, cudaStream_t s) {
     if (prof) cudaEventRecord(prof[k], s);
   }
@@ -321,7 +414,9 @@ struct EdmEngine {
     const int sgrid = (int)std::max<int64_t>(1, (N / 4 + kBlock) / kBlock);  // 4 slots per thread
     const int cgrid = 148 * 8;
     const int gm = (int)std::min<int64_t>((n_grid + 255) / 256, 4096);
-    for (const Pass& ps : passes) {
+    for (size_t i = 0; i < passes.size(); ++i) {
+      const Pass& ps = passes[i];
+      if (pass_prof) cudaEventRecord(pass_prof[i], s);
       switch (ps.kind) {
         case P_BIND_CAND: k_bind_candidates<F64><<<sgrid, kBlock, 0, s>>>(dp, st, ps.match, ps.index); break;
         case P_BIND_APPLY: k_bind_apply<F64><<<rb, 128, 0, s>>>(dp, R, st, ps.index); break;
@@ -331,13 +426,21 @@ struct EdmEngine {
           k_contacts<F64><<<sgrid, kBlock, 0, s>>>(dp, st, ps.match, cat_lists);
           break;
         case P_CAT: k_catalytic<F64><<<cgrid, kBlock, 0, s>>>(dp, st, ps.index); break;
-        case P_REC_CAND: k_recruit_candidates<F64><<<sgrid, kBlock, 0, s>>>(dp, st, ps.match, ps.index); break;
-        case P_REC_APPLY: k_recruit_apply<F64><<<rb, 128, 0, s>>>(dp, R, st, ps.index); break;
-        case P_DETACH: k_detach<F64><<<sgrid, kBlock, 0, s>>>(dp, st, ps.match, ps.index); break;
-        case P_CONV: k_convert<F64><<<sgrid, kBlock, 0, s>>>(dp, st, ps.match, ps.index); break;
+        case P_REC_APPLY:
+          k_recruit_apply<F64><<<rb, 128, 0, s>>>(dp, R, st, ps.index, draw, rec_after[ps.index], rec_keep[ps.index]);
+          break;
+        case P_DRAWS:
+          cudaMemsetAsync(pl_count, 0, sizeof(int32_t), s);
+          k_pass_draws<<<sgrid, kBlock, 0, s>>>(dp, st, draw);
+          break;
+        case P_GROUP: k_particle_passes<F64><<<148, kBlock, 0, s>>>(dp, st, groups[ps.index]); break;
+        case P_REC_CAND:
+        case P_DETACH:
+        case P_CONV: break;  // fused into P_GROUP passes
         case P_MERGE: k_grid_merge<<<gm > 0 ? gm : 1, 256, 0, s>>>(grid_cnt, grid_delta, n_grid); break;
       }
     }
+    if (pass_prof) cudaEventRecord(pass_prof[passes.size()], s);
     k_step_inc<<<1, 1, 0, s>>>(d_step);
     cells_valid = true;
     mark(4, s);
@@ -416,6 +519,17 @@ int64_t edm_abi_sizeof(int which) {
 }
 
 const char* edm_last_error(void) { return g_last_error.c_str(); }
+
+// Upper bound of a rule's Hill factor over every grid count: the largest
+// exact table entry, and beyond the table the device expression, which is at
+// most 1 for inhibition and at most max(1, basal) for activation (1 without
+// K_half); the relative margin covers the expression's last-place rounding.
+static double rule_factor_bound(const EdmRule& R, const double* hill) {
+  double m = 1.0;
+  for (int64_t i = 0; i < R.table_len; ++i) m = std::max(m, hill[R.table_offset + i]);
+  if (R.K_half > 0 && !R.inhibition) m = std::max(m, R.basal);
+  return m * (1.0 + 1e-12);
+}
 
 int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScopeParams* scope, int32_t n_replicas,
                const double* hill, int64_t n_hill, int32_t precision, int32_t device, EdmEngine** out) {
@@ -513,6 +627,13 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
   CUDA_TRY(cudaMemcpy(E->dp, dyn, sizeof(EdmDynParams) * n_replicas, cudaMemcpyHostToDevice));
   ALLOC(E->hill, (size_t)n_hill);
   if (n_hill > 0) CUDA_TRY(cudaMemcpy(E->hill, hill, sizeof(double) * n_hill, cudaMemcpyHostToDevice));
+  {
+    std::vector<double> rmax((size_t)n_replicas * EDM_MAX_RULES, 1.0);
+    for (int r = 0; r < n_replicas; ++r)
+      for (int k = 0; k < dyn[r].n_rules; ++k) rmax[(size_t)r * EDM_MAX_RULES + k] = rule_factor_bound(dyn[r].rule[k], hill);
+    ALLOC(E->rule_max, rmax.size());
+    CUDA_TRY(cudaMemcpy(E->rule_max, rmax.data(), sizeof(double) * rmax.size(), cudaMemcpyHostToDevice));
+  }
   const size_t psz = E->f64 ? sizeof(double2) : sizeof(float2);
   uint8_t *pp0 = nullptr, *pp1 = nullptr;
   ALLOC(pp0, psz * np);
@@ -559,6 +680,11 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
   ALLOC(E->contact_count, EDM_MAX_CAT);
   ALLOC(E->moved, np);
   ALLOC(E->moved_count, (size_t)n_replicas);
+  ALLOC(E->pl, (size_t)np);
+  ALLOC(E->pl_count, 1);
+  ALLOC(E->pl_index, (size_t)np);
+  CUDA_TRY(cudaMemset(E->pl_index, 0xFF, sizeof(int32_t) * np));
+  CUDA_TRY(cudaMemset(E->pl_count, 0, sizeof(int32_t)));
   ALLOC(E->rep_first, (size_t)n_replicas + 1);
   {
     std::vector<int64_t> rf(pfirst);
@@ -975,6 +1101,40 @@ int edm_profile_steps(EdmEngine* E, int32_t n_steps, int32_t with_photons, float
   for (int k = 0; k < 7; ++k) cudaEventDestroy(ev[k]);
   for (int k = 0; k < EDM_NPROF; ++k) ms_out[k] = (float)(acc[k] / n_steps);
   return EDM_OK;
+}
+
+int edm_profile_passes(EdmEngine* E, int32_t n_steps, float* ms_out, int32_t* kinds_out, int32_t cap, void* stream) {
+  if (!E || n_steps <= 0 || !ms_out || !kinds_out) return fail(EDM_EINVAL, "edm_profile_passes: bad argument");
+  const int n = (int)E->passes.size();
+  if (cap < n) return fail(EDM_EINVAL, "edm_profile_passes: cap below the number of passes");
+  CUDA_TRY(cudaSetDevice(E->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<cudaEvent_t> ev(n + 1);
+  for (auto& e : ev) CUDA_TRY(cudaEventCreate(&e));
+  std::vector<double> acc(n, 0.0);
+  E->pass_prof = ev.data();
+  int rc = EDM_OK;
+  for (int i = 0; i < n_steps && rc == EDM_OK; ++i) {
+    E->enqueue_dynamics(s);
+    const cudaError_t e = cudaEventSynchronize(ev[n]);
+    if (e != cudaSuccess) {
+      rc = fail(EDM_ECUDA, cudaGetErrorString(e));
+      break;
+    }
+    for (int k = 0; k < n; ++k) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+      acc[k] += t;
+    }
+  }
+  E->pass_prof = nullptr;
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (rc != EDM_OK) return rc;
+  for (int k = 0; k < n; ++k) {
+    ms_out[k] = (float)(acc[k] / n_steps);
+    kinds_out[k] = 100 * (int)E->passes[k].kind + E->passes[k].index;
+  }
+  return n;
 }
 
 int edm_launches_per_step(EdmEngine* E, int32_t with_photons) {

@@ -22,11 +22,28 @@
 
 namespace {
 
-// One thread per pixel streams the pixel's row in 16-byte loads; the lanes
-// of a warp read 32 rows side by side, and the next load of each lane hits
-// the sector the previous one opened, so the stack is read from DRAM once.
-// Intensity and sum n_k k are exact integer sums (sum n_k t_k =
-// width * (sum n_k k + intensity / 2)); the phasor sums are float64.
+// Exact float64 value of an integer v < 2^52: the double whose bits are
+// 2^52 + v, minus 2^52 (one add instead of an integer-to-double conversion).
+__device__ __forceinline__ double u52_to_f64(uint64_t v) {
+  const double d = __hiloint2double(0x43300000 | (int)(uint32_t)(v >> 32), (int)(uint32_t)v);
+  return __dsub_rn(d, 4503599627370496.0);
+}
+
+// Bins k and K-1-k share |cos| and |sin| of their phases (phi_{K-1-k} =
+// 2 pi h - phi_k), so a pair adds (n_k + n_{K-1-k}) cos(phi_k) to G and
+// (n_k - n_{K-1-k}) sin(phi_k) to S: two float64 multiply-adds per pair.
+__device__ __forceinline__ void readout_pair(uint32_t na, uint32_t nb, int k, int kb, const double* c_k,
+                                             const double* s_k, uint64_t& I, uint64_t& KW, double& G, double& S) {
+  I += (uint64_t)na + nb;
+  KW += (uint64_t)na * (uint32_t)k + (uint64_t)nb * (uint32_t)kb;
+  G = fma(u52_to_f64((uint64_t)na + nb), c_k[k], G);
+  S = fma(__dsub_rn(u52_to_f64((uint64_t)na + 4294967296ull - nb), 4294967296.0), s_k[k], S);
+}
+
+// One thread per pixel streams the pixel's row in 16-byte loads from both
+// ends; the lanes of a warp read 32 rows side by side, so the stack is read
+// from DRAM once.  Intensity and sum n_k k are exact integer sums (sum n_k
+// t_k = width * (sum n_k k + intensity / 2)); the phasor sums are float64.
 __global__ void __launch_bounds__(256) k_readout(const uint32_t* __restrict__ stack, int64_t n_px, int n_bins,
                                                  double T_ns, int harmonic, int min_mean, int min_phasor,
                                                  double* __restrict__ out) {
@@ -45,18 +62,19 @@ __global__ void __launch_bounds__(256) k_readout(const uint32_t* __restrict__ st
     const uint4* row = reinterpret_cast<const uint4*>(stack + px * (int64_t)n_bins);
     uint64_t I = 0, KW = 0;
     double G = 0.0, S = 0.0;
-    for (int q = 0; q < nq; ++q) {
-      const uint4 v = __ldg(row + q);
-      const uint32_t n4[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int k = 4 * q + i;
-        I += n4[i];
-        KW += (uint64_t)n4[i] * (uint64_t)k;
-        const double n = (double)n4[i];
-        G += n * c_k[k];
-        S += n * s_k[k];
-      }
+    int q = 0;
+    for (; q < nq - 1 - q; ++q) {  // word q (bins 4q..4q+3) against word nq-1-q, reversed
+      const int qb = nq - 1 - q;
+      const uint4 a = __ldg(row + q), b = __ldg(row + qb);
+      readout_pair(a.x, b.w, 4 * q, 4 * qb + 3, c_k, s_k, I, KW, G, S);
+      readout_pair(a.y, b.z, 4 * q + 1, 4 * qb + 2, c_k, s_k, I, KW, G, S);
+      readout_pair(a.z, b.y, 4 * q + 2, 4 * qb + 1, c_k, s_k, I, KW, G, S);
+      readout_pair(a.w, b.x, 4 * q + 3, 4 * qb, c_k, s_k, I, KW, G, S);
+    }
+    if (q == nq - 1 - q) {  // odd word count: the middle word pairs within itself
+      const uint4 a = __ldg(row + q);
+      readout_pair(a.x, a.w, 4 * q, 4 * q + 3, c_k, s_k, I, KW, G, S);
+      readout_pair(a.y, a.z, 4 * q + 1, 4 * q + 2, c_k, s_k, I, KW, G, S);
     }
     const double In = (double)I;
     const double tau = In >= min_mean ? width * ((double)KW + 0.5 * In) / In : nan;

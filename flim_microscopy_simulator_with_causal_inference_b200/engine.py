@@ -70,6 +70,7 @@ def load_library():
     L.edm_get_status.argtypes = [vp, vp, vp]
     L.edm_get_cells.argtypes = [vp, i32, vp, vp, i64, i64, vp]
     L.edm_profile_steps.argtypes = [vp, i32, i32, vp, vp]
+    L.edm_profile_passes.argtypes = [vp, i32, vp, vp, i32, vp]
     L.edm_launches_per_step.argtypes = [vp, i32]
     L.edm_cell_list_static.argtypes = [vp, i64, C.c_double, C.c_double, i32, i32, vp, vp, vp]
     L.edm_readout_lifetimes.argtypes = [vp, i64, i32, C.c_double, i32, i32, i32, vp, vp]
@@ -218,6 +219,19 @@ class Engine:
         _check(self.L.edm_profile_steps(self.handle, int(n), int(bool(with_photons)), _ptr(out),
                                         _stream_handle(stream)), "edm_profile_steps")
         return dict(zip(self.PROFILE_GROUPS, out.astype(float).tolist()))
+
+    PASS_KINDS = ("bind_candidates", "bind_apply", "dissociation", "contacts", "catalytic", "recruit_candidates",
+                  "recruit_apply", "detach", "convert", "grid_merge", "particle_passes", "pass_draws")
+
+    def profile_passes(self, n: int, stream=None) -> list:
+        """Mean device ms per dynamics step of each reaction pass, in schedule
+        order: [(kind, index, ms)] (CUDA events, eager, dynamics only)."""
+        cap = 256
+        out = np.zeros(cap, dtype=np.float32)
+        kinds = np.zeros(cap, dtype=np.int32)
+        n_pass = _check(self.L.edm_profile_passes(self.handle, int(n), _ptr(out), _ptr(kinds), cap,
+                                                  _stream_handle(stream)), "edm_profile_passes")
+        return [(self.PASS_KINDS[kinds[k] // 100], int(kinds[k] % 100), float(out[k])) for k in range(n_pass)]
 
     def launches_per_step(self, with_photons: bool = True) -> int:
         return _check(self.L.edm_launches_per_step(self.handle, int(bool(with_photons))), "edm_launches_per_step")

@@ -330,6 +330,17 @@ int edm_get_status(EdmEngine* eng, uint32_t* status, void* stream);
 #define EDM_NPROF 7
 int edm_profile_steps(EdmEngine* eng, int32_t n_steps, int32_t with_photons,
                       float* ms_out, void* stream);
+/* Instrumented eager dynamics steps: runs n_steps dynamics steps with CUDA
+ * events between the reaction passes and writes, per pass of the step's
+ * schedule, its mean device time (ms) to ms_out[k] and its kind to
+ * kinds_out[k] = 100 * kind + index (kind 0 binding candidates, 1 binding
+ * apply, 2 dissociation, 3 catalytic contacts, 4 catalytic pass, 6
+ * recruitment apply, 9 grid merge, 10 run of recruitment-candidate,
+ * detachment and conversion passes over the listed particles, 11 the draw
+ * sweep that lists them).  Returns the number of passes (at most
+ * cap) or a negative error.  No reference counterpart. */
+int edm_profile_passes(EdmEngine* eng, int32_t n_steps, float* ms_out,
+                       int32_t* kinds_out, int32_t cap, void* stream);
 /* Kernels of this library launched per pipeline step. */
 int edm_launches_per_step(EdmEngine* eng, int32_t with_photons);
 
