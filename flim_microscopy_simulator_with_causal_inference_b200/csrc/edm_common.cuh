@@ -55,6 +55,16 @@ __device__ __forceinline__ double uniform1(uint64_t seed, int64_t step, int stre
   return uniform2(seed, step, stream, a, b).u0;
 }
 
+// The integer m of uniform1 = m 2^-53.  For a bound b, u < b holds exactly
+// when m < ceil(b 2^53), so a draw meets a precomputed threshold with one
+// integer compare.
+__device__ __forceinline__ uint64_t draw_u53(uint64_t seed, int64_t step, int stream, uint64_t a, uint64_t b) {
+  uint32_t c0 = (uint32_t)a, c1 = (uint32_t)b, c2 = (uint32_t)((uint64_t)step);
+  uint32_t c3 = ((uint32_t)stream << 16) | (uint32_t)(((uint64_t)step >> 32) & 0xFFFFu);
+  philox10(c0, c1, c2, c3, (uint32_t)seed, (uint32_t)(seed >> 32));
+  return (((uint64_t)c1 << 32) | c0) >> 11;
+}
+
 // ln q by the atanh series (Abramowitz & Stegun 4.1.27), q = m 2^e with
 // m in [sqrt(1/2), sqrt(2)), s = (m-1)/(m+1), 12 odd terms, Horner in s^2.
 __device__ __forceinline__ double ln_series(double q) {

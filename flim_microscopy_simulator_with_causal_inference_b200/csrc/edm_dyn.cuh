@@ -33,6 +33,7 @@ namespace edm {
 
 constexpr int kBlock = 256;
 constexpr int kSweepChunk = 128;  // slots per warp in the flag sweeps (4 per lane)
+constexpr int kMaxPP = 32;        // recruitment-candidate, detachment and conversion passes per step
 constexpr int kRecCap = 128;
 constexpr int kBindCap = 512;
 
@@ -53,7 +54,11 @@ struct DevState {
   int32_t* grid_cnt;     // density-grid counts (snapshot of the current pass)
   int32_t* grid_delta;   // pending changes of the current pass
   const double* hill;
-  const double* rule_max;  // [R][EDM_MAX_RULES] upper bound of each rule's Hill factor
+  // draw thresholds: a keyed draw u = m 2^-53 with m >= the threshold is
+  // rejected by its pass whatever the grid counts (threshold = ceil(b 2^53),
+  // b = prob times the largest Hill factor of each rule of the pass)
+  const uint64_t* pass_thr;  // [R][kMaxPP] per-particle passes, in schedule order
+  const uint64_t* cat_thr;   // [R][EDM_MAX_CAT] catalytic passes
   int64_t* counters;     // [R][EDM_NCOUNTERS]
   uint32_t* status;
   const int64_t* d_step;
@@ -75,8 +80,8 @@ struct DevState {
   int32_t* moved;
   int32_t* moved_count;  // [R]
   // particles whose keyed draws pass some per-particle pass's bound this step:
-  // (slot, bit mask of those passes); pl_index[slot] = its entry
-  int2* pl;
+  // (slot, bit mask of those passes, replica, local id); pl_index[slot] = its entry
+  int4* pl;
   int32_t* pl_count;
   int32_t* pl_index;
   int n_rep;
@@ -333,16 +338,6 @@ __device__ __forceinline__ double rule_factor(const EdmDynParams& p, int rule, c
   const EdmRule& R = p.rule[rule];
   const int k = st.grid_cnt[grid_cell_of(p.grid[R.grid], x, y)];
   return hill_of(R, st.hill, k, st.status);
-}
-
-// An upper bound of prob * rule_factor(rule) [* rule_factor(rule2)] for the
-// replica (rule -1: no factor).  Rounded products are monotone in their
-// factors, so a keyed draw u with u >= the bound is rejected whatever the
-// grid counts; the passes test it before they fetch positions and counts.
-__device__ __forceinline__ double prob_bound(const DevState& st, int r, double prob, int rule, int rule2 = -1) {
-  if (rule >= 0) prob = prob * st.rule_max[(int64_t)r * EDM_MAX_RULES + rule];
-  if (rule2 >= 0) prob = prob * st.rule_max[(int64_t)r * EDM_MAX_RULES + rule2];
-  return prob;
 }
 
 // Grid bookkeeping of a particle changing (species, alive) at one position.
@@ -816,7 +811,7 @@ struct CatLists {
 };
 
 template <bool F64>
-__global__ void __launch_bounds__(kBlock) k_contacts(const EdmDynParams* __restrict__ P, DevState st, Match m,
+__global__ void __launch_bounds__(kBlock, 6) k_contacts(const EdmDynParams* __restrict__ P, DevState st, Match m,
                                                      CatLists L) {
   __shared__ int2 buf[kContactSmem];
   __shared__ int nbuf[EDM_MAX_CAT], base[EDM_MAX_CAT];
@@ -904,8 +899,9 @@ __global__ void __launch_bounds__(kBlock, 8) k_catalytic(const EdmDynParams* __r
     const Geo g(p);
     const int ide = st.ids[es.x] - (int)g.poff, ids = st.ids[es.y] - (int)g.poff;
     const uint32_t lo = ide < ids ? ide : ids, hi = ide < ids ? ids : ide;
-    const double u = uniform1(p.seed, *st.d_step, EDM_S_CAT + cidx, lo, hi);
-    if (!(u < prob_bound(st, r, C.prob, C.rule))) continue;
+    const uint64_t m = draw_u53(p.seed, *st.d_step, EDM_S_CAT + cidx, lo, hi);
+    if (m >= st.cat_thr[(int64_t)r * EDM_MAX_CAT + cidx]) continue;
+    const double u = __dmul_rn(__ull2double_rn(m), 0x1p-53);
     double xs, ys;
     abs_pos<F64>(st.pos_post, st.cell_post, es.y, g, xs, ys);
     double peff = C.prob;
@@ -921,39 +917,40 @@ __global__ void __launch_bounds__(kBlock, 8) k_catalytic(const EdmDynParams* __r
 
 // ---- per-particle passes: recruitment candidates, detachments, conversions ----
 // Each decides for one particle from its flags, its keyed draw u, and (only
-// when u is below the pass's probability bound, prob_bound) its position and
-// the grid counts.  A step draws every particle's u once, for every such pass
-// the particle can still reach, in one sweep placed before the first of them
-// (k_pass_draws); the few particles with some u below its bound go to a list,
-// and the passes visit only that list.  A particle that is not listed for a
-// pass would be rejected by it, so skipping it changes nothing.
-constexpr int kMaxPP = 32;
+// when u is below the pass's threshold, pass_thr) its position and the grid
+// counts.  One sweep before the first of these passes (k_pass_draws) draws,
+// for every particle, the passes whose match holds its state; the few
+// particles with some draw below its threshold go to a list, and the passes
+// visit only that list.  A pass that changes a listed particle's state
+// (detachment, conversion, recruitment) draws at once the later passes that
+// match the new state.  A particle left off the list for a pass would be
+// rejected by it, so skipping it changes nothing.
 enum GroupPass : int8_t { kGroupRecruit = 0, kGroupDetach = 1, kGroupConvert = 2 };
 struct DrawPlan {
-  Match any;                             // states that reach some pass
-  uint32_t reach[2][EDM_MAX_SPECIES];    // passes reachable from (alive, species)
-  int8_t kind[kMaxPP];                   // GroupPass of each per-particle pass
-  int8_t index[kMaxPP];                  // its exchange or conversion
+  Match any;                           // states that some pass matches
+  uint32_t reach[2][EDM_MAX_SPECIES];  // passes matching (alive, species), from the sweep on
+  uint32_t after[kMaxPP];              // passes after pass k matching the state pass k leaves
+  int8_t kind[kMaxPP];                 // GroupPass of each per-particle pass
+  int8_t index[kMaxPP];                // its exchange or conversion
   int n;
 };
 
-// Whether the keyed draw of per-particle pass (kind, idx) for local id `id`
-// lies below the pass's probability bound (otherwise the pass rejects).
-__device__ __forceinline__ bool pass_may_accept(const EdmDynParams& p, const DevState& st, int r, int id, int kind,
-                                                int idx, int64_t step) {
-  if (kind == kGroupRecruit) {
-    const EdmExch& X = p.exch[idx];
-    const double u = uniform1(p.seed, step, EDM_S_EX_ACCEPT + 4 * idx, (uint64_t)id, 0);
-    return u < prob_bound(st, r, X.prob_on, X.rule_on, X.rule_on >= 0 ? X.rule_on2 : -1);
+__device__ __forceinline__ int pass_stream(int kind, int idx) {
+  return kind == kGroupRecruit ? EDM_S_EX_ACCEPT + 4 * idx
+                               : (kind == kGroupDetach ? EDM_S_EX_DETACH + 4 * idx : EDM_S_CONV + idx);
+}
+
+// Bits of the passes in `todo` whose keyed draw for local id `id` lies below
+// the pass's threshold (the others reject the particle).
+__device__ __forceinline__ uint32_t draw_passes(const DevState& st, const DrawPlan& D, uint64_t seed, int r, int id,
+                                                int64_t step, uint32_t todo) {
+  uint32_t bits = 0;
+  for (; todo; todo &= todo - 1) {
+    const int k = __ffs(todo) - 1;
+    const uint64_t m = draw_u53(seed, step, pass_stream(D.kind[k], D.index[k]), (uint64_t)id, 0);
+    if (m < st.pass_thr[(int64_t)r * kMaxPP + k]) bits |= 1u << k;
   }
-  if (kind == kGroupDetach) {
-    const EdmExch& X = p.exch[idx];
-    const double u = uniform1(p.seed, step, EDM_S_EX_DETACH + 4 * idx, (uint64_t)id, 0);
-    return u < prob_bound(st, r, X.prob_off, X.rule_off);
-  }
-  const EdmConv& V = p.conv[idx];
-  const double u = uniform1(p.seed, step, EDM_S_CONV + idx, (uint64_t)id, 0);
-  return u < prob_bound(st, r, V.prob, V.rule);
+  return bits;
 }
 
 __global__ void __launch_bounds__(kBlock, 8) k_pass_draws(const EdmDynParams* __restrict__ P, DevState st,
@@ -962,20 +959,14 @@ __global__ void __launch_bounds__(kBlock, 8) k_pass_draws(const EdmDynParams* __
   if (threadIdx.x == 0) sd = D;
   __syncthreads();
   sweep4(st, sd.any, [&](int r, int64_t s) {
-    const EdmDynParams& p = P[r];
     const uint8_t f = st.flags[s];
     const int sp = fl_species(f);
-    uint32_t todo = sp < EDM_MAX_SPECIES ? sd.reach[fl_alive(f) ? 1 : 0][sp] : 0u;
-    const int id = st.ids[s] - (int)p.particle_offset;
-    const int64_t step = *st.d_step;
-    uint32_t bits = 0;
-    for (; todo; todo &= todo - 1) {
-      const int k = __ffs(todo) - 1;
-      if (pass_may_accept(p, st, r, id, sd.kind[k], sd.index[k], step)) bits |= 1u << k;
-    }
+    const uint32_t todo = sp < EDM_MAX_SPECIES ? sd.reach[fl_alive(f) ? 1 : 0][sp] : 0u;
+    const int id = st.ids[s] - (int)P[r].particle_offset;
+    const uint32_t bits = draw_passes(st, sd, P[r].seed, r, id, *st.d_step, todo);
     if (bits) {
       const int q = atomicAdd(st.pl_count, 1);
-      st.pl[q] = make_int2((int)s, (int)bits);
+      st.pl[q] = make_int4((int)s, (int)bits, r, id);
       st.pl_index[s] = q;
     }
   });
@@ -983,12 +974,11 @@ __global__ void __launch_bounds__(kBlock, 8) k_pass_draws(const EdmDynParams* __
 
 // Apply the first max_recruits accepted candidates in particle order.
 // A recruited particle is alive from here on, so the passes after this one
-// that it can reach (`after`) get its draws now, in its list entry (the
-// entry exists: the particle was listed for this exchange's candidates);
-// `keep` holds the bits of the passes before.
+// that match it (`after`) get its draws now, in its list entry (the entry
+// exists: the particle was listed for this exchange's candidates).
 template <bool F64>
 __global__ void k_recruit_apply(const EdmDynParams* __restrict__ P, int n_rep, DevState st, int e, DrawPlan D,
-                                uint32_t after, uint32_t keep) {
+                                uint32_t after) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n_rep) return;
   const EdmDynParams& p = P[r];
@@ -1031,15 +1021,10 @@ __global__ void k_recruit_apply(const EdmDynParams* __restrict__ P, int n_rep, D
     note_moved(st, r, p, slot);
     grid_add(p, st.grid_delta, X.species, x, y, 1);
     if (after) {
-      const int64_t step = *st.d_step;
-      uint32_t bits = 0;
-      for (uint32_t todo = after; todo; todo &= todo - 1) {
-        const int k = __ffs(todo) - 1;
-        if (pass_may_accept(p, st, r, ids[a], D.kind[k], D.index[k], step)) bits |= 1u << k;
-      }
+      const uint32_t bits = draw_passes(st, D, p.seed, r, ids[a], *st.d_step, after);
       const int q = st.pl_index[slot];
-      if (q >= 0 && q < *st.pl_count && st.pl[q].x == (int)slot) st.pl[q].y = (int)(((uint32_t)st.pl[q].y & keep) | bits);
-      else set_status(st.status, EDM_STATUS_RECRUIT_CAP);
+      if (q >= 0 && q < *st.pl_count && st.pl[q].x == (int)slot) st.pl[q].y |= (int)bits;
+      else set_status(st.status, EDM_STATUS_RECRUIT_CAP);  // cannot happen: see above
     }
   }
   atomic_add_i64(&st.counters[(int64_t)r * EDM_NCOUNTERS + EDM_C_RECRUITED], take);
@@ -1047,11 +1032,11 @@ __global__ void k_recruit_apply(const EdmDynParams* __restrict__ P, int n_rep, D
 
 // Recruitment candidate of exchange e (dynamics.py:1229-1458): a dormant
 // particle of the species whose keyed draw accepts at the keyed position.
+// The per-particle passes below run on listed particles only.
 __device__ __forceinline__ void recruit_candidate(const EdmDynParams& p, const DevState& st, int r, int id, int e) {
   const EdmExch& X = p.exch[e];
   const int64_t step = *st.d_step;
   const double ua = uniform1(p.seed, step, EDM_S_EX_ACCEPT + 4 * e, (uint64_t)id, 0);
-  if (!(ua < prob_bound(st, r, X.prob_on, X.rule_on, X.rule_on >= 0 ? X.rule_on2 : -1))) return;
   const U2 up = uniform2(p.seed, step, EDM_S_EX_POS + 4 * e, (uint64_t)id, 0);
   const double cx = up.u0 * p.Lx, cy = up.u1 * p.Ly;
   double peff = X.prob_on;
@@ -1090,7 +1075,6 @@ __device__ __forceinline__ uint8_t detach_one(const EdmDynParams& p, const Geo& 
                                               int64_t s, int id, LazyPos<F64>& pos, int e, uint8_t f) {
   const EdmExch& X = p.exch[e];
   const double u = uniform1(p.seed, *st.d_step, EDM_S_EX_DETACH + 4 * e, (uint64_t)id, 0);
-  if (!(u < prob_bound(st, r, X.prob_off, X.rule_off))) return f;
   pos.get(st, s, g);
   double peff = X.prob_off;
   if (X.rule_off >= 0) peff = X.prob_off * rule_factor(p, X.rule_off, st, pos.x, pos.y);
@@ -1111,7 +1095,6 @@ __device__ __forceinline__ uint8_t convert_one(const EdmDynParams& p, const Geo&
                                                int64_t s, int id, LazyPos<F64>& pos, int v, uint8_t f) {
   const EdmConv& V = p.conv[v];
   const double u = uniform1(p.seed, *st.d_step, EDM_S_CONV + v, (uint64_t)id, 0);
-  if (!(u < prob_bound(st, r, V.prob, V.rule))) return f;
   pos.get(st, s, g);
   double peff = V.prob;
   if (V.rule >= 0) peff = V.prob * rule_factor(p, V.rule, st, pos.x, pos.y);
@@ -1142,30 +1125,40 @@ struct PassGroup {
 
 template <bool F64>
 __global__ void __launch_bounds__(kBlock) k_particle_passes(const EdmDynParams* __restrict__ P, DevState st,
-                                                            PassGroup G) {
+                                                            PassGroup G, DrawPlan D) {
   __shared__ PassGroup sg;
-  if (threadIdx.x == 0) sg = G;
+  __shared__ DrawPlan sd;
+  if (threadIdx.x == 0) {
+    sg = G;
+    sd = D;
+  }
   __syncthreads();
   const int n = *st.pl_count;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-    const int2 e = st.pl[q];
-    const uint32_t bits = (uint32_t)e.y;
+    const int4 e = st.pl[q];
+    uint32_t bits = (uint32_t)e.y;
     if (!(bits & sg.bits)) continue;
     const int64_t s = e.x;
-    int r = st.chunk_rep[s / kSweepChunk];
-    while (r + 1 < st.n_rep && st.rep_first[r + 1] <= s) ++r;
+    const int r = e.z, id = e.w;
     const EdmDynParams& p = P[r];
     const Geo g(p);
-    const int id = st.ids[s] - (int)g.poff;
     uint8_t f = st.flags[s];
+    const uint32_t bits0 = bits;
     LazyPos<F64> pos;  // these passes move no particle
     for (int k = 0; k < sg.n; ++k) {
-      if (!((bits >> sg.pp[k]) & 1u) || !matches(f, sg.m[k])) continue;
+      const int pk = sg.pp[k];
+      if (!((bits >> pk) & 1u) || !matches(f, sg.m[k])) continue;
       const int kind = sg.kind[k], idx = sg.index[k];
-      if (kind == kGroupRecruit) recruit_candidate(p, st, r, id, idx);
-      else if (kind == kGroupDetach) f = detach_one<F64>(p, g, st, r, s, id, pos, idx, f);
-      else f = convert_one<F64>(p, g, st, r, s, id, pos, idx, f);
+      if (kind == kGroupRecruit) {
+        recruit_candidate(p, st, r, id, idx);
+        continue;
+      }
+      const uint8_t f0 = f;
+      f = kind == kGroupDetach ? detach_one<F64>(p, g, st, r, s, id, pos, idx, f)
+                               : convert_one<F64>(p, g, st, r, s, id, pos, idx, f);
+      if (f != f0) bits |= draw_passes(st, sd, p.seed, r, id, *st.d_step, sd.after[pk] & ~bits);
     }
+    if (bits != bits0) st.pl[q].y = (int)bits;
   }
 }
 

@@ -78,7 +78,8 @@ struct EdmEngine {
   EdmPhotParams* pp = nullptr;
   EdmScopeParams* sp = nullptr;
   double* hill = nullptr;
-  double* rule_max = nullptr;  // [R][EDM_MAX_RULES]
+  std::vector<double> rule_max;  // [R][EDM_MAX_RULES] upper bound of each rule's Hill factor (host)
+  uint64_t *pass_thr = nullptr, *cat_thr = nullptr;  // draw thresholds ([R][kMaxPP], [R][EDM_MAX_CAT])
   int2 *pblk = nullptr, *eblk = nullptr, *phblk = nullptr, *pxblk = nullptr;
   int npblk = 0, neblk = 0, nphblk = 0, npxblk = 0;
   void* pos_pre = nullptr;
@@ -116,7 +117,7 @@ struct EdmEngine {
   std::vector<Pass> passes;
   std::vector<PassGroup> groups;  // runs of per-particle passes (P_GROUP index)
   DrawPlan draw{};                // the draw sweep of the per-particle passes
-  uint32_t rec_after[EDM_MAX_EXCH] = {}, rec_keep[EDM_MAX_EXCH] = {};  // per recruitment apply
+  uint32_t rec_after[EDM_MAX_EXCH] = {};  // per recruitment apply: later passes matching a recruit
   int2* contacts = nullptr;
   int32_t* contact_count = nullptr;
   int64_t contact_cap = 0;
@@ -125,7 +126,7 @@ struct EdmEngine {
   int64_t* rep_first = nullptr;
   int32_t* chunk_rep = nullptr;  // replica of the first slot of each 128-slot chunk
   int32_t *moved = nullptr, *moved_count = nullptr;
-  int2* pl = nullptr;  // listed particles of the per-particle passes: (slot, pass bits)
+  int4* pl = nullptr;  // listed particles of the per-particle passes: (slot, pass bits, replica, id)
   int32_t *pl_count = nullptr, *pl_index = nullptr;
   std::vector<int32_t> emit_host;  // emitter list last uploaded
   std::vector<uint8_t> has_dye_host;  // has_dye of the last edm_set_state
@@ -151,7 +152,8 @@ struct EdmEngine {
     s.grid_cnt = grid_cnt;
     s.grid_delta = grid_delta;
     s.hill = hill;
-    s.rule_max = rule_max;
+    s.pass_thr = pass_thr;
+    s.cat_thr = cat_thr;
     s.counters = counters;
     s.status = status;
     s.d_step = d_step;
@@ -328,39 +330,33 @@ struct EdmEngine {
       draw.index[pp_of[i]] = (int8_t)passes[i].index;
     }
     auto state = [](int sp, int alive) { return 1u << (alive * EDM_MAX_SPECIES + sp); };
-    // per-particle passes from position `from` on that a particle in one of the states R can reach
-    auto reach_from = [&](size_t from, uint32_t R) {
+    // per-particle passes from position `from` on whose match holds a state of R
+    auto matching_from = [&](size_t from, uint32_t R) {
       uint32_t mask = 0;
       for (size_t i = from; i < passes.size(); ++i) {
         if (pp_of[i] < 0) continue;
         const Pass& ps = passes[i];
         const uint32_t M = (ps.match.mask[1] << EDM_MAX_SPECIES) | (ps.match.mask[0] & ((1u << EDM_MAX_SPECIES) - 1));
-        if (!(R & M)) continue;
-        mask |= 1u << pp_of[i];
-        if (ps.kind == P_DETACH) {
-          const int x = p.exch[ps.index].species;
-          if (R & state(x, 1)) R |= state(x, 0);
-        } else if (ps.kind == P_CONV) {
-          const EdmConv& V = p.conv[ps.index];
-          if (R & state(V.from, 1)) R |= state(V.to, 1);
-        }
+        if (R & M) mask |= 1u << pp_of[i];
       }
       return mask;
     };
     for (int alive = 0; alive < 2; ++alive)
       for (int sp = 0; sp < p.n_species; ++sp) {
-        draw.reach[alive][sp] = reach_from(first, state(sp, alive));
+        draw.reach[alive][sp] = matching_from(first, state(sp, alive));
         if (draw.reach[alive][sp]) draw.any.mask[alive] |= 1u << sp;
       }
+    for (size_t i = 0; i < passes.size(); ++i) {  // the state a detachment / conversion leaves
+      if (passes[i].kind == P_DETACH) draw.after[pp_of[i]] = matching_from(i + 1, state(p.exch[passes[i].index].species, 0));
+      if (passes[i].kind == P_CONV) draw.after[pp_of[i]] = matching_from(i + 1, state(p.conv[passes[i].index].to, 1));
+    }
     std::vector<Pass> fused;
-    int pp_before = 0;
     for (size_t i = 0; i < passes.size();) {
       if (i == first) fused.push_back({P_DRAWS, 0, draw.any});
       if (!per_particle(passes[i].kind)) {
         if (passes[i].kind == P_REC_APPLY) {
           const int e = passes[i].index;
-          rec_after[e] = reach_from(i + 1, state(p.exch[e].species, 1));
-          rec_keep[e] = pp_before >= 32 ? ~0u : (1u << pp_before) - 1u;
+          rec_after[e] = matching_from(i + 1, state(p.exch[e].species, 1));
         }
         fused.push_back(passes[i++]);
         continue;
@@ -374,13 +370,55 @@ struct EdmEngine {
         G.m[G.n] = passes[i].match;
         G.bits |= 1u << k;
         ++G.n;
-        ++pp_before;
         ++i;
       }
       groups.push_back(G);
       fused.push_back({P_GROUP, (int)groups.size() - 1, Match{}});
     }
     passes.swap(fused);
+    return EDM_OK;
+  }
+
+  // Draw thresholds, per replica: ceil(b 2^53) for the bound b = prob times
+  // the largest Hill factor of each of the pass's rules, multiplied in the
+  // order the pass multiplies its factors, so that b >= the pass's
+  // probability for any grid count.
+  int upload_thresholds() {
+    auto thr_of = [](double b) -> uint64_t {
+      if (!(b > 0.0)) return 0;
+      const double B = std::ceil(std::ldexp(b, 53));
+      return B >= 9007199254740992.0 ? (1ull << 53) : (uint64_t)B;
+    };
+    std::vector<uint64_t> pt((size_t)R * kMaxPP, 0), ct((size_t)R * EDM_MAX_CAT, 0);
+    for (int r = 0; r < R; ++r) {
+      const EdmDynParams& q = hdp[r];
+      const double* rm = &rule_max[(size_t)r * EDM_MAX_RULES];
+      for (int k = 0; k < draw.n; ++k) {
+        const int idx = draw.index[k];
+        double b;
+        if (draw.kind[k] == kGroupRecruit) {
+          const EdmExch& X = q.exch[idx];
+          b = X.prob_on;
+          if (X.rule_on >= 0) {
+            b = b * rm[X.rule_on];
+            if (X.rule_on2 >= 0) b = b * rm[X.rule_on2];
+          }
+        } else if (draw.kind[k] == kGroupDetach) {
+          const EdmExch& X = q.exch[idx];
+          b = X.rule_off >= 0 ? X.prob_off * rm[X.rule_off] : X.prob_off;
+        } else {
+          const EdmConv& V = q.conv[idx];
+          b = V.rule >= 0 ? V.prob * rm[V.rule] : V.prob;
+        }
+        pt[(size_t)r * kMaxPP + k] = thr_of(b);
+      }
+      for (int c = 0; c < q.n_cat; ++c) {
+        const EdmCat& C = q.cat[c];
+        ct[(size_t)r * EDM_MAX_CAT + c] = thr_of(C.rule >= 0 ? C.prob * rm[C.rule] : C.prob);
+      }
+    }
+    CUDA_TRY(cudaMemcpy(pass_thr, pt.data(), sizeof(uint64_t) * pt.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(cat_thr, ct.data(), sizeof(uint64_t) * ct.size(), cudaMemcpyHostToDevice));
     return EDM_OK;
   }
 
@@ -427,13 +465,13 @@ struct EdmEngine {
           break;
         case P_CAT: k_catalytic<F64><<<cgrid, kBlock, 0, s>>>(dp, st, ps.index); break;
         case P_REC_APPLY:
-          k_recruit_apply<F64><<<rb, 128, 0, s>>>(dp, R, st, ps.index, draw, rec_after[ps.index], rec_keep[ps.index]);
+          k_recruit_apply<F64><<<rb, 128, 0, s>>>(dp, R, st, ps.index, draw, rec_after[ps.index]);
           break;
         case P_DRAWS:
           cudaMemsetAsync(pl_count, 0, sizeof(int32_t), s);
           k_pass_draws<<<sgrid, kBlock, 0, s>>>(dp, st, draw);
           break;
-        case P_GROUP: k_particle_passes<F64><<<148, kBlock, 0, s>>>(dp, st, groups[ps.index]); break;
+        case P_GROUP: k_particle_passes<F64><<<148, kBlock, 0, s>>>(dp, st, groups[ps.index], draw); break;
         case P_REC_CAND:
         case P_DETACH:
         case P_CONV: break;  // fused into P_GROUP passes
@@ -627,13 +665,11 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
   CUDA_TRY(cudaMemcpy(E->dp, dyn, sizeof(EdmDynParams) * n_replicas, cudaMemcpyHostToDevice));
   ALLOC(E->hill, (size_t)n_hill);
   if (n_hill > 0) CUDA_TRY(cudaMemcpy(E->hill, hill, sizeof(double) * n_hill, cudaMemcpyHostToDevice));
-  {
-    std::vector<double> rmax((size_t)n_replicas * EDM_MAX_RULES, 1.0);
-    for (int r = 0; r < n_replicas; ++r)
-      for (int k = 0; k < dyn[r].n_rules; ++k) rmax[(size_t)r * EDM_MAX_RULES + k] = rule_factor_bound(dyn[r].rule[k], hill);
-    ALLOC(E->rule_max, rmax.size());
-    CUDA_TRY(cudaMemcpy(E->rule_max, rmax.data(), sizeof(double) * rmax.size(), cudaMemcpyHostToDevice));
-  }
+  E->rule_max.assign((size_t)n_replicas * EDM_MAX_RULES, 1.0);
+  for (int r = 0; r < n_replicas; ++r)
+    for (int k = 0; k < dyn[r].n_rules; ++k) E->rule_max[(size_t)r * EDM_MAX_RULES + k] = rule_factor_bound(dyn[r].rule[k], hill);
+  ALLOC(E->pass_thr, (size_t)n_replicas * kMaxPP);
+  ALLOC(E->cat_thr, (size_t)n_replicas * EDM_MAX_CAT);
   const size_t psz = E->f64 ? sizeof(double2) : sizeof(float2);
   uint8_t *pp0 = nullptr, *pp1 = nullptr;
   ALLOC(pp0, psz * np);
@@ -671,7 +707,7 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
   ALLOC(E->bind_count, n_replicas);
   ALLOC(E->bind_key, (size_t)n_replicas * kBindCap);
   ALLOC(E->bind_ab, (size_t)n_replicas * kBindCap * 2);
-  if ((rc = E->build_schedule()) != EDM_OK) {
+  if ((rc = E->build_schedule()) != EDM_OK || (rc = E->upload_thresholds()) != EDM_OK) {
     delete E;
     return rc;
   }

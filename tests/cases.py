@@ -77,12 +77,27 @@ def proximity_small(seed: int = 13) -> dict:
     return d
 
 
+def exchange_heavy(seed: int = 17) -> dict:
+    """rich_small with recruitment, detachment and conversion probabilities
+    of 0.01-0.9 per step, so that a particle is recruited and detached, or
+    converted twice (PTEN_T1 -> PTEN_T2 -> PTEN_T1), within one step."""
+    d = rich_small(seed=seed)
+    for ex in d["compartment_exchanges"]:
+        ex["k_on"] *= 5.0
+        ex["k_off"] *= 1000.0
+        ex["max_recruits_per_step"] = 8
+    for cv in d["unimolecular_conversions"]:
+        cv["rate"] *= 400.0
+    return d
+
+
 CASES = {
     "rich_small": rich_small,
     "binding_regions": binding_regions,
     "harmonic_small": harmonic_small,
     "sine_small": sine_small,
     "proximity_small": proximity_small,
+    "exchange_heavy": exchange_heavy,
 }
 
 

@@ -3,7 +3,7 @@
 Run in a container that has the reference source tree (EDM_REFERENCE_ROOT,
 default /root/reference):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [name ...]   (default: every system)
 
 For every test system of tests/cases.py the reference's own DynamicsEngine,
 PhotonSimulator and VirtualMicroscope run K BD steps with the keyed draws
@@ -93,7 +93,7 @@ def generate(name: str) -> dict:
 def main():
     warnings.filterwarnings("ignore")
     here = Path(__file__).resolve().parent
-    for name in cases.CASES:
+    for name in sys.argv[1:] or list(cases.CASES):
         data = generate(name)
         np.savez_compressed(here / f"{name}.npz", **data)
         print(name, "counters", data["counters"].tolist(), "flim counts", int(data["flim"].sum()))
