@@ -51,7 +51,7 @@ STEPS_PER_FRAME = 100
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5, help="timed frames (100 BD steps each)")
+    ap.add_argument("--steps", type=int, default=10, help="timed frames (100 BD steps each)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--replicas", type=int, default=512)
