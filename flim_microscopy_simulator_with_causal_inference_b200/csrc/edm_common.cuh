@@ -95,55 +95,70 @@ __device__ __forceinline__ double ln_series(double q) {
                    __dadd_rn(__dmul_rn(de, 0x1.a39ef35793c76p-33), lnm));
 }
 
-// Standard normal pair, Marsaglia polar method; attempt t uses counter b = t.
-// The rejection loop only draws candidates; the logarithm and square root run
-// once after it, so lanes of a warp that accept at different attempts do not
-// each run them.
+// sin and cos of 2 pi u, u in [0, 1): 4u = k + f with f reduced to
+// [-1/2, 1/2) (both exact), x = f pi/2 in [-pi/4, pi/4), Taylor series of sin
+// to x^17 and cos to x^18 (truncation below 3e-19) in Horner form with a
+// fixed operation order, then the quadrant k: the host oracle evaluates the
+// same sequence, so both give identical bits.
+__device__ __forceinline__ void sincos_2pi(double u, double& c, double& s) {
+  constexpr double kS[9] = {0x1.0000000000000p+0,  -0x1.5555555555555p-3, 0x1.1111111111111p-7,
+                            -0x1.a01a01a01a01ap-13, 0x1.71de3a556c734p-19, -0x1.ae64567f544e4p-26,
+                            0x1.6124613a86d09p-33,  -0x1.ae7f3e733b81fp-41, 0x1.952c77030ad4ap-49};
+  constexpr double kC[10] = {0x1.0000000000000p+0,  -0x1.0000000000000p-1, 0x1.5555555555555p-5,
+                             -0x1.6c16c16c16c17p-10, 0x1.a01a01a01a01ap-16, -0x1.27e4fb7789f5cp-22,
+                             0x1.1eed8eff8d898p-29,  -0x1.93974a8c07c9dp-37, 0x1.ae7f3e733b81fp-45,
+                             -0x1.6827863b97d97p-53};
+  const double v = __dmul_rn(u, 4.0);
+  int k = (int)v;
+  double f = __dadd_rn(v, -(double)k);
+  if (f >= 0.5) {
+    f = __dadd_rn(f, -1.0);
+    k += 1;
+  }
+  const double x = __dmul_rn(f, 0x1.921fb54442d18p+0);
+  const double x2 = __dmul_rn(x, x);
+  double ps = kS[8];
+#pragma unroll
+  for (int i = 7; i >= 0; --i) ps = __dadd_rn(__dmul_rn(ps, x2), kS[i]);
+  double pc = kC[9];
+#pragma unroll
+  for (int i = 8; i >= 0; --i) pc = __dadd_rn(__dmul_rn(pc, x2), kC[i]);
+  const double sn = __dmul_rn(x, ps);
+  switch (k & 3) {
+    case 0: c = pc; s = sn; break;
+    case 1: c = -sn; s = pc; break;
+    case 2: c = -pc; s = -sn; break;
+    default: c = sn; s = -pc; break;
+  }
+}
+
+// Standard normal pair by the Box-Muller transform (Box & Muller 1958) of the
+// key's uniform pair (counter b = 0): r = sqrt(-2 ln(1 - u0)),
+// (z0, z1) = r (cos 2 pi u1, sin 2 pi u1); one Philox draw, no rejection.
 __device__ __forceinline__ U2 normal2(uint64_t seed, int64_t step, int stream, uint64_t a) {
-  double x = 0.0, y = 0.0, q = 0.0;
-  uint32_t t = 0;
-  for (; t < 64; ++t) {
-    const U2 u = uniform2(seed, step, stream, a, t);
-    x = __dadd_rn(__dmul_rn(2.0, u.u0), -1.0);
-    y = __dadd_rn(__dmul_rn(2.0, u.u1), -1.0);
-    q = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
-    if (q > 0.0 && q < 1.0) break;
-  }
+  const U2 u = uniform2(seed, step, stream, a, 0);
+  const double r = __dsqrt_rn(__dmul_rn(-2.0, ln_series(__dadd_rn(1.0, -u.u0))));
+  double c, s;
+  sincos_2pi(u.u1, c, s);
   U2 z;
-  if (t == 64) {
-    z.u0 = 0.0;
-    z.u1 = 0.0;
-    return z;
-  }
-  const double f = __dsqrt_rn(__ddiv_rn(__dmul_rn(-2.0, ln_series(q)), q));
-  z.u0 = __dmul_rn(x, f);
-  z.u1 = __dmul_rn(y, f);
+  z.u0 = __dmul_rn(r, c);
+  z.u1 = __dmul_rn(r, s);
   return z;
 }
 
-// The same normal pair in float32 for the float32 engine: the candidate
-// draws and the acceptance test are those of normal2 (float64), so both
-// accept the same candidate; only sqrt(-2 ln q / q) is evaluated in float32
-// (relative error ~1e-6, far below the float32 path's position tolerance).
+// The same normal pair in float32 for the float32 engine: the same uniforms,
+// the transform in float32 (relative error ~1e-6, far below the float32
+// path's position tolerance); ln(1 - u0) as log1pf(-u0) below 1/2, where the
+// float32 difference would lose u0.
 __device__ __forceinline__ void normal2_f32(uint64_t seed, int64_t step, int stream, uint64_t a, float& z0,
                                             float& z1) {
-  double x = 0.0, y = 0.0, q = 0.0;
-  uint32_t t = 0;
-  for (; t < 64; ++t) {
-    const U2 u = uniform2(seed, step, stream, a, t);
-    x = __dadd_rn(__dmul_rn(2.0, u.u0), -1.0);
-    y = __dadd_rn(__dmul_rn(2.0, u.u1), -1.0);
-    q = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
-    if (q > 0.0 && q < 1.0) break;
-  }
-  if (t == 64) {
-    z0 = z1 = 0.0f;
-    return;
-  }
-  const float qf = (float)q;
-  const float f = sqrtf(-2.0f * logf(qf) / qf);
-  z0 = (float)x * f;
-  z1 = (float)y * f;
+  const U2 u = uniform2(seed, step, stream, a, 0);
+  const float w = u.u0 > 0.5 ? logf((float)(1.0 - u.u0)) : log1pf(-(float)u.u0);
+  const float r = sqrtf(-2.0f * w);
+  float sf, cf;
+  sincospif(2.0f * (float)u.u1, &sf, &cf);
+  z0 = r * cf;
+  z1 = r * sf;
 }
 
 // ---- particle flags: bits 0-6 species, bit 7 alive -------------------------

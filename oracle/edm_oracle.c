@@ -86,25 +86,57 @@ double orc_ln(double q) {
   return de * ORC_LN2_HI + (de * ORC_LN2_LO + lnm);
 }
 
-/* Standard normal pair by the Marsaglia polar method (Marsaglia & Bray 1964),
- * attempt t uses counter b = t.  64 attempts fail with probability 1e-43. */
+/* sin and cos of 2 pi u, u in [0, 1): 4u = k + f with f reduced to
+ * [-1/2, 1/2) (both exact), x = f pi/2 in [-pi/4, pi/4), Taylor series of
+ * sin to x^17 and cos to x^18 (truncation below 3e-19) in Horner form with
+ * a fixed operation order, then the quadrant k.  The device copy evaluates
+ * the same sequence. */
+static const double ORC_SIN_C[9] = {
+    0x1.0000000000000p+0,  -0x1.5555555555555p-3, 0x1.1111111111111p-7,
+    -0x1.a01a01a01a01ap-13, 0x1.71de3a556c734p-19, -0x1.ae64567f544e4p-26,
+    0x1.6124613a86d09p-33,  -0x1.ae7f3e733b81fp-41, 0x1.952c77030ad4ap-49};
+static const double ORC_COS_C[10] = {
+    0x1.0000000000000p+0,  -0x1.0000000000000p-1, 0x1.5555555555555p-5,
+    -0x1.6c16c16c16c17p-10, 0x1.a01a01a01a01ap-16, -0x1.27e4fb7789f5cp-22,
+    0x1.1eed8eff8d898p-29,  -0x1.93974a8c07c9dp-37, 0x1.ae7f3e733b81fp-45,
+    -0x1.6827863b97d97p-53};
+#define ORC_PI_2 0x1.921fb54442d18p+0
+
+void orc_sincos_2pi(double u, double* c, double* s) {
+  double v = u * 4.0;
+  int k = (int)v;
+  double f = v - (double)k;
+  if (f >= 0.5) {
+    f = f - 1.0;
+    k += 1;
+  }
+  double x = f * ORC_PI_2;
+  double x2 = x * x;
+  double ps = ORC_SIN_C[8];
+  for (int i = 7; i >= 0; --i) ps = ps * x2 + ORC_SIN_C[i];
+  double pc = ORC_COS_C[9];
+  for (int i = 8; i >= 0; --i) pc = pc * x2 + ORC_COS_C[i];
+  double sn = x * ps;
+  switch (k & 3) {
+    case 0: *c = pc; *s = sn; break;
+    case 1: *c = -sn; *s = pc; break;
+    case 2: *c = -pc; *s = -sn; break;
+    default: *c = sn; *s = -pc; break;
+  }
+}
+
+/* Standard normal pair by the Box-Muller transform (Box & Muller 1958) of
+ * the key's uniform pair (counter b = 0): r = sqrt(-2 ln(1 - u0)),
+ * (z0, z1) = r (cos 2 pi u1, sin 2 pi u1). */
 void orc_normal2(uint64_t seed, int64_t step, int32_t stream, uint64_t a,
                  double* z0, double* z1) {
-  for (uint64_t t = 0; t < 64; ++t) {
-    double u0, u1;
-    orc_uniform2(seed, step, stream, a, t, &u0, &u1);
-    double x = 2.0 * u0 - 1.0;
-    double y = 2.0 * u1 - 1.0;
-    double q = x * x + y * y;
-    if (q > 0.0 && q < 1.0) {
-      double f = sqrt((-2.0 * orc_ln(q)) / q);
-      *z0 = x * f;
-      *z1 = y * f;
-      return;
-    }
-  }
-  *z0 = 0.0;
-  *z1 = 0.0;
+  double u0, u1;
+  orc_uniform2(seed, step, stream, a, 0, &u0, &u1);
+  double r = sqrt(-2.0 * orc_ln(1.0 - u0));
+  double c, s;
+  orc_sincos_2pi(u1, &c, &s);
+  *z0 = r * c;
+  *z1 = r * s;
 }
 
 void orc_fill_uniform(uint64_t seed, int64_t step, int32_t stream,

@@ -24,6 +24,7 @@ void orc_uniform2(uint64_t seed, int64_t step, int32_t stream, uint64_t a,
 void orc_normal2(uint64_t seed, int64_t step, int32_t stream, uint64_t a,
                  double* z0, double* z1);
 double orc_ln(double q);
+void orc_sincos_2pi(double u, double* c, double* s);
 /* vector helpers used by the reference shim */
 void orc_fill_uniform(uint64_t seed, int64_t step, int32_t stream,
                       const int64_t* a, const int64_t* b, int64_t n,
