@@ -671,34 +671,49 @@ __global__ void __launch_bounds__(kBlock) k_move(const EdmDynParams* __restrict_
   const int id = st.ids[s] - (int)g.poff;
   const int64_t step = *st.d_step;
 
-  // pair forces, in the reference's accumulation order
+  // Pair forces.  The float64 path sums them in the reference's accumulation
+  // order (a sum of two terms is the same either way, so only three or more
+  // terms are re-summed in order).  The float32 path sums them in 2^-20
+  // fixed point, exact and independent of the sweep order, so runs repeat
+  // bit for bit.
   double Fx = 0.0, Fy = 0.0;
+  long long qx = 0, qy = 0;
   int nterms = 0;
   for_each_force_term<F64>(p, g, st, s, sp, id, [&](uint64_t, double fx, double fy) {
     ++nterms;
-    Fx += fx;
-    Fy += fy;
-  });
-  if (nterms > 1) {
-    Fx = 0.0;
-    Fy = 0.0;
-    uint64_t last = 0;
-    bool first = true;
-    for (int k = 0; k < nterms; ++k) {
-      uint64_t best = ~0ull;
-      double bx = 0.0, by = 0.0;
-      for_each_force_term<F64>(p, g, st, s, sp, id, [&](uint64_t key, double fx, double fy) {
-        if ((first || key > last) && key < best) {
-          best = key;
-          bx = fx;
-          by = fy;
-        }
-      });
-      Fx += bx;
-      Fy += by;
-      last = best;
-      first = false;
+    if constexpr (F64) {
+      Fx += fx;
+      Fy += fy;
+    } else {
+      qx += __double2ll_rn(fx * 0x1p20);
+      qy += __double2ll_rn(fy * 0x1p20);
     }
+  });
+  if constexpr (F64) {
+    if (nterms > 2) {
+      Fx = 0.0;
+      Fy = 0.0;
+      uint64_t last = 0;
+      bool first = true;
+      for (int k = 0; k < nterms; ++k) {
+        uint64_t best = ~0ull;
+        double bx = 0.0, by = 0.0;
+        for_each_force_term<F64>(p, g, st, s, sp, id, [&](uint64_t key, double fx, double fy) {
+          if ((first || key > last) && key < best) {
+            best = key;
+            bx = fx;
+            by = fy;
+          }
+        });
+        Fx += bx;
+        Fy += by;
+        last = best;
+        first = false;
+      }
+    }
+  } else {
+    Fx = (double)qx * 0x1p-20;
+    Fy = (double)qy * 0x1p-20;
   }
 
   double x, y;
