@@ -957,28 +957,25 @@ __device__ __forceinline__ int pass_stream(int kind, int idx) {
 
 // Bits of the passes in `todo` whose keyed draw for local id `id` lies below
 // the pass's threshold (the others reject the particle).
-__device__ __forceinline__ uint32_t draw_passes(const DevState& st, const DrawPlan& D, uint64_t seed, int r, int id,
-                                                int64_t step, uint32_t todo) {
+__device__ __forceinline__ uint32_t draw_passes(const DevState& st, const DrawPlan* __restrict__ D, uint64_t seed,
+                                                int r, int id, int64_t step, uint32_t todo) {
   uint32_t bits = 0;
   for (; todo; todo &= todo - 1) {
     const int k = __ffs(todo) - 1;
-    const uint64_t m = draw_u53(seed, step, pass_stream(D.kind[k], D.index[k]), (uint64_t)id, 0);
+    const uint64_t m = draw_u53(seed, step, pass_stream(D->kind[k], D->index[k]), (uint64_t)id, 0);
     if (m < st.pass_thr[(int64_t)r * kMaxPP + k]) bits |= 1u << k;
   }
   return bits;
 }
 
 __global__ void __launch_bounds__(kBlock, 8) k_pass_draws(const EdmDynParams* __restrict__ P, DevState st,
-                                                       DrawPlan D) {
-  __shared__ DrawPlan sd;
-  if (threadIdx.x == 0) sd = D;
-  __syncthreads();
-  sweep4(st, sd.any, [&](int r, int64_t s) {
+                                                       const DrawPlan* __restrict__ D, Match any) {
+  sweep4(st, any, [&](int r, int64_t s) {
     const uint8_t f = st.flags[s];
     const int sp = fl_species(f);
-    const uint32_t todo = sp < EDM_MAX_SPECIES ? sd.reach[fl_alive(f) ? 1 : 0][sp] : 0u;
+    const uint32_t todo = sp < EDM_MAX_SPECIES ? D->reach[fl_alive(f) ? 1 : 0][sp] : 0u;
     const int id = st.ids[s] - (int)P[r].particle_offset;
-    const uint32_t bits = draw_passes(st, sd, P[r].seed, r, id, *st.d_step, todo);
+    const uint32_t bits = draw_passes(st, D, P[r].seed, r, id, *st.d_step, todo);
     if (bits) {
       const int q = atomicAdd(st.pl_count, 1);
       st.pl[q] = make_int4((int)s, (int)bits, r, id);
@@ -992,7 +989,8 @@ __global__ void __launch_bounds__(kBlock, 8) k_pass_draws(const EdmDynParams* __
 // that match it (`after`) get its draws now, in its list entry (the entry
 // exists: the particle was listed for this exchange's candidates).
 template <bool F64>
-__global__ void k_recruit_apply(const EdmDynParams* __restrict__ P, int n_rep, DevState st, int e, DrawPlan D,
+__global__ void k_recruit_apply(const EdmDynParams* __restrict__ P, int n_rep, DevState st, int e,
+                                const DrawPlan* __restrict__ D,
                                 uint32_t after) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n_rep) return;
@@ -1140,14 +1138,9 @@ struct PassGroup {
 
 template <bool F64>
 __global__ void __launch_bounds__(kBlock) k_particle_passes(const EdmDynParams* __restrict__ P, DevState st,
-                                                            PassGroup G, DrawPlan D) {
-  __shared__ PassGroup sg;
-  __shared__ DrawPlan sd;
-  if (threadIdx.x == 0) {
-    sg = G;
-    sd = D;
-  }
-  __syncthreads();
+                                                            const PassGroup* __restrict__ G,
+                                                            const DrawPlan* __restrict__ D) {
+  const PassGroup& sg = *G;
   const int n = *st.pl_count;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
     const int4 e = st.pl[q];
@@ -1171,7 +1164,7 @@ __global__ void __launch_bounds__(kBlock) k_particle_passes(const EdmDynParams* 
       const uint8_t f0 = f;
       f = kind == kGroupDetach ? detach_one<F64>(p, g, st, r, s, id, pos, idx, f)
                                : convert_one<F64>(p, g, st, r, s, id, pos, idx, f);
-      if (f != f0) bits |= draw_passes(st, sd, p.seed, r, id, *st.d_step, sd.after[pk] & ~bits);
+      if (f != f0) bits |= draw_passes(st, D, p.seed, r, id, *st.d_step, D->after[pk] & ~bits);
     }
     if (bits != bits0) st.pl[q].y = (int)bits;
   }

@@ -117,6 +117,8 @@ struct EdmEngine {
   std::vector<Pass> passes;
   std::vector<PassGroup> groups;  // runs of per-particle passes (P_GROUP index)
   DrawPlan draw{};                // the draw sweep of the per-particle passes
+  DrawPlan* d_draw = nullptr;     // device copies of the plan and the runs
+  PassGroup* d_groups = nullptr;
   uint32_t rec_after[EDM_MAX_EXCH] = {};  // per recruitment apply: later passes matching a recruit
   int2* contacts = nullptr;
   int32_t* contact_count = nullptr;
@@ -419,6 +421,12 @@ struct EdmEngine {
     }
     CUDA_TRY(cudaMemcpy(pass_thr, pt.data(), sizeof(uint64_t) * pt.size(), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(cat_thr, ct.data(), sizeof(uint64_t) * ct.size(), cudaMemcpyHostToDevice));
+    int rc;
+    if ((rc = alloc(&d_draw, 1)) != EDM_OK || (rc = alloc(&d_groups, std::max<size_t>(1, groups.size()))) != EDM_OK)
+      return rc;
+    CUDA_TRY(cudaMemcpy(d_draw, &draw, sizeof(DrawPlan), cudaMemcpyHostToDevice));
+    if (!groups.empty())
+      CUDA_TRY(cudaMemcpy(d_groups, groups.data(), sizeof(PassGroup) * groups.size(), cudaMemcpyHostToDevice));
     return EDM_OK;
   }
 
@@ -465,13 +473,13 @@ struct EdmEngine {
           break;
         case P_CAT: k_catalytic<F64><<<cgrid, kBlock, 0, s>>>(dp, st, ps.index); break;
         case P_REC_APPLY:
-          k_recruit_apply<F64><<<rb, 128, 0, s>>>(dp, R, st, ps.index, draw, rec_after[ps.index]);
+          k_recruit_apply<F64><<<rb, 128, 0, s>>>(dp, R, st, ps.index, d_draw, rec_after[ps.index]);
           break;
         case P_DRAWS:
           cudaMemsetAsync(pl_count, 0, sizeof(int32_t), s);
-          k_pass_draws<<<sgrid, kBlock, 0, s>>>(dp, st, draw);
+          k_pass_draws<<<sgrid, kBlock, 0, s>>>(dp, st, d_draw, draw.any);
           break;
-        case P_GROUP: k_particle_passes<F64><<<148, kBlock, 0, s>>>(dp, st, groups[ps.index], draw); break;
+        case P_GROUP: k_particle_passes<F64><<<148, kBlock, 0, s>>>(dp, st, d_groups + ps.index, d_draw); break;
         case P_REC_CAND:
         case P_DETACH:
         case P_CONV: break;  // fused into P_GROUP passes
