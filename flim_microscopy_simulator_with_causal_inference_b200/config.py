@@ -367,6 +367,14 @@ class SimulationConfig:
     ram_limit_gb: float = 12.0
     displacement_cap_fraction: float = 0.5
     region_smoothing_width: float = 0.05
+    # engine switches that the reference's scripts set on the config object
+    # (read with getattr in dynamics.py:2078-2120; not YAML keys there)
+    use_adaptation: bool = False
+    adaptation_tau_w: float = 60.0
+    adaptation_K_w: float = 10.0
+    adaptation_n_w: float = 2.0
+    use_local_pi3k_recruitment: bool = False
+    recruit_sigma: float = 0.5
     _species_map: Dict[str, int] = field(default_factory=dict, repr=False)
     _fluoro_map: Dict[str, int] = field(default_factory=dict, repr=False)
 
@@ -539,6 +547,10 @@ def _fluorophore(d: Dict[str, Any]) -> FluorophoreType:
     return f
 
 
+SCRIPT_ATTRIBUTES = ("use_adaptation", "adaptation_tau_w", "adaptation_K_w", "adaptation_n_w",
+                     "use_local_pi3k_recruitment", "recruit_sigma")
+
+
 def config_from_dict(raw: Dict[str, Any]) -> SimulationConfig:
     """Build and validate a SimulationConfig from an already-parsed YAML dict."""
     if not isinstance(raw, dict):
@@ -606,6 +618,12 @@ def config_from_dict(raw: Dict[str, Any]) -> SimulationConfig:
         n_threads=raw.get("n_threads", 8),
         ram_limit_gb=raw.get("ram_limit_gb", 12.0),
     )
+    # "_script_attributes": the switches a script would set on the config
+    # object after loading (e.g. use_adaptation); kept out of the YAML schema
+    for k, v in raw.get("_script_attributes", {}).items():
+        if k not in SCRIPT_ATTRIBUTES:
+            raise ConfigError(f"unknown script attribute '{k}'")
+        setattr(cfg, k, v)
     cfg.validate()
     return cfg
 

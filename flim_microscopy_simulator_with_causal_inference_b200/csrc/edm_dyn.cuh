@@ -84,6 +84,10 @@ struct DevState {
   int4* pl;
   int32_t* pl_count;
   int32_t* pl_index;
+  // per global grid cell: the adaptation field w (float64, on the adaptation
+  // grid's cells) and the local-recruitment CDF (on a feedback grid's cells)
+  double* adapt_w;
+  double* local_cdf;
   int n_rep;
   int64_t n_slots;
 };
@@ -324,6 +328,33 @@ __device__ __forceinline__ int64_t grid_cell_of(const EdmGrid& G, double x, doub
   const int gx = clampi((int)__ddiv_rn(x, G.sx), G.nx);
   const int gy = clampi((int)__ddiv_rn(y, G.sy), G.ny);
   return G.offset + (int64_t)gx * G.ny + gy;
+}
+
+// Density of a grid cell holding k particles: the reference's k-fold
+// sequential float64 sum of inv_area (dynamics.py:1685-1703).
+__device__ __forceinline__ double kfold_density(int k, double inv_area) {
+  double rho = 0.0;
+  for (int i = 0; i < k; ++i) rho = __dadd_rn(rho, inv_area);
+  return rho;
+}
+
+// Adaptation factor 1/(1 + (w/K)^n) of catalytic feedback rule `rule` at
+// (x, y) (dynamics.py:1077-1083): w is read as adaptation_field[gx, gy] with
+// the feedback grid's (gx, gy), i.e. at flat index gx * ny_adapt + gy of the
+// adaptation grid (the host rejects grids where that leaves the array); w = 0
+// without a PIP3 grid.
+__device__ __forceinline__ double adapt_factor(const EdmDynParams& p, const double* __restrict__ w_all, int rule,
+                                               double x, double y) {
+  const EdmGrid& G = p.grid[p.rule[rule].grid];
+  const int gx = clampi((int)__ddiv_rn(x, G.sx), G.nx);
+  const int gy = clampi((int)__ddiv_rn(y, G.sy), G.ny);
+  double w = 0.0;
+  if (p.adapt_grid >= 0) {
+    const EdmGrid& A = p.grid[p.adapt_grid];
+    w = w_all[A.offset + (int64_t)gx * A.ny + gy];
+  }
+  if (p.adapt_K > 0) return __ddiv_rn(1.0, __dadd_rn(1.0, pow(__ddiv_rn(w, p.adapt_K), p.adapt_n)));
+  return 1.0;
 }
 
 // Add d to every grid counting species sp, at (x, y) — into `arr`.
@@ -921,6 +952,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_catalytic(const EdmDynParams* __r
     abs_pos<F64>(st.pos_post, st.cell_post, es.y, g, xs, ys);
     double peff = C.prob;
     if (C.rule >= 0) peff = C.prob * rule_factor(p, C.rule, st, xs, ys);
+    if (C.rule >= 0 && ((p.adapt_cat_mask >> cidx) & 1)) peff = peff * adapt_factor(p, st.adapt_w, C.rule, xs, ys);
     if (u < peff) {
       if (cas_u8(&st.flags[es.y], fs, fl_make(C.product, true))) {
         atomic_add_i64(&st.counters[(int64_t)r * EDM_NCOUNTERS + EDM_C_CATALYTIC], 1);
@@ -1050,8 +1082,26 @@ __device__ __forceinline__ void recruit_candidate(const EdmDynParams& p, const D
   const EdmExch& X = p.exch[e];
   const int64_t step = *st.d_step;
   const double ua = uniform1(p.seed, step, EDM_S_EX_ACCEPT + 4 * e, (uint64_t)id, 0);
-  const U2 up = uniform2(p.seed, step, EDM_S_EX_POS + 4 * e, (uint64_t)id, 0);
-  const double cx = up.u0 * p.Lx, cy = up.u1 * p.Ly;
+  double cx, cy;
+  if (X.local_recruit) {  // density-biased position (dynamics.py:1115-1217)
+    const EdmGrid& G = p.grid[p.rule[X.rule_on].grid];
+    const double rl = uniform1(p.seed, step, EDM_S_EX_LOC + 4 * e, (uint64_t)id, 0);
+    const U2 off = normal2(p.seed, step, EDM_S_EX_OFFSET + e, (uint64_t)id);
+    const double* cdf = st.local_cdf + G.offset;
+    int lo = 0, hi = G.nx * G.ny - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (cdf[mid] < rl) lo = mid + 1;
+      else hi = mid;
+    }
+    const int gx = lo / G.ny, gy = lo - gx * G.ny;
+    cx = py_fmod(__dadd_rn(__dmul_rn(__dadd_rn((double)gx, 0.5), G.sx), __dmul_rn(off.u0, p.recruit_sigma)), p.Lx);
+    cy = py_fmod(__dadd_rn(__dmul_rn(__dadd_rn((double)gy, 0.5), G.sy), __dmul_rn(off.u1, p.recruit_sigma)), p.Ly);
+  } else {
+    const U2 up = uniform2(p.seed, step, EDM_S_EX_POS + 4 * e, (uint64_t)id, 0);
+    cx = up.u0 * p.Lx;
+    cy = up.u1 * p.Ly;
+  }
   double peff = X.prob_on;
   if (X.rule_on >= 0 && X.rule_on2 >= 0) {
     peff = X.prob_on * rule_factor(p, X.rule_on, st, cx, cy) * rule_factor(p, X.rule_on2, st, cx, cy);
@@ -1308,6 +1358,54 @@ __global__ void __launch_bounds__(kBlock) k_dissociate(const EdmDynParams* __res
 }
 
 // grid_cnt += grid_delta; grid_delta = 0
+// Adaptation field update w += dt/tau_w (rho_PIP3 - w) on every cell of each
+// replica's adaptation grid (dynamics.py:1093-1112, 2227-2242); block row =
+// replica.
+__global__ void k_adapt(const EdmDynParams* __restrict__ P, const int32_t* __restrict__ cnt,
+                        double* __restrict__ w) {
+  const EdmDynParams& p = P[blockIdx.y];
+  if (p.adapt_grid < 0) return;
+  const EdmGrid& A = p.grid[p.adapt_grid];
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.nx * A.ny; c += gridDim.x * blockDim.x) {
+    const int64_t i = A.offset + c;
+    const double rho = kfold_density(cnt[i], p.adapt_inv_area);
+    w[i] = __dadd_rn(w[i], __dmul_rn(p.adapt_inv_tau, __dadd_rn(rho, -w[i])));
+  }
+}
+
+// Local-recruitment CDF of exchange e for each replica (block = replica):
+// cumulative max(density, 0.01) over the feedback grid's cells in (gx, gy)
+// order, sequentially as the reference sums it, then divided by the total
+// (dynamics.py:2356-2371).
+__global__ void k_local_cdf(const EdmDynParams* __restrict__ P, const int32_t* __restrict__ cnt,
+                            double* __restrict__ cdf_all, int e) {
+  const EdmDynParams& p = P[blockIdx.x];
+  const EdmExch& X = p.exch[e];
+  if (!X.local_recruit || X.rule_on < 0) return;
+  const EdmRule& R = p.rule[X.rule_on];
+  const EdmGrid& G = p.grid[R.grid];
+  const int n = G.nx * G.ny;
+  double* cdf = cdf_all + G.offset;
+  for (int c = threadIdx.x; c < n; c += blockDim.x) {
+    const double rho = kfold_density(cnt[G.offset + c], R.inv_area);
+    cdf[c] = rho > 0.01 ? rho : 0.01;
+  }
+  __syncthreads();
+  __shared__ double total_s;
+  if (threadIdx.x == 0) {
+    double total = 0.0;
+    for (int c = 0; c < n; ++c) {
+      total = __dadd_rn(total, cdf[c]);
+      cdf[c] = total;
+    }
+    total_s = total;
+  }
+  __syncthreads();
+  const double total = total_s;
+  for (int c = threadIdx.x; c < n; c += blockDim.x)
+    cdf[c] = total > 0 ? __ddiv_rn(cdf[c], total) : __ddiv_rn((double)c + 1.0, (double)n);
+}
+
 __global__ void k_grid_merge(int32_t* __restrict__ cnt, int32_t* __restrict__ delta, int64_t n) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const int d = delta[i];

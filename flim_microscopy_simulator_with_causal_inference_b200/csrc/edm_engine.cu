@@ -39,7 +39,7 @@ int fail(int code, const std::string& msg) { return edm::report_error(code, msg)
   } while (0)
 
 enum PassKind { P_BIND_CAND, P_BIND_APPLY, P_DISSOC, P_CONTACTS, P_CAT, P_REC_CAND, P_REC_APPLY, P_DETACH, P_CONV, P_MERGE,
-                P_GROUP, P_DRAWS };
+                P_GROUP, P_DRAWS, P_ADAPT, P_LOCAL_CDF };
 struct Pass {
   PassKind kind;
   int index;
@@ -130,6 +130,7 @@ struct EdmEngine {
   int32_t *moved = nullptr, *moved_count = nullptr;
   int4* pl = nullptr;  // listed particles of the per-particle passes: (slot, pass bits, replica, id)
   int32_t *pl_count = nullptr, *pl_index = nullptr;
+  double *adapt_w = nullptr, *local_cdf = nullptr;  // per global grid cell
   std::vector<int32_t> emit_host;  // emitter list last uploaded
   std::vector<uint8_t> has_dye_host;  // has_dye of the last edm_set_state
   bool cells_valid = false;  // the cell list matches the state (a dynamics step ran since set_state)
@@ -175,6 +176,8 @@ struct EdmEngine {
     s.pl = pl;
     s.pl_count = pl_count;
     s.pl_index = pl_index;
+    s.adapt_w = adapt_w;
+    s.local_cdf = local_cdf;
     s.n_rep = R;
     s.n_slots = N;
     return s;
@@ -248,6 +251,14 @@ struct EdmEngine {
       passes.push_back({P_DISSOC, b, match({B.product}, 1)});
       writes({B.ra, B.rb, B.product});
     }
+    // adaptation field, after binding and before catalysis (dynamics.py:2227-2242)
+    if (p.adapt_grid >= 0) {
+      if (dirty[p.adapt_grid]) {
+        passes.push_back({P_MERGE, 0, none});
+        std::fill(dirty.begin(), dirty.end(), false);
+      }
+      passes.push_back({P_ADAPT, 0, none});
+    }
     if (p.n_cat > 0) {
       enzyme_mask = 0;
       uint32_t touched = 0;
@@ -283,6 +294,7 @@ struct EdmEngine {
     for (int e = 0; e < p.n_exch; ++e) {
       if (any_positive([&](const EdmDynParams& q) { return q.exch[e].prob_on; })) {
         reads({p.exch[e].rule_on, p.exch[e].rule_on2});
+        if (p.exch[e].local_recruit) passes.push_back({P_LOCAL_CDF, e, none});
         passes.push_back({P_REC_CAND, e, match({p.exch[e].species}, 0)});
         passes.push_back({P_REC_APPLY, e, none});
         writes({p.exch[e].species});
@@ -480,6 +492,8 @@ struct EdmEngine {
           k_pass_draws<<<sgrid, kBlock, 0, s>>>(dp, st, d_draw, draw.any);
           break;
         case P_GROUP: k_particle_passes<F64><<<148, kBlock, 0, s>>>(dp, st, d_groups + ps.index, d_draw); break;
+        case P_ADAPT: k_adapt<<<dim3(4, R), 256, 0, s>>>(dp, grid_cnt, adapt_w); break;
+        case P_LOCAL_CDF: k_local_cdf<<<R, 256, 0, s>>>(dp, grid_cnt, local_cdf, ps.index); break;
         case P_REC_CAND:
         case P_DETACH:
         case P_CONV: break;  // fused into P_GROUP passes
@@ -627,6 +641,17 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
         return fail(EDM_EINVAL, "edm_create: Hill table out of range");
       }
     }
+    if (p.adapt_grid >= p.n_grids || p.adapt_grid != p0.adapt_grid) {
+      delete E;
+      return fail(EDM_EINVAL, "edm_create: adaptation grid out of range or not shared by the replicas");
+    }
+    for (int e = 0; e < p.n_exch; ++e) {
+      if (p.exch[e].local_recruit != p0.exch[e].local_recruit ||
+          (p.exch[e].local_recruit && (p.exch[e].rule_on < 0 || p.exch[e].rule_on >= p.n_rules))) {
+        delete E;
+        return fail(EDM_EINVAL, "edm_create: local recruitment needs a feedback rule, the same in every replica");
+      }
+    }
     pfirst.push_back(np);
     pcount.push_back(p.n_particles);
     np += p.n_particles;
@@ -727,6 +752,8 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
   ALLOC(E->pl, (size_t)np);
   ALLOC(E->pl_count, 1);
   ALLOC(E->pl_index, (size_t)np);
+  ALLOC(E->adapt_w, (size_t)std::max<int64_t>(ng, 1));
+  ALLOC(E->local_cdf, (size_t)std::max<int64_t>(ng, 1));
   CUDA_TRY(cudaMemset(E->pl_index, 0xFF, sizeof(int32_t) * np));
   CUDA_TRY(cudaMemset(E->pl_count, 0, sizeof(int32_t)));
   ALLOC(E->rep_first, (size_t)n_replicas + 1);

@@ -221,7 +221,8 @@ class Engine:
         return dict(zip(self.PROFILE_GROUPS, out.astype(float).tolist()))
 
     PASS_KINDS = ("bind_candidates", "bind_apply", "dissociation", "contacts", "catalytic", "recruit_candidates",
-                  "recruit_apply", "detach", "convert", "grid_merge", "particle_passes", "pass_draws")
+                  "recruit_apply", "detach", "convert", "grid_merge", "particle_passes", "pass_draws",
+                  "adaptation", "local_cdf")
 
     def profile_passes(self, n: int, stream=None) -> list:
         """Mean device ms per dynamics step of each reaction pass, in schedule

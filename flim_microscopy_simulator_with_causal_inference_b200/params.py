@@ -73,7 +73,7 @@ class EdmCat(C.Structure):
 
 class EdmExch(C.Structure):
     _fields_ = [("species", C.c_int32), ("max_recruits", C.c_int32), ("rule_on", C.c_int32),
-                ("rule_on2", C.c_int32), ("rule_off", C.c_int32), ("pad", C.c_int32),
+                ("rule_on2", C.c_int32), ("rule_off", C.c_int32), ("local_recruit", C.c_int32),
                 ("prob_on", C.c_double), ("prob_off", C.c_double)]
 
 
@@ -105,6 +105,9 @@ class EdmDynParams(C.Structure):
         ("n_grids", C.c_int32), ("n_rules", C.c_int32),
         ("bind", EdmBind * MAX_BIND), ("cat", EdmCat * MAX_CAT), ("exch", EdmExch * MAX_EXCH),
         ("conv", EdmConv * MAX_CONV), ("grid", EdmGrid * MAX_GRIDS), ("rule", EdmRule * MAX_RULES),
+        ("adapt_grid", C.c_int32), ("adapt_cat_mask", C.c_int32),
+        ("adapt_inv_tau", C.c_double), ("adapt_K", C.c_double), ("adapt_n", C.c_double),
+        ("adapt_inv_area", C.c_double), ("recruit_sigma", C.c_double),
         ("seed", C.c_uint64),
     ]
 
@@ -210,6 +213,14 @@ class DynDerived:
     conversions: List[dict] = field(default_factory=list)
     grids: List[Tuple] = field(default_factory=list)
     rules: List[Tuple] = field(default_factory=list)
+    # adaptation field (dynamics.py:2078-2096): grid index (-1 off), modulated catalytic reactions
+    adapt_grid: int = -1
+    adapt_cat_mask: int = 0
+    adapt_inv_tau: float = 0.0
+    adapt_K: float = 0.0
+    adapt_n: float = 0.0
+    adapt_inv_area: float = 0.0
+    recruit_sigma: float = 0.5
 
 
 def derive_dynamics(config: SimulationConfig) -> DynDerived:
@@ -373,6 +384,43 @@ def derive_dynamics(config: SimulationConfig) -> DynDerived:
     for cv in config.unimolecular_conversions:
         d.conversions.append(dict(from_id=names[cv.from_species], to_id=names[cv.to_species],
                                   prob=min(1.0, cv.rate * dt), rule=rule_of(cv.feedback_rule)))
+
+    # local (density-biased) recruitment (dynamics.py:2029-2045, 2116-2120, 2354): exchanges with a
+    # single feedback rule whose name holds 'pip3_activation'
+    use_local = bool(getattr(config, "use_local_pi3k_recruitment", False))
+    d.recruit_sigma = float(getattr(config, "recruit_sigma", 0.5))
+    for ex, r in zip(config.compartment_exchanges, d.exchanges):
+        r["local"] = int(use_local and bool(ex.feedback_rule) and "pip3_activation" in ex.feedback_rule
+                         and r["rule_on"] >= 0 and r["rule_on2"] < 0)
+
+    # adaptation field (dynamics.py:2078-2096, 1998-2007): a 1 µm grid of PIP3 density relaxed with
+    # tau_w; catalytic reactions whose enzyme name holds 'PI3K' (and that have feedback) are
+    # modulated by 1/(1 + (w/K)^n), w read at the feedback grid's (gx, gy)
+    if getattr(config, "use_adaptation", False):
+        anx, any_ = max(3, int(Lx / 1.0)), max(3, int(Ly / 1.0))
+        asx, asy = Lx / anx, Ly / any_
+        pip3 = names.get("PIP3", -1)
+        if pip3 >= 0:
+            g = (pip3, anx, any_, asx, asy)
+            if g not in d.grids:
+                d.grids.append(g)
+            d.adapt_grid = d.grids.index(g)
+        d.adapt_inv_tau = dt / float(getattr(config, "adaptation_tau_w", 60.0))
+        d.adapt_K = float(getattr(config, "adaptation_K_w", 10.0))
+        d.adapt_n = float(getattr(config, "adaptation_n_w", 2.0))
+        area = asx * asy
+        d.adapt_inv_area = 1.0 / area if area > 0.0 else 0.0
+        for k, (cat, r) in enumerate(zip(config.catalytic_reactions, d.catalytic)):
+            if "PI3K" in cat.enzyme and r["rule"] >= 0:
+                _, fnx, fny, _, _ = d.grids[d.rules[r["rule"]][0]]
+                # the reference reads adaptation_field[gx, gy] with the feedback grid's (gx, gy): past
+                # its (anx, any_) array when the feedback grid is larger (undefined memory there)
+                if (fnx - 1) * any_ + (fny - 1) >= anx * any_:
+                    raise NotImplementedError(
+                        f"adaptation of catalytic reaction '{cat.name}': its feedback grid ({fnx}x{fny}) is larger "
+                        f"than the 1 µm adaptation grid ({anx}x{any_}); the reference then reads past the "
+                        "adaptation array (dynamics.py:1078). Use a 1 µm feedback grid_resolution.")
+                d.adapt_cat_mask |= 1 << k
     return d
 
 
@@ -401,10 +449,6 @@ def n_buckets(d: DynDerived) -> int:
 
 def check_supported(config: SimulationConfig) -> None:
     """Features of the reference outside this engine raise here, loudly."""
-    if getattr(config, "use_adaptation", False):
-        raise NotImplementedError("use_adaptation (dynamics.py:1093-1112) is not implemented on the GPU path")
-    if getattr(config, "use_local_pi3k_recruitment", False):
-        raise NotImplementedError("use_local_pi3k_recruitment (dynamics.py:1115-1217) is not implemented on the GPU path")
     if config.n_species > MAX_SPECIES:
         raise ConfigError(f"at most {MAX_SPECIES} species")
     for cat in config.catalytic_reactions:
@@ -497,6 +541,7 @@ def build_dyn_params(config: SimulationConfig, n_particles: int, seed: Optional[
         e = P.exch[k]
         e.species, e.max_recruits = r["species"], r["max_recruits"]
         e.rule_on, e.rule_on2, e.rule_off = r["rule_on"], r["rule_on2"], r["rule_off"]
+        e.local_recruit = r["local"]
         e.prob_on, e.prob_off = r["prob_on"], r["prob_off"]
     P.n_conv = len(d.conversions)
     for k, r in enumerate(d.conversions):
@@ -523,6 +568,9 @@ def build_dyn_params(config: SimulationConfig, n_particles: int, seed: Optional[
         R.K_half, R.n_hill, R.basal, R.inv_area = K, n, basal, inv_area
         tables.append(hill_table(inv_area, K, n, inhib, basal, tlen))
         hoff += tlen
+    P.adapt_grid, P.adapt_cat_mask = d.adapt_grid, d.adapt_cat_mask
+    P.adapt_inv_tau, P.adapt_K, P.adapt_n = d.adapt_inv_tau, d.adapt_K, d.adapt_n
+    P.adapt_inv_area, P.recruit_sigma = d.adapt_inv_area, d.recruit_sigma
     P.seed = int(config.random_seed if seed is None else seed) & 0xFFFFFFFFFFFFFFFF
     hill = np.concatenate(tables) if tables else np.zeros(0, dtype=np.float64)
     return P, hill, d

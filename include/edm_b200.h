@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define EDM_ABI_VERSION 1
+#define EDM_ABI_VERSION 2
 
 /* ---- fixed capacities of the parameter blocks --------------------------- */
 #define EDM_MAX_SPECIES 16
@@ -114,7 +114,8 @@ typedef struct {
 
 typedef struct {
   int32_t species, max_recruits;
-  int32_t rule_on, rule_on2, rule_off, pad; /* -1 when absent                 */
+  int32_t rule_on, rule_on2, rule_off;      /* -1 when absent                 */
+  int32_t local_recruit; /* 1: density-biased positions (dynamics.py:1115-1217) */
   double prob_on, prob_off;
 } EdmExch;
 
@@ -159,6 +160,14 @@ typedef struct {
   EdmConv conv[EDM_MAX_CONV];
   EdmGrid grid[EDM_MAX_GRIDS];
   EdmRule rule[EDM_MAX_RULES];
+  /* adaptation field (dynamics.py:1093-1112, 2078-2096, 2227-2242):
+   * adapt_grid = the grid counting PIP3 on the 1 µm adaptation grid, -1 off;
+   * catalytic reaction c is modulated when bit c of adapt_cat_mask is set */
+  int32_t adapt_grid, adapt_cat_mask;
+  double adapt_inv_tau;  /* dt / tau_w                                        */
+  double adapt_K, adapt_n;
+  double adapt_inv_area; /* 1 / (cell_sx cell_sy) of the adaptation grid      */
+  double recruit_sigma;  /* Gaussian spread of local recruitment (µm)         */
   /* noise key */
   uint64_t seed;
 } EdmDynParams;
@@ -337,7 +346,8 @@ int edm_profile_steps(EdmEngine* eng, int32_t n_steps, int32_t with_photons,
  * apply, 2 dissociation, 3 catalytic contacts, 4 catalytic pass, 6
  * recruitment apply, 9 grid merge, 10 run of recruitment-candidate,
  * detachment and conversion passes over the listed particles, 11 the draw
- * sweep that lists them).  Returns the number of passes (at most
+ * sweep that lists them, 12 adaptation-field update, 13 local-recruitment
+ * CDF).  Returns the number of passes (at most
  * cap) or a negative error.  No reference counterpart. */
 int edm_profile_passes(EdmEngine* eng, int32_t n_steps, float* ms_out,
                        int32_t* kinds_out, int32_t cap, void* stream);

@@ -237,12 +237,17 @@ int orc_dyn_alloc(OrcDyn* s, const EdmDynParams* p, int64_t N) {
   if (!s->pos || !s->species || !s->alive || !s->bond || !s->head || !s->next ||
       !s->pairs || !s->forces)
     return -1;
+  if (p->adapt_grid >= 0) {  /* dynamics.py:2088-2090: zeros */
+    const EdmGrid* A = &p->grid[p->adapt_grid];
+    s->adapt_w = (double*)calloc((size_t)A->nx * A->ny, sizeof(double));
+    if (!s->adapt_w) return -1;
+  }
   return 0;
 }
 
 void orc_dyn_free(OrcDyn* s) {
   free(s->pos); free(s->species); free(s->alive); free(s->bond);
-  free(s->head); free(s->next); free(s->pairs); free(s->forces);
+  free(s->head); free(s->next); free(s->pairs); free(s->forces); free(s->adapt_w);
   memset(s, 0, sizeof(*s));
 }
 
@@ -275,6 +280,19 @@ static double hill_at(const EdmDynParams* p, int rule, const double* dens, doubl
     double h = ratio_n / (1.0 + ratio_n);
     return R->basal + (1.0 - R->basal) * h;
   }
+  return 1.0;
+}
+
+/* Adaptation factor 1/(1 + (w/K)^n) (dynamics.py:1077-1083): w is read as
+ * adaptation_field[gx, gy] with the feedback grid's (gx, gy), i.e. at flat
+ * index gx * ny_adapt + gy of the adaptation array; w = 0 without PIP3. */
+static double adapt_at(const EdmDynParams* p, const OrcDyn* s, int rule, double x, double y) {
+  const EdmGrid* G = &p->grid[p->rule[rule].grid];
+  int gx = clampi((int)(x / G->sx), G->nx);
+  int gy = clampi((int)(y / G->sy), G->ny);
+  double w = 0.0;
+  if (p->adapt_grid >= 0) w = s->adapt_w[gx * p->grid[p->adapt_grid].ny + gy];
+  if (p->adapt_K > 0) return 1.0 / (1.0 + pow(w / p->adapt_K, p->adapt_n));
   return 1.0;
 }
 
@@ -513,6 +531,14 @@ int orc_dyn_step(const EdmDynParams* p, OrcDyn* s, int64_t step) {
   double* dens1 = (double*)malloc(sizeof(double) * (size_t)gmax);
   double* dens2 = (double*)malloc(sizeof(double) * (size_t)gmax);
 
+  /* 7a. adaptation field: w += dt/tau_w (rho_PIP3 - w) (dynamics.py:1093-1112, 2227-2242) */
+  if (p->adapt_grid >= 0) {
+    const EdmGrid* A = &p->grid[p->adapt_grid];
+    density_field(p, s, p->adapt_grid, dens1);
+    for (int64_t c = 0; c < (int64_t)A->nx * A->ny; ++c)
+      s->adapt_w[c] += p->adapt_inv_tau * (dens1[c] - s->adapt_w[c]);
+  }
+
   /* 7b. catalytic passes (dynamics.py:825-983, 2245-2297) */
   for (int c = 0; c < p->n_cat; ++c) {
     const EdmCat* C = &p->cat[c];
@@ -529,6 +555,7 @@ int orc_dyn_step(const EdmDynParams* p, OrcDyn* s, int64_t step) {
       if (dsq > C->contact_sq) continue;
       double peff = C->prob;
       if (C->rule >= 0) peff = C->prob * hill_at(p, C->rule, dens1, pos[2 * si], pos[2 * si + 1]);
+      if (C->rule >= 0 && ((p->adapt_cat_mask >> c) & 1)) peff = peff * adapt_at(p, s, C->rule, pos[2 * si], pos[2 * si + 1]);
       double u0, u1;
       orc_uniform2(seed, step, EDM_S_CAT + c, (uint64_t)i, (uint64_t)j, &u0, &u1);
       if (u0 < peff) {
@@ -549,6 +576,21 @@ int orc_dyn_step(const EdmDynParams* p, OrcDyn* s, int64_t step) {
       density_field(p, s, p->rule[X->rule_on].grid, dens1);
     }
     int64_t nrec = 0;
+    /* local recruitment: CDF of max(density, 0.01) over the feedback grid (dynamics.py:2356-2371) */
+    const EdmGrid* LG = X->rule_on >= 0 ? &p->grid[p->rule[X->rule_on].grid] : NULL;
+    int64_t ncdf = 0;
+    if (X->local_recruit && LG) {
+      ncdf = (int64_t)LG->nx * LG->ny;
+      double total = 0.0;
+      for (int64_t k = 0; k < ncdf; ++k) {
+        total += dens1[k] > 0.01 ? dens1[k] : 0.01;
+        dens2[k] = total;
+      }
+      if (total > 0)
+        for (int64_t k = 0; k < ncdf; ++k) dens2[k] /= total;
+      else
+        for (int64_t k = 0; k < ncdf; ++k) dens2[k] = (k + 1.0) / (double)ncdf;
+    }
     for (int64_t i = 0; i < N; ++i) {
       if (nrec >= X->max_recruits) break;
       if (alive[i]) continue;
@@ -557,6 +599,20 @@ int orc_dyn_step(const EdmDynParams* p, OrcDyn* s, int64_t step) {
       orc_uniform2(seed, step, EDM_S_EX_ACCEPT + 4 * e, (uint64_t)i, 0, &ua, &ub);
       orc_uniform2(seed, step, EDM_S_EX_POS + 4 * e, (uint64_t)i, 0, &px, &py);
       double cx = px * p->Lx, cy = py * p->Ly;
+      if (ncdf > 0) {  /* dynamics.py:1115-1217 */
+        double rl, rl2, o0, o1;
+        orc_uniform2(seed, step, EDM_S_EX_LOC + 4 * e, (uint64_t)i, 0, &rl, &rl2);
+        orc_normal2(seed, step, EDM_S_EX_OFFSET + e, (uint64_t)i, &o0, &o1);
+        int64_t lo = 0, hi = ncdf - 1;
+        while (lo < hi) {
+          int64_t mid = (lo + hi) / 2;
+          if (dens2[mid] < rl) lo = mid + 1;
+          else hi = mid;
+        }
+        int64_t gx = lo / LG->ny, gy = lo % LG->ny;
+        cx = py_fmod(((double)gx + 0.5) * LG->sx + o0 * p->recruit_sigma, p->Lx);
+        cy = py_fmod(((double)gy + 0.5) * LG->sy + o1 * p->recruit_sigma, p->Ly);
+      }
       double peff = X->prob_on;
       if (dual) {
         peff = X->prob_on * hill_at(p, X->rule_on, dens1, cx, cy) * hill_at(p, X->rule_on2, dens2, cx, cy);

@@ -48,6 +48,7 @@ typedef struct {
   int32_t* pairs;     /* [max_pairs][2]       */
   int64_t n_pairs, max_pairs;
   double* forces;     /* [N][2]               */
+  double* adapt_w;    /* adaptation field w [nx][ny] of the adaptation grid, or NULL */
 } OrcDyn;
 
 int orc_dyn_alloc(OrcDyn* s, const EdmDynParams* p, int64_t N);

@@ -91,7 +91,7 @@ class OrcDyn(C.Structure):
                 ("alive", C.c_void_p), ("bond", C.c_void_p),
                 ("counters", C.c_int64 * NCOUNTERS), ("head", C.c_void_p), ("next", C.c_void_p),
                 ("pairs", C.c_void_p), ("n_pairs", C.c_int64), ("max_pairs", C.c_int64),
-                ("forces", C.c_void_p)]
+                ("forces", C.c_void_p), ("adapt_w", C.c_void_p)]
 
 
 class OrcPhotParams(C.Structure):

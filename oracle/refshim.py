@@ -57,6 +57,8 @@ def ref_config_from_dict(raw: dict, overrides: dict | None = None):
     """Load a YAML dict through the reference's own loader."""
     ed = import_reference()
     from ed_mrdt.config import load_config
+    raw = dict(raw)
+    overrides = {**raw.pop("_script_attributes", {}), **(overrides or {})}
     with tempfile.NamedTemporaryFile("w", suffix=".yaml", delete=False) as fh:
         yaml.safe_dump(raw, fh)
         path = fh.name
@@ -167,9 +169,14 @@ class ShimmedDynamics:
             q.append(("random", O.uniforms(s, t, S_DISSOC + 2 * r, ids)))
         for c, _ in enumerate(e._catalytic_reactions):
             q.append(("random", pair_u(S_CAT + c)))
-        for x, _ in enumerate(e._compartment_exchanges):
+        for x, ex in enumerate(e._compartment_exchanges):
             q.append(("random", O.uniforms(s, t, S_EX_ACCEPT + 4 * x, ids)))
             q.append(("random", O.uniforms(s, t, S_EX_POS + 4 * x, ids, two=True)))
+            # local recruitment draws its location and offsets next (dynamics.py:2354-2373)
+            if (getattr(e, "_use_local_recruitment", False) and ex.get("use_local", False)
+                    and ex["feedback"] is not None and ex["feedback_2"] is None):
+                q.append(("random", O.uniforms(s, t, S_EX_LOC + 4 * x, ids)))
+                q.append(("standard_normal", lambda shape, x=x: O.normals(s, t, S_EX_OFFSET + x, ids)))
             q.append(("random", O.uniforms(s, t, S_EX_DETACH + 4 * x, ids)))
         for v, _ in enumerate(e._unimolecular_conversions):
             q.append(("random", O.uniforms(s, t, S_CONV + v, ids)))

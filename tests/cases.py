@@ -91,6 +91,22 @@ def exchange_heavy(seed: int = 17) -> dict:
     return d
 
 
+def adaptive_local(seed: int = 19) -> dict:
+    """rich_small with the two script-set switches of the reference's PIP3/PTEN
+    wave script: the adaptation field (tau_w shortened to 10 ms so that w
+    follows the PIP3 density within the test) and density-biased local PI3K
+    recruitment; feedback grids at 1 µm, as that script sets them."""
+    d = rich_small(seed=seed)
+    for fb in d["feedback_rules"]:
+        fb["grid_resolution"] = 1.0
+    for ex in d["compartment_exchanges"]:
+        ex["k_on"] *= 5.0
+    d["_script_attributes"] = {"use_adaptation": True, "adaptation_tau_w": 0.01, "adaptation_K_w": 10.0,
+                               "adaptation_n_w": 2.0, "use_local_pi3k_recruitment": True,
+                               "recruit_sigma": 0.5}
+    return d
+
+
 CASES = {
     "rich_small": rich_small,
     "binding_regions": binding_regions,
@@ -98,6 +114,7 @@ CASES = {
     "sine_small": sine_small,
     "proximity_small": proximity_small,
     "exchange_heavy": exchange_heavy,
+    "adaptive_local": adaptive_local,
 }
 
 

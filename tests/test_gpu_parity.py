@@ -30,7 +30,8 @@ def test_noise_streams_bit_identical():
         assert np.array_equal(device_uniforms(seed, step, stream, keys, b), O.uniforms(seed, step, stream, keys, b, two=True))
 
 
-@pytest.mark.parametrize("case", ["rich_small", "binding_regions", "harmonic_small", "exchange_heavy"])
+@pytest.mark.parametrize("case", ["rich_small", "binding_regions", "harmonic_small", "exchange_heavy",
+                                  "adaptive_local"])
 def test_fp64_free_running_matches_oracle(case):
     P = Pair(cases.get(case), precision=64)
     steps = 40
@@ -47,6 +48,8 @@ def test_fp64_free_running_matches_oracle(case):
     if case == "exchange_heavy":  # recruitments, detachments and conversions all fired
         assert (P.orc.counters[3:6] > 0).all(), P.orc.counters[:6]
         assert P.eng.status() == 0
+    if case == "adaptive_local":  # catalysis under adaptation and local recruitment both fired
+        assert P.orc.counters[2] > 0 and P.orc.counters[3] > 0, P.orc.counters[:6]
 
 
 def test_fp64_cell_lists_match_oracle():
@@ -99,7 +102,8 @@ def test_fp64_graph_chunks_match_eager():
     assert np.array_equal(A.eng.counters(), B.eng.counters())
 
 
-@pytest.mark.parametrize("case", ["rich_small", "binding_regions", "sine_small", "exchange_heavy"])
+@pytest.mark.parametrize("case", ["rich_small", "binding_regions", "sine_small", "exchange_heavy",
+                                  "adaptive_local"])
 def test_fp32_lockstep_matches_oracle(case):
     P = Pair(cases.get(case), precision=32)
     worst = 0.0
