@@ -117,6 +117,9 @@ struct EdmEngine {
   std::vector<Pass> passes;
   std::vector<PassGroup> groups;  // runs of per-particle passes (P_GROUP index)
   DrawPlan draw{};                // the draw sweep of the per-particle passes
+  bool draws_early = false;       // the sweep runs on side_stream beside the passes before the first run
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   DrawPlan* d_draw = nullptr;     // device copies of the plan and the runs
   PassGroup* d_groups = nullptr;
   uint32_t rec_after[EDM_MAX_EXCH] = {};  // per recruitment apply: later passes matching a recruit
@@ -364,9 +367,29 @@ struct EdmEngine {
       if (passes[i].kind == P_DETACH) draw.after[pp_of[i]] = matching_from(i + 1, state(p.exch[passes[i].index].species, 0));
       if (passes[i].kind == P_CONV) draw.after[pp_of[i]] = matching_from(i + 1, state(p.conv[passes[i].index].to, 1));
     }
+    // The sweep only reads flags and ids.  When no per-particle pass matches a
+    // species the catalytic passes convert, the passes between the binding
+    // passes and the first per-particle pass (adaptation, contact search,
+    // catalytic passes, merges) change nothing it reads, so it can start right
+    // after the binding passes, on a side stream beside them.
+    uint32_t touched = 0, pp_species = 0;
+    for (int c = 0; c < p.n_cat; ++c) touched |= (1u << p.cat[c].substrate) | (1u << p.cat[c].product);
+    for (size_t i = 0; i < passes.size(); ++i)
+      if (pp_of[i] >= 0) pp_species |= passes[i].match.mask[0] | passes[i].match.mask[1];
+    size_t at = first;
+    draws_early = false;
+    if (!(touched & pp_species)) {
+      size_t b = 0;
+      while (b < first && (passes[b].kind == P_BIND_CAND || passes[b].kind == P_BIND_APPLY || passes[b].kind == P_DISSOC))
+        ++b;
+      if (b < first) {
+        at = b;
+        draws_early = true;
+      }
+    }
     std::vector<Pass> fused;
     for (size_t i = 0; i < passes.size();) {
-      if (i == first) fused.push_back({P_DRAWS, 0, draw.any});
+      if (i == at) fused.push_back({P_DRAWS, 0, draw.any});
       if (!per_particle(passes[i].kind)) {
         if (passes[i].kind == P_REC_APPLY) {
           const int e = passes[i].index;
@@ -472,6 +495,7 @@ struct EdmEngine {
     const int sgrid = (int)std::max<int64_t>(1, (N / 4 + kBlock) / kBlock);  // 4 slots per thread
     const int cgrid = 148 * 8;
     const int gm = (int)std::min<int64_t>((n_grid + 255) / 256, 4096);
+    bool joined = true;  // the side stream's draw sweep has been waited for
     for (size_t i = 0; i < passes.size(); ++i) {
       const Pass& ps = passes[i];
       if (pass_prof) cudaEventRecord(pass_prof[i], s);
@@ -487,11 +511,30 @@ struct EdmEngine {
         case P_REC_APPLY:
           k_recruit_apply<F64><<<rb, 128, 0, s>>>(dp, R, st, ps.index, d_draw, rec_after[ps.index]);
           break;
-        case P_DRAWS:
-          cudaMemsetAsync(pl_count, 0, sizeof(int32_t), s);
-          k_pass_draws<<<sgrid, kBlock, 0, s>>>(dp, st, d_draw, draw.any);
+        case P_DRAWS: {
+          // beside the following passes on the side stream (not while timing passes one by one)
+          const bool fork = draws_early && !pass_prof && side_stream;
+          cudaStream_t ds = s;
+          if (fork) {
+            cudaEventRecord(ev_fork, s);
+            cudaStreamWaitEvent(side_stream, ev_fork, 0);
+            ds = side_stream;
+          }
+          cudaMemsetAsync(pl_count, 0, sizeof(int32_t), ds);
+          k_pass_draws<<<sgrid, kBlock, 0, ds>>>(dp, st, d_draw, draw.any);
+          if (fork) {
+            cudaEventRecord(ev_join, side_stream);
+            joined = false;
+          }
           break;
-        case P_GROUP: k_particle_passes<F64><<<148, kBlock, 0, s>>>(dp, st, d_groups + ps.index, d_draw); break;
+        }
+        case P_GROUP:
+          if (!joined) {
+            cudaStreamWaitEvent(s, ev_join, 0);
+            joined = true;
+          }
+          k_particle_passes<F64><<<148, kBlock, 0, s>>>(dp, st, d_groups + ps.index, d_draw);
+          break;
         case P_ADAPT: k_adapt<<<dim3(4, R), 256, 0, s>>>(dp, grid_cnt, adapt_w); break;
         case P_LOCAL_CDF: k_local_cdf<<<R, 256, 0, s>>>(dp, grid_cnt, local_cdf, ps.index); break;
         case P_REC_CAND:
@@ -552,6 +595,9 @@ struct EdmEngine {
   bool read_pending = false;
 
   ~EdmEngine() {
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side_stream) cudaStreamDestroy(side_stream);
     if (ev_snap) cudaEventDestroy(ev_snap);
     if (ev_read) cudaEventDestroy(ev_read);
     if (copy_stream) cudaStreamDestroy(copy_stream);
@@ -743,6 +789,11 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
   if ((rc = E->build_schedule()) != EDM_OK || (rc = E->upload_thresholds()) != EDM_OK) {
     delete E;
     return rc;
+  }
+  if (E->draws_early) {
+    CUDA_TRY(cudaStreamCreateWithFlags(&E->side_stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&E->ev_fork, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&E->ev_join, cudaEventDisableTiming));
   }
   E->contact_cap = std::max<int64_t>(4 * np, 1 << 20);  // per catalytic reaction
   ALLOC(E->contacts, (size_t)E->contact_cap * std::max(1, E->hdp[0].n_cat));
