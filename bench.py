@@ -18,6 +18,10 @@ pipeline steps, then finalize_frame (dark counts, afterpulsing).
 * roofline   the dominant kernel group's algorithmic bytes / CUDA-event time;
 * fp64_plain the plain float64 path (same kernels, one 13,000-particle
              system, per-step launches, no graphs) for the FP32/FP64 ratio;
+* large_membrane the 1.3M-particle 100x100 µm^2 harmonic membrane on the
+             float32 and float64 paths (CUDA graphs of 100 steps each), with
+             the float32 path's per-step position error in lockstep with the
+             float64 path and its reaction-count deviation over 100 steps;
 * cpu_baseline the CPU oracle (the reference algorithm restated in C) on
              this host's cores on a bounded sample of the same workload.
 
@@ -60,6 +64,7 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--flim-replicas", type=int, default=256, help="FLIM acquisition replicas (256^2 px each)")
     ap.add_argument("--no-flim", action="store_true")
+    ap.add_argument("--no-large", action="store_true", help="skip the 1.3M-particle float32-vs-float64 comparison")
     return ap.parse_args()
 
 
@@ -248,6 +253,63 @@ def flim_cpu_sample(n_replicas: int, seed: int, steps: int = 1):
             FO.poisson_histograms(e["mu"], seed + r)
     dt = time.perf_counter() - t0
     return n_replicas * steps * 65536 / dt, dt, n_replicas
+
+
+def large_membrane_bench(device: int, stream) -> dict:
+    """The 1.3M-particle membrane (100x100 µm^2, harmonic repulsion, 200x200
+    density grid) on the float32 and float64 GPU paths: throughput of each
+    (100 steps in CUDA graphs, dynamics + photons + detection), the float32
+    path's position error after one step from the float64 path's state
+    (5 lockstep steps), and the relative deviation of its reaction counts
+    after 100 free-running steps from the same initial state."""
+    import torch
+    from flim_microscopy_simulator_with_causal_inference_b200 import workloads as W
+    from flim_microscopy_simulator_with_causal_inference_b200.batch import Ensemble
+    raw = W.config2(n_frames=1)
+    ens = {prec: Ensemble([raw], precision=prec, photons=True, device=device) for prec in (32, 64)}
+    n_mem = ens[32].total_membrane
+    rates, counts = {}, {}
+    for prec, e in ens.items():
+        e.engine.pipeline_steps(100, True, 100, stream=stream)  # capture + warm
+        stream.synchronize()
+        e.upload(stream=stream)  # back to the initial state, step 0
+        e.engine.set_step(0)
+        c0 = e.engine.counters(stream=stream).sum(axis=0)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        e.engine.pipeline_steps(100, True, 100, stream=stream)
+        b.record(stream)
+        stream.synchronize()
+        rates[prec] = n_mem * 100 / (a.elapsed_time(b) / 1e3)
+        counts[prec] = e.engine.counters(stream=stream).sum(axis=0) - c0
+    ev = counts[64][2:6].astype(np.float64)
+    dev = float(np.abs(counts[32][2:6] - counts[64][2:6]).sum() / max(1.0, ev.sum()))
+    # lockstep: the float32 path steps from the float64 path's state
+    e32, e64 = ens[32].engine, ens[64].engine
+    worst = 0.0
+    same_events = True
+    for _ in range(5):
+        st = e64.get_state(stream=stream)
+        e32.set_state(st["positions"], st["species"], st["alive"], st["bond"], st["has_dye"], ens[64].host["dye"],
+                      st["ctmc"], st["bleached"], stream=stream)
+        e32.set_step(e64.get_step())
+        e64.pipeline_steps(1, True, 0, stream=stream)
+        e32.pipeline_steps(1, True, 0, stream=stream)
+        a64, a32 = e64.get_state(stream=stream), e32.get_state(stream=stream)
+        d = np.abs(a32["positions"] - a64["positions"])
+        d = np.minimum(d, np.array([100.0, 100.0]) - d)  # periodic box
+        worst = max(worst, float(d.max()))
+        same_events &= bool(np.array_equal(a32["species"], a64["species"]) and np.array_equal(a32["alive"], a64["alive"]))
+    del ens
+    torch.cuda.empty_cache()
+    return {"workload": "1.3M-particle 100x100 um^2 PIP3/PTEN membrane, harmonic repulsion, 200x200 density grid, "
+                        "dynamics + PSS photons + TCSPC per step, CUDA graphs of 100 steps",
+            "unit": UNIT, "fp32": rates[32], "fp64": rates[64], "fp32_over_fp64": rates[32] / rates[64],
+            "lockstep_max_position_error_um": worst, "lockstep_event_sets_identical": same_events,
+            "reaction_count_rel_deviation_100_steps": dev,
+            "reaction_counts_100_steps": {"fp32": counts[32][2:6].tolist(), "fp64": counts[64][2:6].tolist(),
+                                          "fields": ["catalytic", "recruited", "detached", "converted"]}}
 
 
 def flim_bench(args, device: int, rank: int, world: int, stream):
@@ -471,6 +533,10 @@ def main():
         fp64 = c1.total_membrane * n64 / (f0.elapsed_time(f1) / 1e3)
         del c1
 
+    large = None
+    if not args.no_large and rank == 0:
+        large = large_membrane_bench(device, stream)
+
     # ---- batched FLIM acquisition -------------------------------------------
     flim = None
     if not args.no_flim:
@@ -510,6 +576,7 @@ def main():
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "alg_bytes_per_particle": alg[dom], "alg_bytes": alg[dom] * N, "kernel_ms": groups[dom]},
             "kernel_ms_per_step": groups,
+            "large_membrane": large,
             "fp64_plain": None if fp64 is None else {"value": fp64, "unit": UNIT,
                                                      "workload": "13,000-particle system with sine D(x), float64, "
                                                                  "per-step launches, full BD step"},
