@@ -535,7 +535,10 @@ def main():
 
     large = None
     if not args.no_large and rank == 0:
-        large = large_membrane_bench(device, stream)
+        try:  # a secondary comparison: report its failure in the line rather than lose the line
+            large = large_membrane_bench(device, stream)
+        except Exception as ex:  # noqa: BLE001
+            large = {"error": f"{type(ex).__name__}: {ex}"}
 
     # ---- batched FLIM acquisition -------------------------------------------
     flim = None
