@@ -801,8 +801,20 @@ __global__ void __launch_bounds__(kBlock) k_move(const EdmDynParams* __restrict_
     for (int it = 0; it < 64 && o.x < 0.0f; ++it) { o.x += g.sxf; --cx; }
     for (int it = 0; it < 64 && o.y >= g.syf; ++it) { o.y -= g.syf; ++cy; }
     for (int it = 0; it < 64 && o.y < 0.0f; ++it) { o.y += g.syf; --cy; }
-    if (o.x >= g.sxf || o.x < 0.0f) o.x = 0.0f;
-    if (o.y >= g.syf || o.y < 0.0f) o.y = 0.0f;
+    // a tiny negative offset plus the cell side rounds to the cell side: the
+    // point is the next cell's origin (not this cell's, a cell away)
+    if (o.x >= g.sxf) {
+      o.x = 0.0f;
+      ++cx;
+    } else if (o.x < 0.0f) {
+      o.x = 0.0f;
+    }
+    if (o.y >= g.syf) {
+      o.y = 0.0f;
+      ++cy;
+    } else if (o.y < 0.0f) {
+      o.y = 0.0f;
+    }
     if (g.px) {  // |cx| stays within 64 cells of the box: a few wraps at most
       while (cx >= g.nx) cx -= g.nx;
       while (cx < 0) cx += g.nx;

@@ -148,3 +148,37 @@ def test_fp64_proximity_photons_before_any_dynamics_step():
     assert pid.size > 0
     assert np.array_equal(pid, ob[0]) and np.array_equal(ch, ob[2]) and np.array_equal(fr, ob[3])
     np.testing.assert_allclose(tt, ob[1], rtol=1e-14, atol=0)
+
+
+def test_fp32_lockstep_large_membrane_no_cell_jumps():
+    """The float32 path against the float64 path on the 1.3M-particle membrane
+    (1.86M with pools), one step at a time from the float64 state: a particle
+    whose offset lands within rounding of a cell's lower side must stay there,
+    not a cell (0.165 µm) away.  Strongly overlapping harmonic pairs move by
+    the displacement cap in a float32 direction, so the bound here is 1e-4 µm,
+    still three orders below a cell."""
+    import torch
+    from flim_microscopy_simulator_with_causal_inference_b200 import workloads as W
+    from flim_microscopy_simulator_with_causal_inference_b200.batch import Ensemble
+    raw = W.config2(n_frames=1)
+    s = torch.cuda.Stream()
+    ens = {p: Ensemble([raw], precision=p, photons=True, device=0) for p in (32, 64)}
+    e32, e64 = ens[32].engine, ens[64].engine
+    dye = ens[64].host["dye"]
+    e64.pipeline_steps(5, True, 0, stream=s)
+    worst = 0.0
+    for _ in range(4):
+        st = e64.get_state(stream=s)
+        e32.set_state(st["positions"], st["species"], st["alive"], st["bond"], st["has_dye"], dye, st["ctmc"],
+                      st["bleached"], stream=s)
+        e32.set_step(e64.get_step())
+        e64.pipeline_steps(1, True, 0, stream=s)
+        e32.pipeline_steps(1, True, 0, stream=s)
+        a64, a32 = e64.get_state(stream=s), e32.get_state(stream=s)
+        assert np.array_equal(a32["species"], a64["species"]) and np.array_equal(a32["alive"], a64["alive"])
+        d = np.abs(a32["positions"] - a64["positions"])
+        d = np.minimum(d, 100.0 - d)  # periodic 100 µm box
+        worst = max(worst, float(d.max()))
+    assert worst < 1e-4, worst
+    del ens
+    torch.cuda.empty_cache()
