@@ -653,6 +653,11 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
   E->has_scope = scope != nullptr && phot != nullptr;
   if (E->has_phot) E->hpp.assign(phot, phot + n_replicas);
   if (E->has_scope) E->hsp.assign(scope, scope + n_replicas);
+  for (int r = 0; E->has_scope && r < n_replicas; ++r)
+    if (E->hsp[r].psf_range_px < 0 || E->hsp[r].psf_range_px > kPsfMaxR) {
+      delete E;
+      return fail(EDM_EUNSUP, "edm_create: PSF window wider than 16 pixels each side (pixels below sigma/4)");
+    }
   // validate the CSR layout and that every replica has the same pass structure
   int64_t np = 0, nc = 0, ng = 0, ne = 0, nph = 0, nfl = 0;
   std::vector<int64_t> pfirst, pcount, efirst, ecount, phfirst, phcount, pxfirst, pxcount;

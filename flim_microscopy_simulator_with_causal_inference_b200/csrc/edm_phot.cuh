@@ -17,6 +17,8 @@
 
 namespace edm {
 
+constexpr int kPsfMaxR = 16;  // largest PSF window half-width in pixels (4 sigma / pixel, rounded up)
+
 struct PhotState {
   const int32_t* emit_id;   // global particle id of each emitter (particle order per replica)
   int32_t* emit_n;          // photons (donor + acceptor) of the current batch
@@ -335,17 +337,28 @@ __global__ void __launch_bounds__(kBlock) k_scope(const EdmDynParams* __restrict
   const int R = sp.psf_range_px;
   if (i0 < -R || i0 >= sp.nx + R) return;
   if (j0 < -R || j0 >= sp.ny + R) return;
+  // Pixel weights exp(-(dx^2 + dy^2) / 2 sigma^2) over the in-FOV pixels of
+  // the (2R+1)^2 window, summed and searched in the reference's order (di
+  // outer, dj inner): the Gaussian factors into exp(-dx^2 / 2 sigma^2)
+  // exp(-dy^2 / 2 sigma^2), so a window costs 2(2R+1)+(2R+1) exps, not
+  // 2(2R+1)^2 (the weights differ from the unfactored form by an ulp or two).
+  double wy[2 * kPsfMaxR + 1];
+  const int Rc = R <= kPsfMaxR ? R : kPsfMaxR;  // the host keeps R <= kPsfMaxR
+  for (int dj = -Rc; dj <= Rc; ++dj) {
+    const int jj = j0 + dj;
+    const double dy = y - (((double)jj + 0.5) * sp.pixel_size + sp.offset_y);
+    wy[dj + Rc] = (jj < 0 || jj >= sp.ny) ? -1.0 : exp(-(dy * dy) * inv2);
+  }
   double total = 0.0;
   int n = 0;
-  for (int di = -R; di <= R; ++di) {
+  for (int di = -Rc; di <= Rc; ++di) {
     const int ii = i0 + di;
     if (ii < 0 || ii >= sp.nx) continue;
     const double dx = x - (((double)ii + 0.5) * sp.pixel_size + sp.offset_x);
-    for (int dj = -R; dj <= R; ++dj) {
-      const int jj = j0 + dj;
-      if (jj < 0 || jj >= sp.ny) continue;
-      const double dy = y - (((double)jj + 0.5) * sp.pixel_size + sp.offset_y);
-      total += exp(-(dx * dx + dy * dy) * inv2);
+    const double wx = exp(-(dx * dx) * inv2);
+    for (int dj = 0; dj <= 2 * Rc; ++dj) {
+      if (wy[dj] < 0.0) continue;
+      total += wx * wy[dj];
       ++n;
     }
   }
@@ -353,19 +366,19 @@ __global__ void __launch_bounds__(kBlock) k_scope(const EdmDynParams* __restrict
   const double u = uniform1(p.seed, key, EDM_S_SC_ASSIGN, (uint64_t)k, 0) * total;
   int si = -1, sj = -1, fi = -1, fj = -1;
   double cum = 0.0;
-  for (int di = -R; di <= R && si < 0; ++di) {
+  for (int di = -Rc; di <= Rc && si < 0; ++di) {
     const int ii = i0 + di;
     if (ii < 0 || ii >= sp.nx) continue;
     const double dx = x - (((double)ii + 0.5) * sp.pixel_size + sp.offset_x);
-    for (int dj = -R; dj <= R; ++dj) {
-      const int jj = j0 + dj;
-      if (jj < 0 || jj >= sp.ny) continue;
+    const double wx = exp(-(dx * dx) * inv2);
+    for (int dj = 0; dj <= 2 * Rc; ++dj) {
+      if (wy[dj] < 0.0) continue;
+      const int jj = j0 + dj - Rc;
       if (fi < 0) {
         fi = ii;
         fj = jj;
       }
-      const double dy = y - (((double)jj + 0.5) * sp.pixel_size + sp.offset_y);
-      cum += exp(-(dx * dx + dy * dy) * inv2);
+      cum += wx * wy[dj];
       if (cum >= u) {
         si = ii;
         sj = jj;
