@@ -219,40 +219,56 @@ def reference_arm(args, rank: int, world: int):
                                f"{steps_used} BD steps per timed step, about 10 s)", "replicas": args.replicas},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"16 median-size replicas x {steps_used} full BD steps "
-                                   "(dynamics+photophysics+TCSPC), about 10 s per timed step"},
+                                   "(dynamics+photophysics+TCSPC), about 10 s per timed step, on " + PORT_NOTE},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     if not args.no_flim:
-        fv, fdt, fr = flim_cpu_sample(16, args.seed)
+        fv, fdt, fr, fcores = flim_cpu_sample(16, args.seed)
         line["flim"] = {"metric": "FLIM px/s", "value": fv, "unit": "px/s",
                         "workload": FLIM_WORKLOAD.format(R=args.flim_replicas),
-                        "cpu_baseline": {"value": fv, "unit": "px/s", "cores": 1, "kind": "port",
+                        "cpu_baseline": {"value": fv, "unit": "px/s", "cores": fcores, "kind": "port",
                                          "sample": f"{fr} replicas, float64 numpy restatement + numpy Poisson "
-                                                   f"({fdt:.1f} s); the reference has no batched acquisition"}}
+                                                   f"({fdt:.1f} s), one replica per process; the reference has no "
+                                                   "batched acquisition"}}
     print(json.dumps(line), flush=True)
 
 
 FLIM_WORKLOAD = ("batched FLIM acquisition: {R} replicas x 256x256 px x 256 bins, 50,000 donors per replica "
                  "(bound fraction U(0,1)), 31-tap PSF (sigma 100 nm), 1000 photons/px budget")
 FLIM_BYTES_PER_PX = 256 * 4 + 8  # histogram written + the two intensity values read
+PORT_NOTE = ("the C restatement of the reference's algorithm (oracle/edm_oracle.c, pinned bit-exactly to the "
+             "reference), not the reference's own Python/Numba code")
 
 
-def flim_cpu_sample(n_replicas: int, seed: int, steps: int = 1):
-    """The float64 numpy restatement (oracle/flim_oracle.py) of the acquisition
-    on a bounded sample of replicas: expected histograms + numpy Poisson.
-    Returns FLIM px/s, seconds, replicas."""
+def _flim_cpu_replica(args):
+    """One replica of the float64 numpy restatement (a worker process's task)."""
+    n_replicas, seed, r = args
     from flim_microscopy_simulator_with_causal_inference_b200 import flim_acquire as FA
     from flim_microscopy_simulator_with_causal_inference_b200.config import config_from_dict
     from oracle import flim_oracle as FO
+    if r < 0:  # warm-up task: imports only
+        return 0
     p, _ = FA.build_flim_params(config_from_dict(FA.flim_config()), n_replicas, 50_000, 1000.0, seed)
     bf = FA.bound_fractions(n_replicas, seed)
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        for r in range(n_replicas):
-            e = FO.acquire_expected(p, bf, r)
-            FO.poisson_histograms(e["mu"], seed + r)
-    dt = time.perf_counter() - t0
-    return n_replicas * steps * 65536 / dt, dt, n_replicas
+    e = FO.acquire_expected(p, bf, r)
+    FO.poisson_histograms(e["mu"], seed + r)
+    return 65536
+
+
+def flim_cpu_sample(n_replicas: int, seed: int):
+    """The float64 numpy restatement (oracle/flim_oracle.py) of the acquisition
+    on a bounded sample of replicas, one replica per worker process on every
+    host core (spawned: the parent holds a CUDA context).  Returns FLIM px/s,
+    seconds, replicas, cores."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    cores = min(os.cpu_count() or 1, n_replicas)
+    with ProcessPoolExecutor(max_workers=cores, mp_context=mp.get_context("spawn")) as ex:
+        list(ex.map(_flim_cpu_replica, [(n_replicas, seed, -1)] * cores))
+        t0 = time.perf_counter()
+        px = sum(ex.map(_flim_cpu_replica, [(n_replicas, seed, r) for r in range(n_replicas)]))
+        dt = time.perf_counter() - t0
+    return px / dt, dt, n_replicas, cores
 
 
 def large_membrane_bench(device: int, stream) -> dict:
@@ -500,21 +516,48 @@ def main():
     h2d = state_bytes_in / STEPS_PER_FRAME
     d2h = (flim_elems * 4 + state_bytes_out) / STEPS_PER_FRAME
 
-    # ---- per-kernel-group timing (CUDA events, eager) -----------------------
+    # ---- per-kernel timing (CUDA events inside a captured graph) -------------
     prof = eng.profile_steps(20, True, stream=stream)
+    passes = eng.profile_passes(10, stream=stream)  # reaction passes one by one (eager, for the breakdown)
     N = ens.total_particles
-    alg = {  # algorithmic bytes per particle of each group (float32 path)
-        "scatter": 2 * (8 + 4 + 1 + 4) + 4,   # read + write slot record, inverse map
-        "move": (8 + 4 + 1 + 4) + (8 + 4),     # read pre-move slot, write post-move position/cell
-    }
+    n_buckets = int(sum(p.nx * p.ny + 1 for p in ens.dyn_params))
     groups = {k: prof[k] for k in ("cell_scan", "scatter", "move", "reactions", "photophysics", "detection")}
-    dom = max(("scatter", "move"), key=lambda k: groups[k])
+    # Candidate kernels with their algorithmic bytes per launch (float32 path).  Single-kernel
+    # groups are timed inside the graph; the reaction passes eagerly, scaled so that they add up to
+    # the reactions group's in-graph time.
+    cand = {
+        "k_scan (3 launches)": (groups["cell_scan"], 20 * n_buckets, "20 B per sort bucket"),
+        "k_scatter": (groups["scatter"], 38 * N, "38 B per slot: slot record read + written, inverse map"),
+        "k_move": (groups["move"], 29 * N, "29 B per slot: 17 B pre-move slot read, 12 B position + cell written"),
+    }
+    eager_rx = sum(ms for _, _, ms in passes)
+    scale_rx = groups["reactions"] / eager_rx if eager_rx > 0 else 1.0
+    for kind, idx, ms in passes:
+        if kind == "contacts":
+            cand["k_contacts"] = (ms * scale_rx, 22 * N, "22 B per slot: flag sweep + every slot's cell, flags, "
+                                                         "pre- and post-move position read once")
+        elif kind == "pass_draws":
+            cand["k_pass_draws"] = (ms * scale_rx, 1 * N, "1 B per slot: flag sweep")
+    dom = max(cand, key=lambda k: cand[k][0])
+    dom_ms, dom_bytes, dom_def = cand[dom]
     peak, peak_kind = peaks()
-    achieved = alg[dom] * N / (groups[dom] / 1e3) / 1e9
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
     traffic = None
     tr_file = ROOT / "profiles" / "traffic.json"
     if tr_file.exists() and args.replicas == 512 and world == 1:  # the committed figures are for this workload
         traffic = json.loads(tr_file.read_text()).get(dom)
+    step_ms = ms / args.steps / STEPS_PER_FRAME  # device ms per BD step, whole job
+    step_roofline = {
+        "alg_bytes_per_particle_step": 64,
+        "definition": "16 B packed state read + written, cell-sorted copy written + read once per particle-step",
+        "membrane": {"particles": n_mem, "achieved": 64 * n_mem / (step_ms / 1e3) / 1e9,
+                     "frac": 64 * n_mem / (step_ms / 1e3) / 1e9 / peak},
+        "all_slots": {"particles": N, "achieved": 64 * N / (step_ms / 1e3) / 1e9,
+                      "frac": 64 * N / (step_ms / 1e3) / 1e9 / peak},
+        "ms_per_bd_step": step_ms,
+    }
+    kernel_roofline = {k: {"ms": v[0], "alg_bytes": v[1], "frac": v[1] / (v[0] / 1e3) / 1e9 / peak,
+                           "definition": v[2]} for k, v in cand.items()}
 
     # ---- plain float64 path: one 13,000-particle system, per-step launches ---
     fp64 = None
@@ -553,11 +596,13 @@ def main():
         cores = os.cpu_count() or 1
         v, dt, ps, nsteps = oracle_sample_sized([raws[i] for i in order], cores, target_s=10.0)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": f"16 median-size replicas x {nsteps} full BD steps ({ps} particle-steps, {dt:.1f} s)"}
+               "sample": f"16 median-size replicas x {nsteps} full BD steps ({ps} particle-steps, {dt:.1f} s) on "
+                         + PORT_NOTE}
         if flim is not None:
-            fv, fdt, fr = flim_cpu_sample(16, args.seed)
-            flim["cpu_baseline"] = {"value": fv, "unit": "px/s", "cores": 1, "kind": "port",
-                                    "sample": f"{fr} replicas, float64 numpy restatement + numpy Poisson ({fdt:.1f} s)"}
+            fv, fdt, fr, fcores = flim_cpu_sample(16, args.seed)
+            flim["cpu_baseline"] = {"value": fv, "unit": "px/s", "cores": fcores, "kind": "port",
+                                    "sample": f"{fr} replicas, float64 numpy restatement + numpy Poisson ({fdt:.1f} s), "
+                                              "one replica per process; the reference has no batched acquisition"}
 
     if rank == 0:
         line = {
@@ -577,8 +622,12 @@ def main():
                             "ends after the last read), state D2H; bytes are per BD step"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "alg_bytes_per_particle": alg[dom], "alg_bytes": alg[dom] * N, "kernel_ms": groups[dom]},
+                         "alg_bytes": dom_bytes, "alg_bytes_definition": dom_def, "kernel_ms": dom_ms,
+                         "step": step_roofline, "kernels": kernel_roofline},
             "kernel_ms_per_step": groups,
+            "kernel_ms_sum_vs_step": {"sum_of_groups": sum(groups.values()), "graph_ms_per_bd_step": step_ms,
+                                      "profiled_step_ms": prof["step"]},
+            "reaction_passes_eager_ms": [[k, i, m] for k, i, m in passes],
             "large_membrane": large,
             "fp64_plain": None if fp64 is None else {"value": fp64, "unit": UNIT,
                                                      "workload": "13,000-particle system with sine D(x), float64, "

@@ -500,13 +500,54 @@ class SimulationResult:
         ])
 
 
+def subframe_series(rows: np.ndarray, prev_counters: np.ndarray, config: SimulationConfig,
+                    fret_E_cls: np.ndarray) -> dict:
+    """The reference's per-step sub-frame series (pipeline.py:567-642) from
+    census rows recorded on the device, one row per BD step ([n][fields], one
+    replica): event and photon counts are differences of the cumulative
+    counters (prev_counters = the 7 counters before the first row), complexes
+    are alive bonded particles / 2, and the mean FRET efficiency is taken
+    over the alive unbleached carriers of dye 0 -- per donor
+    k tau_D / (1 + k tau_D) by FRET class (fret_E_cls, dye 0's row of the
+    exact table) in proximity mode, E(r/R0) times bound / donors in bond
+    mode."""
+    cum = rows[:, PR.CEN_COUNTERS:PR.CEN_COUNTERS + 7]
+    d = np.diff(np.vstack([np.asarray(prev_counters, dtype=np.int64)[None, :7], cum]), axis=0)
+    n_bound = rows[:, PR.CEN_BOND_ALIVE] // 2
+    out = {"n_complexes": n_bound, "n_bleached": rows[:, PR.CEN_BLEACHED].copy()}
+    for k, name in enumerate(("n_bindings", "n_dissociations", "n_catalytic", "n_recruited", "n_detached",
+                              "n_converted", "total_photons")):
+        out[name] = d[:, k]
+    out["species"] = {sp.name: rows[:, PR.CEN_SPECIES + si].copy() for si, sp in enumerate(config.species)}
+    mean = np.zeros(rows.shape[0])
+    if config.fret_pairs:
+        fp = config.fret_pairs[0]
+        n_don = rows[:, PR.CEN_DONORS]
+        has = n_don > 0
+        if getattr(fp, "fret_mode", "bond") == "proximity":
+            cls = rows[:, PR.CEN_DONOR_CLS:PR.CEN_DONOR_CLS + PR.MAX_FCLASS]
+            tot = (cls * np.asarray(fret_E_cls, dtype=np.float64)[None, :PR.MAX_FCLASS]).sum(axis=1)
+            mean[has] = tot[has] / n_don[has]
+        else:
+            e_const = 1.0 / (1.0 + (fp.intra_complex_distance / fp.R0) ** 6)
+            for k in np.nonzero(has)[0]:
+                nb, nd = int(n_bound[k]), int(n_don[k])
+                mean[k] = e_const * nb / (nb + (nd - nb))
+    out["mean_fret_E"] = mean
+    return out
+
+
 class SimulationPipeline:
     """BD -> photophysics -> microscope -> FLIM frames (pipeline.py:236-738),
     device-resident within each frame."""
 
     def __init__(self, config: SimulationConfig, progress_callback: Optional[Callable] = None,
-                 record_subframe: bool = False, precision: int = 64, device: int = 0, graph_chunk: int = 100):
+                 record_subframe: bool = False, precision: int = 64, device: int = 0, graph_chunk: int = 100,
+                 h5_path: Optional[str] = None):
+        """h5_path: stream every frame to an HDF5 file in the reference's
+        layout (ed_mrdt/io.py) from a host thread while the next frame runs."""
         self.config = config
+        self.h5_path = h5_path
         self.record_subframe = record_subframe
         self.precision = precision
         self.device = device
@@ -543,34 +584,24 @@ class SimulationPipeline:
         self._microscope = VirtualMicroscope(cfg, self._state, precision=self.precision, device=self.device)
 
     def _extract_ground_truth(self) -> GroundTruth:
-        """Exact per-frame state (pipeline.py:357-455)."""
+        """Exact per-frame state (pipeline.py:357-455).  FRET classes, E and
+        tau_DA of every donor, and the bond / bleaching / species / free-donor
+        counts are evaluated on the device (edm_ground_truth); the state
+        arrays are the host copies the frame loop has just synced."""
         st = self._state
         cfg = self.config
-        N = st.N
-        fret_E = np.zeros(N)
-        tau_DA = np.zeros(N)
-        k_arr = self._photon_sim._k_fret if self._photon_sim._active else np.zeros(N)
-        for fp in cfg.fret_pairs:
-            didx = next((i for i, f in enumerate(cfg.fluorophores) if f.name == fp.donor_type), None)
-            if didx is None:
-                continue
-            rm = self._photon_sim.rate_matrices[didx]
-            tauD = rm.lifetime(rm.excited)
-            if tauD <= 0 or math.isinf(tauD):
-                continue
-            sel = st.has_dye & ~st.is_bleached & (st.dye_type_id == didx)
-            kf = k_arr[sel]
-            fret_E[sel] = np.where(kf > 0, kf * tauD / (1.0 + kf * tauD), 0.0)
-            tau_DA[sel] = np.where(kf > 0, tauD / (1.0 + kf * tauD), tauD)
+        eng = st._device_owner.engine
+        fret_E, tau_DA, census = eng.ground_truth()
+        c = census[0]
         n_free = 0
         for fp in cfg.fret_pairs:
             for fi, f in enumerate(cfg.fluorophores):
-                if f.name == fp.donor_type:
-                    n_free += int(np.sum(st.has_dye & (st.dye_type_id == fi) & ~st.is_bleached & (st.bond_partner < 0)))
-        counts = {sp.name: int(np.sum((st.species_id == i) & st.is_alive)) for i, sp in enumerate(cfg.species)}
+                if f.name == fp.donor_type and fi < PR.MAX_FLUO:
+                    n_free += int(c[PR.CEN_FREE_DYE + fi])
+        counts = {sp.name: int(c[PR.CEN_SPECIES + i]) for i, sp in enumerate(cfg.species)}
         return GroundTruth(st.positions.copy(), st.species_id.copy(), st.bond_partner.copy(), st.is_alive.copy(),
                            st.has_dye.copy(), st.dye_type_id.copy(), st.is_bleached.copy(), fret_E, tau_DA,
-                           int(np.sum(st.bond_partner >= 0)) // 2, int(np.sum(st.is_bleached)), n_free, counts)
+                           int(c[PR.CEN_BOND_ALL]) // 2, int(c[PR.CEN_BLEACHED]), n_free, counts)
 
     def run(self) -> SimulationResult:
         t_all = time.perf_counter()
@@ -584,16 +615,23 @@ class SimulationPipeline:
         frames: List[FrameResult] = []
         tot_em = tot_det = 0
         sub = None
-        if self.record_subframe:
-            sub = self._subframe_alloc()
         c_prev = eng.counters()[0].copy()
         sys.ensure_device()
+        if self.record_subframe:
+            sub = self._subframe_alloc()
+            eng.record_enable(self.n_bd_per_frame)
+            sub["prev"] = c_prev[:7].copy()
+        step0 = eng.get_step()
+        writer = None
+        if self.h5_path is not None:
+            from .io import StreamingHDF5Writer
+            writer = StreamingHDF5Writer(self.h5_path, self.config, self._state.N).open()
         for fidx in range(self.n_frames):
             tf = time.perf_counter()
+            eng.pipeline_steps(self.n_bd_per_frame, True, self.graph_chunk, stream=stream)
             if self.record_subframe:
-                self._run_frame_recorded(sub, fidx, stream)
-            else:
-                eng.pipeline_steps(self.n_bd_per_frame, True, self.graph_chunk, stream=stream)
+                rows = eng.record_read(step0 + fidx * self.n_bd_per_frame, self.n_bd_per_frame, stream=stream)
+                self._decode_subframe(sub, rows[:, 0, :])
             stream.synchronize()
             sys.mark_device_newer()
             c_now = eng.counters()[0].copy()
@@ -603,20 +641,29 @@ class SimulationPipeline:
             frame = self._microscope.finalize_frame()
             c_prev = eng.counters()[0].copy()
             sys.sync_host()
-            self._photon_sim.update_fret_rates()
             gt = self._extract_ground_truth()
             bio = (fidx + 1) * self.frame_interval
             wall = time.perf_counter() - tf
             frames.append(FrameResult(fidx, bio, frame, gt, em, det, wall))
+            if writer is not None:
+                writer.write_frame(frames[-1])
             tot_em += em
             tot_det += det
             self._progress(fidx, self.n_frames, f"t={bio:.3f}s | photons={det:,} | counts={frame.total_counts:,} "
                                                 f"| complexes={gt.n_complexes} | bleached={gt.n_bleached} "
                                                 f"| wall={wall:.2f}s")
+        if self.record_subframe:
+            eng.record_enable(0)
+        # the reference leaves PhotonSimulator._k_fret at the last frame's update_fret_rates
+        self._photon_sim.update_fret_rates()
         c = eng.counters()[0]
         res = SimulationResult(self.config, frames, time.perf_counter() - t_all, 0.0, tot_em, tot_det,
                                int(c[PR.C_BINDINGS]), int(c[PR.C_DISSOC]), int(np.sum(self._state.is_bleached)),
                                self._subframe_result(sub) if sub is not None else None)
+        if writer is not None:
+            writer.finalize(total_wall_time=res.total_wall_time_s, peak_ram_mb=res.peak_ram_mb,
+                            total_bindings=res.total_bindings, total_dissociations=res.total_dissociations)
+            writer.close()
         self._dynamics._pull_counters(sys)
         self._progress(self.n_frames - 1, self.n_frames, f"DONE. {res.summary()}")
         return res
@@ -629,51 +676,19 @@ class SimulationPipeline:
                     mean_fret_E=np.zeros(n), species={sp.name: z() for sp in self.config.species},
                     n_catalytic=z(), n_recruited=z(), n_detached=z(), n_converted=z())
 
-    def _run_frame_recorded(self, sub, fidx, stream):
-        sys = self._state._device_owner
-        eng = sys.engine
-        st = self._state
-        prev = eng.counters()[0].copy()
-        for _ in range(self.n_bd_per_frame):
-            eng.pipeline_steps(1, True, 0, stream=stream)
-            stream.synchronize()
-            sys.mark_device_newer()
-            sys.sync_host()
-            c = eng.counters()[0].copy()
-            i = sub["i"]
-            sub["n_complexes"][i] = np.sum(st.bond_partner[st.is_alive] >= 0) // 2
-            sub["n_bindings"][i] = c[PR.C_BINDINGS] - prev[PR.C_BINDINGS]
-            sub["n_dissociations"][i] = c[PR.C_DISSOC] - prev[PR.C_DISSOC]
-            sub["n_bleached"][i] = np.sum(st.is_bleached)
-            sub["total_photons"][i] = c[PR.C_PHOTONS] - prev[PR.C_PHOTONS]
-            for k, name in ((PR.C_CATALYTIC, "n_catalytic"), (PR.C_RECRUITED, "n_recruited"),
-                            (PR.C_DETACHED, "n_detached"), (PR.C_CONVERTED, "n_converted")):
-                sub[name][i] = c[k] - prev[k]
-            sub["mean_fret_E"][i] = self._mean_fret_E(int(sub["n_complexes"][i]))
-            for si, sp in enumerate(self.config.species):
-                sub["species"][sp.name][i] = np.sum((st.species_id == si) & st.is_alive)
-            sub["i"] = i + 1
-            prev = c
-
-    def _mean_fret_E(self, n_bound: int) -> float:
-        """Mean FRET efficiency over the alive unbleached donors (pipeline.py:587-619):
-        per-donor E from k_FRET in proximity mode, E(r/R0) for bound donors in
-        bond mode."""
-        if not self.config.fret_pairs:
-            return 0.0
-        st = self._state
-        fp = self.config.fret_pairs[0]
-        donors = st.has_dye & st.is_alive & ~st.is_bleached & (st.dye_type_id == 0)
-        n_don = int(np.sum(donors))
-        if n_don == 0:
-            return 0.0
-        if getattr(fp, "fret_mode", "bond") == "proximity":
-            self._photon_sim.update_fret_rates()
-            k = self._photon_sim._k_fret[donors]
-            tau_d = self._photon_sim._tau_all[0]
-            return float(np.mean(k * tau_d / (1.0 + k * tau_d)))
-        e_const = 1.0 / (1.0 + (fp.intra_complex_distance / fp.R0) ** 6)
-        return e_const * n_bound / n_don
+    def _decode_subframe(self, sub, rows: np.ndarray) -> None:
+        """Append one frame of census rows to the sub-frame series."""
+        e_cls = np.array(self._state._device_owner.engine._phot[0].fret_E[0][:PR.MAX_FCLASS])
+        series = subframe_series(rows, sub["prev"], self.config, e_cls)
+        sub["prev"] = rows[-1, PR.CEN_COUNTERS:PR.CEN_COUNTERS + 7].copy()
+        sl = slice(sub["i"], sub["i"] + rows.shape[0])
+        for k, v in series.items():
+            if k == "species":
+                for name, arr in v.items():
+                    sub["species"][name][sl] = arr
+            else:
+                sub[k][sl] = v
+        sub["i"] = sl.stop
 
     def _subframe_result(self, sub) -> SubFrameData:
         return SubFrameData(

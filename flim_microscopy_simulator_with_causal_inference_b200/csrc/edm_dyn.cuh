@@ -553,15 +553,19 @@ __device__ __forceinline__ void for_each_force_term(const EdmDynParams& p, const
         dsq = min_image_sq(xi, yi, v.x, v.y, g, dx, dy);
         if (!(dsq < range_sq)) return;
       } else {
+        // float32 range test (with a 1e-4 relative margin) on every
+        // neighbour; the few pairs inside it get their separation in float64
+        // from (cell, offset): the float32 sum below rounds at the ulp of a
+        // cell side, a large fraction of |dx| for nearly coincident pairs
         const float2 oj = ((const float2*)st.pos_pre)[j];
         const float fdx = -(float)dcx * g.sxf + (oi.x - oj.x);
         const float fdy = -(float)dcy * g.syf + (oi.y - oj.y);
         const float fdsq = fdx * fdx + fdy * fdy;
         if (!(fdsq < range_sqf)) return;
-        if (!((double)fdsq < g.cutoff_sq)) return;
-        dx = fdx;
-        dy = fdy;
-        dsq = fdsq;
+        dx = (double)(-dcx) * g.sx + ((double)oi.x - (double)oj.x);
+        dy = (double)(-dcy) * g.sy + ((double)oi.y - (double)oj.y);
+        dsq = dx * dx + dy * dy;
+        if (!(dsq < range_sq)) return;
       }
       const uint8_t fj = st.flags[j];
       if (!fl_alive(fj)) return;
@@ -571,55 +575,33 @@ __device__ __forceinline__ void for_each_force_term(const EdmDynParams& p, const
       const int idj = st.ids[j] - (int)g.poff;
       const uint64_t order = idj < id ? (uint64_t)idj
                                       : ((1ull << 60) | ((uint64_t)ordinal << 32) | (uint64_t)(0xFFFFFFFFu - (uint32_t)idj));
+      // The pair force itself is float64 on both paths: a pair inside force
+      // range is rare (a few per thousand particles at the membrane
+      // densities), and a capped move takes the direction of this force.
       if (p.use_wca) {
         const double eps = p.eps[sp * EDM_MAX_SPECIES + spj];
         if (eps > 0.0) {
-          if constexpr (F64) {
-            const double rcut2 = sig * sig * 1.2599210498948732;
-            if (dsq < rcut2 && dsq >= 1e-30) {
-              const double inv_r2 = 1.0 / dsq;
-              const double s2 = sig * sig * inv_r2;
-              const double s6 = s2 * s2 * s2;
-              const double s12 = s6 * s6;
-              double f = 24.0 * eps * (2.0 * s12 - s6) * inv_r2;
-              const double fmax = 2400.0 * eps / (sig * sig);
-              if (f > fmax) f = fmax;
-              emit(order, f * dx, f * dy);
-            }
-          } else {
-            const float sgf = (float)sig, epf = (float)eps;
-            const float fd = (float)dsq;
-            const float rcut2 = sgf * sgf * 1.2599210498948732f;
-            if (fd < rcut2 && fd >= 1e-30f) {
-              const float inv_r2 = 1.0f / fd;
-              const float s2 = sgf * sgf * inv_r2;
-              const float s6 = s2 * s2 * s2;
-              const float s12 = s6 * s6;
-              float f = 24.0f * epf * (2.0f * s12 - s6) * inv_r2;
-              const float fmax = 2400.0f * epf / (sgf * sgf);
-              if (f > fmax) f = fmax;
-              emit(order, (double)(f * (float)dx), (double)(f * (float)dy));
-            }
+          const double rcut2 = sig * sig * 1.2599210498948732;
+          if (dsq < rcut2 && dsq >= 1e-30) {
+            const double inv_r2 = 1.0 / dsq;
+            const double s2 = sig * sig * inv_r2;
+            const double s6 = s2 * s2 * s2;
+            const double s12 = s6 * s6;
+            double f = 24.0 * eps * (2.0 * s12 - s6) * inv_r2;
+            const double fmax = 2400.0 * eps / (sig * sig);
+            if (f > fmax) f = fmax;
+            emit(order, f * dx, f * dy);
           }
         }
       }
       if (p.use_harmonic) {
         const double k = p.kharm[sp * EDM_MAX_SPECIES + spj];
         if (k > 0.0) {
-          if constexpr (F64) {
-            const double s2 = sig * sig;
-            if (dsq < s2 && dsq >= 1e-30) {
-              const double r = sqrt(dsq);
-              const double f = k * (sig - r) / r;
-              emit(order | (1ull << 62), f * dx, f * dy);
-            }
-          } else {
-            const float sgf = (float)sig, kf = (float)k, fd = (float)dsq;
-            if (fd < sgf * sgf && fd >= 1e-30f) {
-              const float r = sqrtf(fd);
-              const float f = kf * (sgf - r) / r;
-              emit(order | (1ull << 62), (double)(f * (float)dx), (double)(f * (float)dy));
-            }
+          const double s2 = sig * sig;
+          if (dsq < s2 && dsq >= 1e-30) {
+            const double r = sqrt(dsq);
+            const double f = k * (sig - r) / r;
+            emit(order | (1ull << 62), f * dx, f * dy);
           }
         }
       }
@@ -786,23 +768,49 @@ __global__ void __launch_bounds__(kBlock) k_move(const EdmDynParams* __restrict_
     float dxt = (float)gDx * dtf + sn * z0 + Dif * (float)Fx * dtf;
     float dyt = (float)gDy * dtf + sn * z1 + Dif * (float)Fy * dtf;
     const float dr2 = dxt * dxt + dyt * dyt;
-    if ((double)dr2 > p.max_disp_sq) {
-      const float scale = (float)p.max_disp / sqrtf(dr2);
-      dxt *= scale;
-      dyt *= scale;
+    double ddx = (double)dxt, ddy = (double)dyt;
+    if ((double)dr2 > p.max_disp_sq * 0.999) {
+      // at (or within rounding of) the displacement cap the move keeps only
+      // its direction: form and cap it in float64 as dynamics.py:378-385 do
+      ddx = gDx * dt;
+      ddy = gDy * dt;
+      const double sn64 = sqrt(2.0 * Di * dt);
+      ddx += sn64 * (double)z0;
+      ddy += sn64 * (double)z1;
+      ddx += Di * Fx * dt;
+      ddy += Di * Fy * dt;
+      const double d2 = ddx * ddx + ddy * ddy;
+      if (d2 > p.max_disp_sq) {
+        const double scale = p.max_disp / sqrt(d2);
+        ddx *= scale;
+        ddy *= scale;
+      }
     }
     float2 o = ((const float2*)st.pos_pre)[s];
     int cx, cy;
     split_cell(c, g, cx, cy);
-    o.x += dxt;
-    o.y += dyt;
-    // renormalise into [0, cell) and carry the integer cell
-    for (int it = 0; it < 64 && o.x >= g.sxf; ++it) { o.x -= g.sxf; ++cx; }
-    for (int it = 0; it < 64 && o.x < 0.0f; ++it) { o.x += g.sxf; --cx; }
-    for (int it = 0; it < 64 && o.y >= g.syf; ++it) { o.y -= g.syf; ++cy; }
-    for (int it = 0; it < 64 && o.y < 0.0f; ++it) { o.y += g.syf; --cy; }
-    // a tiny negative offset plus the cell side rounds to the cell side: the
-    // point is the next cell's origin (not this cell's, a cell away)
+    // new offset; a move that leaves the cell is renormalised in float64
+    // against the float64 cell side (subtracting the float32 side would
+    // shift the point by their difference at every crossing)
+    const float ox1 = o.x + (float)ddx, oy1 = o.y + (float)ddy;
+    if (ox1 >= 0.0f && ox1 < g.sxf) {
+      o.x = ox1;
+    } else {
+      const double ax = (double)o.x + ddx;
+      const int k = (int)floor(ax / g.sx);
+      cx += k;
+      o.x = (float)(ax - (double)k * g.sx);
+    }
+    if (oy1 >= 0.0f && oy1 < g.syf) {
+      o.y = oy1;
+    } else {
+      const double ay = (double)o.y + ddy;
+      const int k = (int)floor(ay / g.sy);
+      cy += k;
+      o.y = (float)(ay - (double)k * g.sy);
+    }
+    // a remainder within rounding of the cell side rounds to it: the point is
+    // the next cell's origin (not this cell's, a cell away)
     if (o.x >= g.sxf) {
       o.x = 0.0f;
       ++cx;

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "edm_error.h"
+#include "edm_census.cuh"
 #include "edm_phot.cuh"
 
 using namespace edm;
@@ -137,7 +138,13 @@ struct EdmEngine {
   std::vector<int32_t> emit_host;  // emitter list last uploaded
   std::vector<uint8_t> has_dye_host;  // has_dye of the last edm_set_state
   bool cells_valid = false;  // the cell list matches the state (a dynamics step ran since set_state)
-  std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;
+  // captured pipeline chunks, keyed by (steps, with photons, slot parity, recording)
+  std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs;
+  // sub-frame recorder ring [rec_cap][R][EDM_CENSUS_FIELDS] and ground-truth buffers
+  int rec_cap = 0;
+  int64_t* rec_ring = nullptr;
+  int64_t* gt_census = nullptr;
+  double *gt_E = nullptr, *gt_tau = nullptr;
   std::vector<void*> allocs;
 
   DevState dev_state() const {
@@ -468,8 +475,11 @@ struct EdmEngine {
   // optional CUDA events between kernel groups and between reaction passes (profiling only)
   cudaEvent_t* prof = nullptr;
   cudaEvent_t* pass_prof = nullptr;
+  bool prof_capture = false;  // marks become event-record nodes of a graph being captured
   void mark(int k, cudaStream_t s) {
-    if (prof) cudaEventRecord(prof[k], s);
+    if (!prof) return;
+    if (prof_capture) cudaEventRecordWithFlags(prof[k], s, cudaEventRecordExternal);
+    else cudaEventRecord(prof[k], s);
   }
 
   template <bool F64>
@@ -552,6 +562,7 @@ struct EdmEngine {
   int launches_per_step(bool with_photons) const {
     int n = 3 + 1 + 1 + (int)passes.size() + 1;
     if (with_photons) n += (neblk > 0 ? 3 : 1) + 1 + (nphblk > 0 ? 1 : 0) + 1;
+    if (rec_cap > 0) n += 2 + ((has_phot && neblk > 0) ? 1 : 0);
     return n;
   }
 
@@ -586,6 +597,25 @@ struct EdmEngine {
   void enqueue_scope(cudaStream_t s) {
     if (f64) enqueue_scope_t<true>(s);
     else enqueue_scope_t<false>(s);
+  }
+
+  // Census of the state into `base` (ring of `cap` steps, or one block when
+  // cap == 0): counters, bonds, bleaching, species; with photophysics the
+  // donor and free-dye counts (with_cls: donors per FRET class of the step's
+  // photon pass).
+  void enqueue_census(cudaStream_t s, int64_t* base, int cap, bool with_cls) {
+    DevState st = dev_state();
+    PhotState ph = phot_state();
+    const int nrow = R * EDM_CENSUS_FIELDS;
+    k_census_begin<<<(nrow + 255) / 256, 256, 0, s>>>(base, cap, d_step, R, counters);
+    k_census_particles<<<npblk, kBlock, 0, s>>>(dp, pblk, st, has_phot ? bleached : nullptr, base, cap,
+                                               hdp[0].n_species);
+    if (has_phot && neblk > 0) k_census_emitters<<<neblk, kBlock, 0, s>>>(pp, eblk, st, ph, base, cap, with_cls ? 1 : 0);
+  }
+
+  void drop_graphs() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    graphs.clear();
   }
 
   // overlapped frame readout (edm_frame_out_begin / _wait)
@@ -1024,8 +1054,7 @@ int edm_set_state(EdmEngine* E, const EdmHostState* st, void* stream) {
       CUDA_TRY(cudaMemcpyAsync(E->eblk, et.data(), sizeof(int2) * et.size(), cudaMemcpyHostToDevice, s));
     }
     CUDA_TRY(cudaStreamSynchronize(s));  // host vectors above go out of scope
-    for (auto& kv : E->graphs) cudaGraphExecDestroy(kv.second);
-    E->graphs.clear();
+    E->drop_graphs();
   } else {
     CUDA_TRY(cudaStreamSynchronize(s));
   }
@@ -1160,11 +1189,12 @@ int edm_pipeline_steps(EdmEngine* E, int32_t n_steps, int32_t with_photons, int3
       E->enqueue_photons(st);
       E->enqueue_scope(st);
     }
+    if (E->rec_cap > 0) E->enqueue_census(st, E->rec_ring, E->rec_cap, with_photons != 0);
   };
   int done = 0;
   if (graph_chunk > 0 && s != nullptr) {
     while (n_steps - done >= graph_chunk) {
-      const auto key = std::make_tuple(graph_chunk, with_photons ? 1 : 0, E->cur);
+      const auto key = std::make_tuple(graph_chunk, with_photons ? 1 : 0, E->cur, E->rec_cap > 0 ? 1 : 0);
       auto it = E->graphs.find(key);
       if (it == E->graphs.end()) {
         const int cur0 = E->cur;
@@ -1191,42 +1221,72 @@ int edm_pipeline_steps(EdmEngine* E, int32_t n_steps, int32_t with_photons, int3
 int edm_profile_steps(EdmEngine* E, int32_t n_steps, int32_t with_photons, float* ms_out, void* stream) {
   if (!E || n_steps <= 0 || !ms_out) return fail(EDM_EINVAL, "edm_profile_steps: bad argument");
   if (with_photons && !E->has_scope) return fail(EDM_EINVAL, "edm_profile_steps: no photophysics/microscope");
+  if (!stream) return fail(EDM_EINVAL, "edm_profile_steps: needs a non-default stream (the steps are captured)");
   CUDA_TRY(cudaSetDevice(E->device));
   cudaStream_t s = (cudaStream_t)stream;
-  cudaEvent_t ev[7];
-  for (int k = 0; k < 7; ++k) CUDA_TRY(cudaEventCreate(&ev[k]));
-  double acc[EDM_NPROF] = {0, 0, 0, 0, 0, 0, 0};
-  E->prof = ev;
-  for (int i = 0; i < n_steps; ++i) {
-    E->enqueue_dynamics(s);
-    if (with_photons) {
-      E->enqueue_photons(s);
-      cudaEventRecord(ev[5], s);
-      E->enqueue_scope(s);
-      cudaEventRecord(ev[6], s);
+  // Two steps (both parities of the double-buffered slot arrays) are captured
+  // into one graph with event-record nodes between the kernel groups, so the
+  // groups are timed as they run inside the pipeline's graphs.
+  cudaEvent_t ev[2][7];
+  for (int h = 0; h < 2; ++h)
+    for (int k = 0; k < 7; ++k) CUDA_TRY(cudaEventCreate(&ev[h][k]));
+  auto destroy = [&]() {
+    for (int h = 0; h < 2; ++h)
+      for (int k = 0; k < 7; ++k) cudaEventDestroy(ev[h][k]);
+  };
+  const int cur0 = E->cur;
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ge = nullptr;
+  E->prof_capture = true;
+  cudaError_t ce = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+  if (ce == cudaSuccess) {
+    for (int h = 0; h < 2; ++h) {
+      E->prof = ev[h];
+      E->enqueue_dynamics(s);
+      if (with_photons) {
+        E->enqueue_photons(s);
+        E->mark(5, s);
+        E->enqueue_scope(s);
+        E->mark(6, s);
+      }
     }
-    cudaError_t e = cudaEventSynchronize(with_photons ? ev[6] : ev[4]);
-    if (e != cudaSuccess) {
-      E->prof = nullptr;
-      return fail(EDM_ECUDA, cudaGetErrorString(e));
-    }
-    float t;
-    for (int k = 0; k < 4; ++k) {
-      cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
-      acc[k] += t;
-    }
-    if (with_photons) {
-      cudaEventElapsedTime(&t, ev[4], ev[5]);
-      acc[4] += t;
-      cudaEventElapsedTime(&t, ev[5], ev[6]);
-      acc[5] += t;
-    }
-    cudaEventElapsedTime(&t, ev[0], with_photons ? ev[6] : ev[4]);
-    acc[6] += t;
+    ce = cudaStreamEndCapture(s, &g);
   }
   E->prof = nullptr;
-  for (int k = 0; k < 7; ++k) cudaEventDestroy(ev[k]);
-  for (int k = 0; k < EDM_NPROF; ++k) ms_out[k] = (float)(acc[k] / n_steps);
+  E->prof_capture = false;
+  E->cur = cur0;  // the capture advanced the parity twice: unchanged
+  if (ce == cudaSuccess) ce = cudaGraphInstantiate(&ge, g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (ce != cudaSuccess) {
+    destroy();
+    return fail(EDM_ECUDA, cudaGetErrorString(ce));
+  }
+  double acc[EDM_NPROF] = {0, 0, 0, 0, 0, 0, 0};
+  const int reps = (n_steps + 1) / 2;
+  for (int i = 0; i < reps; ++i) {
+    ce = cudaGraphLaunch(ge, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess) break;
+    for (int h = 0; h < 2; ++h) {
+      float t;
+      for (int k = 0; k < 4; ++k) {
+        cudaEventElapsedTime(&t, ev[h][k], ev[h][k + 1]);
+        acc[k] += t;
+      }
+      if (with_photons) {
+        cudaEventElapsedTime(&t, ev[h][4], ev[h][5]);
+        acc[4] += t;
+        cudaEventElapsedTime(&t, ev[h][5], ev[h][6]);
+        acc[5] += t;
+      }
+      cudaEventElapsedTime(&t, ev[h][0], with_photons ? ev[h][6] : ev[h][4]);
+      acc[6] += t;
+    }
+  }
+  cudaGraphExecDestroy(ge);
+  destroy();
+  if (ce != cudaSuccess) return fail(EDM_ECUDA, cudaGetErrorString(ce));
+  for (int k = 0; k < EDM_NPROF; ++k) ms_out[k] = (float)(acc[k] / (2.0 * reps));
   return EDM_OK;
 }
 
@@ -1262,6 +1322,75 @@ int edm_profile_passes(EdmEngine* E, int32_t n_steps, float* ms_out, int32_t* ki
     kinds_out[k] = 100 * (int)E->passes[k].kind + E->passes[k].index;
   }
   return n;
+}
+
+int edm_record_enable(EdmEngine* E, int32_t capacity_steps) {
+  if (!E || capacity_steps < 0) return fail(EDM_EINVAL, "edm_record_enable: bad argument");
+  CUDA_TRY(cudaSetDevice(E->device));
+  if (capacity_steps == E->rec_cap) return EDM_OK;
+  CUDA_TRY(cudaDeviceSynchronize());  // no captured chunk or kernel may still use the old ring
+  E->drop_graphs();
+  if (E->rec_ring) {
+    for (auto& a : E->allocs)
+      if (a == (void*)E->rec_ring) a = nullptr;
+    cudaFree(E->rec_ring);
+    E->rec_ring = nullptr;
+  }
+  E->rec_cap = 0;
+  if (capacity_steps > 0) {
+    int rc = E->alloc(&E->rec_ring, (size_t)capacity_steps * E->R * EDM_CENSUS_FIELDS);
+    if (rc != EDM_OK) return rc;
+    CUDA_TRY(cudaMemset(E->rec_ring, 0, sizeof(int64_t) * (size_t)capacity_steps * E->R * EDM_CENSUS_FIELDS));
+    E->rec_cap = capacity_steps;
+  }
+  return EDM_OK;
+}
+
+int edm_record_read(EdmEngine* E, int64_t first_step, int32_t n_steps, int64_t* host_out, void* stream) {
+  if (!E || first_step < 0 || n_steps < 0 || (n_steps > 0 && !host_out))
+    return fail(EDM_EINVAL, "edm_record_read: bad argument");
+  if (n_steps > E->rec_cap) return fail(EDM_EINVAL, "edm_record_read: more steps than the recorder holds");
+  CUDA_TRY(cudaSetDevice(E->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t row = (size_t)E->R * EDM_CENSUS_FIELDS;
+  int done = 0;
+  while (done < n_steps) {  // at most two runs of ring slots
+    const int64_t slot = (first_step + done) % E->rec_cap;
+    const int run = (int)std::min<int64_t>(n_steps - done, E->rec_cap - slot);
+    CUDA_TRY(cudaMemcpyAsync(host_out + done * row, E->rec_ring + slot * row, sizeof(int64_t) * row * run,
+                             cudaMemcpyDeviceToHost, s));
+    done += run;
+  }
+  return EDM_OK;
+}
+
+int edm_ground_truth(EdmEngine* E, double* fret_E, double* tau_DA, int64_t* census, void* stream) {
+  if (!E) return fail(EDM_EINVAL, "edm_ground_truth: null engine");
+  CUDA_TRY(cudaSetDevice(E->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc;
+  if (!E->gt_census) {
+    if ((rc = E->alloc(&E->gt_census, (size_t)E->R * EDM_CENSUS_FIELDS)) != EDM_OK) return rc;
+    if ((rc = E->alloc(&E->gt_E, (size_t)std::max<int64_t>(E->N, 1))) != EDM_OK) return rc;
+    if ((rc = E->alloc(&E->gt_tau, (size_t)std::max<int64_t>(E->N, 1))) != EDM_OK) return rc;
+  }
+  E->enqueue_census(s, E->gt_census, 0, false);
+  CUDA_TRY(cudaMemsetAsync(E->gt_E, 0, sizeof(double) * E->N, s));
+  CUDA_TRY(cudaMemsetAsync(E->gt_tau, 0, sizeof(double) * E->N, s));
+  if (E->has_phot && E->neblk > 0) {
+    const DevState st = E->dev_state();
+    const PhotState ph = E->phot_state();
+    const int cv = E->cells_valid ? 1 : 0;
+    if (E->f64) k_ground_truth<true><<<E->neblk, kBlock, 0, s>>>(E->dp, E->pp, E->eblk, st, ph, cv, E->gt_E, E->gt_tau);
+    else k_ground_truth<false><<<E->neblk, kBlock, 0, s>>>(E->dp, E->pp, E->eblk, st, ph, cv, E->gt_E, E->gt_tau);
+  }
+  CUDA_TRY(cudaGetLastError());
+  if (fret_E) CUDA_TRY(cudaMemcpyAsync(fret_E, E->gt_E, sizeof(double) * E->N, cudaMemcpyDeviceToHost, s));
+  if (tau_DA) CUDA_TRY(cudaMemcpyAsync(tau_DA, E->gt_tau, sizeof(double) * E->N, cudaMemcpyDeviceToHost, s));
+  if (census)
+    CUDA_TRY(cudaMemcpyAsync(census, E->gt_census, sizeof(int64_t) * E->R * EDM_CENSUS_FIELDS,
+                             cudaMemcpyDeviceToHost, s));
+  return EDM_OK;
 }
 
 int edm_launches_per_step(EdmEngine* E, int32_t with_photons) {

@@ -69,38 +69,18 @@ __device__ __forceinline__ int64_t poisson_lcg(double mean, double u_seed, doubl
   return n > 0 ? n : 0;
 }
 
-// Per emitter: FRET class, photon counts, photophysical transition.
+// FRET class of donor-capable particle gid (slot `slot`, dye dt) for the
+// current state (photophysics.py:528-683, 1021-1114): the reference's
+// update_fret_rates visits the bond-mode pairs, then the proximity pairs, and
+// the last pair matching the particle's dye sets its rate.  A bonded donor
+// gets its pair's bound class (acceptor index `acc` unless intramolecular);
+// proximity mode needs an alive donor and sets the high class when an alive
+// target lies within the radius, the low class otherwise.
 template <bool F64>
-__global__ void __launch_bounds__(kBlock) k_phot_count(const EdmDynParams* __restrict__ DP,
-                                                       const EdmPhotParams* __restrict__ PP,
-                                                       const int2* __restrict__ eblk, DevState st, PhotState ph,
-                                                       int cells_valid) {
-  const Tile t = tile_of(eblk);
-  const EdmPhotParams& pp = PP[t.r];
-  const EdmDynParams& p = DP[t.r];
-  const int64_t e = t.s;
-  if (e >= pp.emitter_offset + pp.n_emitters) return;
-  const int gid = ph.emit_id[e];
-  const int lid = gid - (int)p.particle_offset;
-  ph.emit_n[e] = 0;
-  ph.emit_nd[e] = 0;
-  ph.emit_acc[e] = -1;
-  const int64_t slot = st.slot_of_id[gid];
-  const uint8_t f = st.flags[slot];
-  if (!ph.has_dye[gid] || !fl_alive(f) || ph.bleached[gid]) return;
-  const int dt = ph.dye[gid];
-  if (dt < 0 || dt >= pp.n_fluoro) return;
-  const int s0 = pp.ground[dt], s1 = pp.excited[dt], t1 = pp.t1[dt], bl = pp.bl[dt];
-  const int cur = ph.ctmc[gid];
-  int pss;
-  if (cur == s0 || cur == s1) pss = 0;
-  else if (t1 >= 0 && cur == t1) pss = 1;
-  else if (bl >= 0 && cur == bl) {
-    ph.bleached[gid] = 1;
-    return;
-  } else pss = 0;
-  // FRET rates (photophysics.py:528-683, 1021-1114): last matching pair wins
-  int cls = 0, acc = -1;
+__device__ int fret_class(const EdmDynParams& p, const EdmPhotParams& pp, const DevState& st, const PhotState& ph,
+                          int r, int gid, int64_t slot, int dt, bool alive, int cells_valid, int& acc) {
+  int cls = 0;
+  acc = -1;
   for (int b = 0; b < pp.n_fret; ++b) {
     const EdmFret& F = pp.fret[b];
     if (dt != F.donor_fid) continue;
@@ -116,6 +96,7 @@ __global__ void __launch_bounds__(kBlock) k_phot_count(const EdmDynParams* __res
         }
       }
     } else {
+      if (!alive) continue;  // photophysics.py:640
       // Any alive target within the radius, post-move (the reference's
       // all-pairs search, photophysics.py:591-683).  After a dynamics step
       // it goes through that step's cell list: a target within radius R now
@@ -171,12 +152,47 @@ __global__ void __launch_bounds__(kBlock) k_phot_count(const EdmDynParams* __res
         }
       }
       // particles placed after the sort (recruitment, dissociation) are not in the cell list
-      const int nm = min(st.moved_count[t.r], (int)p.n_particles);
+      const int nm = min(st.moved_count[r], (int)p.n_particles);
       for (int k = 0; k < nm && !found; ++k) found = near(st.moved[p.particle_offset + k]);
       cls = found ? F.cls_high : F.cls_low;
       acc = -1;
     }
   }
+  return cls;
+}
+
+// Per emitter: FRET class, photon counts, photophysical transition.
+template <bool F64>
+__global__ void __launch_bounds__(kBlock) k_phot_count(const EdmDynParams* __restrict__ DP,
+                                                       const EdmPhotParams* __restrict__ PP,
+                                                       const int2* __restrict__ eblk, DevState st, PhotState ph,
+                                                       int cells_valid) {
+  const Tile t = tile_of(eblk);
+  const EdmPhotParams& pp = PP[t.r];
+  const EdmDynParams& p = DP[t.r];
+  const int64_t e = t.s;
+  if (e >= pp.emitter_offset + pp.n_emitters) return;
+  const int gid = ph.emit_id[e];
+  const int lid = gid - (int)p.particle_offset;
+  ph.emit_n[e] = 0;
+  ph.emit_nd[e] = 0;
+  ph.emit_acc[e] = -1;
+  const int64_t slot = st.slot_of_id[gid];
+  const uint8_t f = st.flags[slot];
+  if (!ph.has_dye[gid] || !fl_alive(f) || ph.bleached[gid]) return;
+  const int dt = ph.dye[gid];
+  if (dt < 0 || dt >= pp.n_fluoro) return;
+  const int s0 = pp.ground[dt], s1 = pp.excited[dt], t1 = pp.t1[dt], bl = pp.bl[dt];
+  const int cur = ph.ctmc[gid];
+  int pss;
+  if (cur == s0 || cur == s1) pss = 0;
+  else if (t1 >= 0 && cur == t1) pss = 1;
+  else if (bl >= 0 && cur == bl) {
+    ph.bleached[gid] = 1;
+    return;
+  } else pss = 0;
+  int acc = -1;
+  const int cls = fret_class<F64>(p, pp, st, ph, t.r, gid, slot, dt, true, cells_valid, acc);
   const int64_t key = *ph.d_pstep;
   const double up = uniform1(p.seed, key, EDM_S_PH_POISSON, (uint64_t)lid, 0);
   const double ut = uniform1(p.seed, key, EDM_S_PH_TRANS, (uint64_t)lid, 0);

@@ -72,6 +72,9 @@ def load_library():
     L.edm_profile_steps.argtypes = [vp, i32, i32, vp, vp]
     L.edm_profile_passes.argtypes = [vp, i32, vp, vp, i32, vp]
     L.edm_launches_per_step.argtypes = [vp, i32]
+    L.edm_record_enable.argtypes = [vp, i32]
+    L.edm_record_read.argtypes = [vp, i64, i32, vp, vp]
+    L.edm_ground_truth.argtypes = [vp, vp, vp, vp, vp]
     L.edm_cell_list_static.argtypes = [vp, i64, C.c_double, C.c_double, i32, i32, vp, vp, vp]
     L.edm_readout_lifetimes.argtypes = [vp, i64, i32, C.c_double, i32, i32, i32, vp, vp]
     L.edm_flim_stack_ptr.argtypes = [vp, i32, C.POINTER(vp), C.POINTER(i64), C.POINTER(i32)]
@@ -233,6 +236,44 @@ class Engine:
         n_pass = _check(self.L.edm_profile_passes(self.handle, int(n), _ptr(out), _ptr(kinds), cap,
                                                   _stream_handle(stream)), "edm_profile_passes")
         return [(self.PASS_KINDS[kinds[k] // 100], int(kinds[k] % 100), float(out[k])) for k in range(n_pass)]
+
+    # ---- census: sub-frame recorder and per-frame ground truth --------------
+    def record_enable(self, capacity_steps: int) -> None:
+        """Record every later pipeline step's census rows into a device ring
+        of `capacity_steps` steps (0 stops recording)."""
+        _check(self.L.edm_record_enable(self.handle, int(capacity_steps)), "edm_record_enable")
+
+    def record_read(self, first_step: int, n_steps: int, stream=None, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Census rows [n_steps][R][CENSUS_FIELDS] of steps first_step .. +n_steps."""
+        shape = (int(n_steps), self.R, PR.CENSUS_FIELDS)
+        if out is None:
+            out = np.empty(shape, dtype=np.int64)
+        elif out.shape != shape or out.dtype != np.int64 or not out.flags.c_contiguous:
+            raise ValueError(f"record_read: out must be a contiguous int64 array of shape {shape}")
+        _check(self.L.edm_record_read(self.handle, int(first_step), int(n_steps), _ptr(out), _stream_handle(stream)),
+               "edm_record_read")
+        self._sync(stream)
+        return out
+
+    def ground_truth(self, stream=None):
+        """(fret_E[N], tau_DA[N], census[R][CENSUS_FIELDS]) of the current state."""
+        e = np.empty(self.N, dtype=np.float64)
+        tau = np.empty(self.N, dtype=np.float64)
+        cen = np.empty((self.R, PR.CENSUS_FIELDS), dtype=np.int64)
+        _check(self.L.edm_ground_truth(self.handle, _ptr(e), _ptr(tau), _ptr(cen), _stream_handle(stream)),
+               "edm_ground_truth")
+        self._sync(stream)
+        return e, tau, cen
+
+    @staticmethod
+    def _sync(stream):
+        import torch
+        if stream is None:
+            torch.cuda.synchronize()
+        elif hasattr(stream, "synchronize"):
+            stream.synchronize()
+        else:
+            torch.cuda.ExternalStream(int(stream)).synchronize()
 
     def launches_per_step(self, with_photons: bool = True) -> int:
         return _check(self.L.edm_launches_per_step(self.handle, int(bool(with_photons))), "edm_launches_per_step")

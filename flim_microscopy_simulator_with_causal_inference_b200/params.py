@@ -121,6 +121,11 @@ class EdmFret(C.Structure):
 _T3 = ((C.c_double * MAX_FCLASS) * 2) * MAX_FLUO
 
 
+# census row fields (EdmCensusField of include/edm_b200.h)
+CEN_COUNTERS, CEN_BOND_ALIVE, CEN_BOND_ALL, CEN_BLEACHED, CEN_SPECIES = 0, 7, 8, 9, 10
+CEN_DONORS, CEN_DONOR_CLS, CEN_FREE_DYE, CENSUS_FIELDS = 26, 27, 35, 40
+
+
 class EdmPhotParams(C.Structure):
     _fields_ = [
         ("n_fluoro", C.c_int32), ("n_fret", C.c_int32),
@@ -129,6 +134,8 @@ class EdmPhotParams(C.Structure):
         ("mean_d", _T3), ("mean_f", _T3), ("exp_neg_d", _T3), ("exp_neg_f", _T3),
         ("T00", _T3), ("T0001", _T3),
         ("tau", (C.c_double * MAX_FCLASS) * MAX_FLUO),
+        ("fret_E", (C.c_double * MAX_FCLASS) * MAX_FLUO),
+        ("gt_donor", C.c_int32 * MAX_FLUO),
         ("tau_all", C.c_double * MAX_FLUO),
         ("has_fret_cls", C.c_int32 * MAX_FCLASS),
         ("fret", EdmFret * MAX_FRET),
@@ -876,8 +883,11 @@ def build_phot_params(config: SimulationConfig, n_particles: int, n_labeled: int
             if k > 0.0:
                 tauD = d.tau_all[t]
                 P.tau[t][c] = tauD / (1.0 + k * tauD)
+                # ground truth E (pipeline.py:414); tau_DA above is pipeline.py:415
+                P.fret_E[t][c] = k * tauD / (1.0 + k * tauD)
             else:
                 P.tau[t][c] = d.tau_all[t]
+                P.fret_E[t][c] = 0.0
             for pss in range(2):
                 if k > 0.0:
                     kb = d.k_fret_bound[t]
@@ -896,6 +906,11 @@ def build_phot_params(config: SimulationConfig, n_particles: int, n_labeled: int
                 P.T00[t][pss][c], P.T0001[t][pss][c] = t00, t00 + t01
     for c, k in enumerate(ks):
         P.has_fret_cls[c] = int(k > 0.0)
+    # donors of a FRET pair with a usable lifetime get ground-truth E / tau_DA (pipeline.py:385-398)
+    for fp in config.fret_pairs:
+        fi = next((i for i, f in enumerate(config.fluorophores) if f.name == fp.donor_type), None)
+        if fi is not None and fi < d.n_fluoro and 0.0 < d.tau_all[fi] < math.inf:
+            P.gt_donor[fi] = 1
     P.donor_channel, P.acceptor_channel = d.donor_channel, d.acceptor_channel
     P.max_photons, P.est_photons = d.max_photons, d.est_photons
     P.photon_offset, P.emitter_offset, P.n_emitters = photon_offset, emitter_offset, n_emitters

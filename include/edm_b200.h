@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define EDM_ABI_VERSION 2
+#define EDM_ABI_VERSION 3
 
 /* ---- fixed capacities of the parameter blocks --------------------------- */
 #define EDM_MAX_SPECIES 16
@@ -193,6 +193,12 @@ typedef struct {
   double T00[EDM_MAX_FLUO][2][EDM_MAX_FCLASS];
   double T0001[EDM_MAX_FLUO][2][EDM_MAX_FCLASS];      /* T00 + T01          */
   double tau[EDM_MAX_FLUO][EDM_MAX_FCLASS];           /* tau_DA per class   */
+  /* exact FRET efficiency k tau_D / (1 + k tau_D) per class (0 without
+   * FRET), pipeline.py:410-416 */
+  double fret_E[EDM_MAX_FLUO][EDM_MAX_FCLASS];
+  /* 1 when the fluorophore is the donor of some FRET pair with a finite
+   * positive lifetime: its particles get ground-truth E and tau_DA */
+  int32_t gt_donor[EDM_MAX_FLUO];
   double tau_all[EDM_MAX_FLUO];
   int32_t has_fret_cls[EDM_MAX_FCLASS];               /* k_fret > 0         */
   EdmFret fret[EDM_MAX_FRET];
@@ -328,14 +334,60 @@ int edm_frame_out_begin(EdmEngine* eng, uint32_t* host_out, int64_t n_elems,
                         void* stream);
 int edm_frame_out_wait(EdmEngine* eng);
 
+/* ---- census rows: sub-frame series and per-frame ground truth -------------
+ * One row of EDM_CENSUS_FIELDS int64 per replica holds what the reference's
+ * SimulationPipeline reads off the host state after every BD step
+ * (pipeline.py:567-642, record_subframe=True) and at every frame end
+ * (pipeline.py:399-442, _extract_ground_truth), reduced on the device. */
+enum EdmCensusField {
+  EDM_CEN_COUNTERS = 0,      /* [0, 7): counters EDM_C_BINDINGS .. EDM_C_PHOTONS (cumulative) */
+  EDM_CEN_BOND_ALIVE = 7,    /* alive particles with a bond partner                            */
+  EDM_CEN_BOND_ALL = 8,      /* particles with a bond partner                                  */
+  EDM_CEN_BLEACHED = 9,      /* bleached particles                                             */
+  EDM_CEN_SPECIES = 10,      /* [10, 26): alive particles per species                          */
+  EDM_CEN_DONORS = 26,       /* alive unbleached particles carrying dye 0 (pipeline.py:596-598) */
+  EDM_CEN_DONOR_CLS = 27,    /* [27, 35): those per FRET class of the step's photon pass       */
+  EDM_CEN_FREE_DYE = 35,     /* [35, 39): unbleached particles with dye t and no bond partner  */
+  EDM_CENSUS_FIELDS = 40
+};
+
+/* Sub-frame recorder.  With capacity_steps > 0, every later
+ * edm_pipeline_steps step (eager or inside its CUDA graphs) ends with two
+ * kernels that write the step's census row of every replica into a device
+ * ring of capacity_steps x n_replicas rows: step s (0-based BD step index)
+ * goes to ring slot s % capacity_steps.  capacity_steps = 0 stops recording
+ * and frees the ring.  Changing it drops the engine's captured graphs.
+ * Replaces the per-step host reductions of pipeline.py:567-642. */
+int edm_record_enable(EdmEngine* eng, int32_t capacity_steps);
+/* Copies the rows of steps [first_step, first_step + n_steps) to
+ * host_out[n_steps][n_replicas][EDM_CENSUS_FIELDS] (host memory; pinned
+ * memory makes the copy asynchronous on `stream`).  The steps must be among
+ * the last capacity_steps recorded. */
+int edm_record_read(EdmEngine* eng, int64_t first_step, int32_t n_steps,
+                    int64_t* host_out, void* stream);
+/* Per-frame ground truth (pipeline.py:357-455 after
+ * PhotonSimulator.update_fret_rates, photophysics.py:1021-1114): every
+ * particle's FRET class is evaluated for the current state as the reference's
+ * update_fret_rates does (bond and proximity pairs, last matching pair
+ * wins), and donors get E = k tau_D / (1 + k tau_D) and tau_DA =
+ * tau_D / (1 + k tau_D) (others 0).  Writes fret_E[N] and tau_DA[N] (id
+ * order, replicas concatenated) and census[n_replicas][EDM_CENSUS_FIELDS]
+ * (counters, bonds, bleaching, species and free-donor counts) to host
+ * memory on `stream`; any pointer may be NULL. */
+int edm_ground_truth(EdmEngine* eng, double* fret_E, double* tau_DA,
+                     int64_t* census, void* stream);
+
 /* Counters [n_replicas][EDM_NCOUNTERS] and the sticky status word. */
 int edm_get_counters(EdmEngine* eng, int64_t* out, void* stream);
 int edm_get_status(EdmEngine* eng, uint32_t* status, void* stream);
 
-/* Instrumented eager steps: runs n_steps pipeline steps with CUDA events
- * around each kernel group and writes the mean device time per step (ms) of
- * ms_out[EDM_NPROF]: cell-list scan, scatter, force+move, reaction passes,
- * photophysics, photon detection, whole step.  No reference counterpart. */
+/* Instrumented steps: captures two pipeline steps into a CUDA graph with
+ * event-record nodes around each kernel group, replays it until n_steps
+ * steps (rounded up to even) have run, and writes the mean device time per
+ * step (ms) of ms_out[EDM_NPROF]: cell-list scan, scatter, force+move,
+ * reaction passes, photophysics, photon detection, whole step.  The groups
+ * are timed as they run inside the pipeline's graphs; the stream must not be
+ * the legacy default stream.  No reference counterpart. */
 #define EDM_NPROF 7
 int edm_profile_steps(EdmEngine* eng, int32_t n_steps, int32_t with_photons,
                       float* ms_out, void* stream);
@@ -368,18 +420,22 @@ int edm_get_cells(EdmEngine* eng, int32_t replica, int32_t* cell_start,
  * already handed to another allocator, or a tight loop where cudaMalloc (which
  * may synchronise the device) is not acceptable.
  *
- * Builds the reference's cell list (CellList with cell = L/n, cx = int(x/cell)
- * clamped, key cx*ny + cy) of n caller-owned device positions [n][2]:
- * cell_start_dev[nx*ny + 1] and members_dev[n] (particle indices of cell c in
- * members[cell_start[c] .. cell_start[c+1]), ascending).  It allocates
- * nothing: its scratch is one static device array of
- * EDM_STATIC_MAX_CELLS-sized counters that every GPU loading this library
- * holds until the process exits (about 8 MB).  nx*ny beyond
- * EDM_STATIC_MAX_CELLS is rejected with EDM_EINVAL.  The first call on a
- * device looks up that array's device address (cudaGetSymbolAddress), so
- * make it before any stream capture.  All calls share the one array: calls
- * that overlap on the GPU race; order them on one stream.  Each call clears
- * what must start at zero. */
+ * Builds the cell list of n caller-owned device positions [n][2] (x, y) on
+ * an nx x ny grid over the box [0, Lx) x [0, Ly): cell side = box side /
+ * cells, cx = trunc(x / side_x) and cy = trunc(y / side_y), each clamped into
+ * the grid (so points outside the box land in the edge cells), cell key
+ * cx*ny + cy.  Output: cell_start_dev[nx*ny + 1] and members_dev[n], the
+ * particle indices of cell c in members[cell_start[c] .. cell_start[c+1]),
+ * ascending.  The work is bounded for any occupancy, including every point in
+ * one cell.  It allocates nothing: its scratch is one static device array of
+ * about 8 MB (EDM_STATIC_MAX_CELLS-sized counters) that every GPU loading
+ * this library holds until the process exits.  nx*ny beyond
+ * EDM_STATIC_MAX_CELLS or n beyond EDM_STATIC_MAX_PARTICLES is rejected with
+ * EDM_EINVAL.  The first call on a device looks up that array's device
+ * address (cudaGetSymbolAddress), so make it before any stream capture.  All
+ * calls share the one array: calls that overlap on the GPU race; order them
+ * on one stream.  Each call clears what must start at zero. */
+#define EDM_STATIC_MAX_PARTICLES (1 << 24)
 #define EDM_STATIC_MAX_CELLS (1 << 20)
 int edm_cell_list_static(const double* positions_dev, int64_t n, double Lx,
                          double Ly, int32_t nx, int32_t ny,

@@ -28,7 +28,8 @@ import yaml
 
 from . import oracle as O
 
-REF_ROOT = Path(os.environ.get("EDM_REFERENCE_ROOT", "/root/reference"))
+_ROOT_ENV = os.environ.get("EDM_REFERENCE_ROOT")
+REF_ROOT = Path(_ROOT_ENV) if _ROOT_ENV else None
 
 S_BD_NORMAL, S_BIND, S_DISSOC, S_CAT = 1, 16, 17, 32
 S_EX_ACCEPT, S_EX_POS, S_EX_LOC, S_EX_DETACH, S_EX_OFFSET, S_CONV = 48, 49, 50, 51, 96, 80
@@ -38,13 +39,15 @@ S_SC_DARK, S_SC_DARK_BIN, S_SC_AP, S_SC_AP_BIN = 123, 124, 125, 126
 
 
 def available() -> bool:
-    return (REF_ROOT / "ed_mrdt" / "__init__.py").exists()
+    return REF_ROOT is not None and (REF_ROOT / "ed_mrdt" / "__init__.py").exists()
 
 
 def import_reference():
     """Import the reference package (Numba cache kept outside its tree)."""
+    if REF_ROOT is None:
+        raise RuntimeError("set EDM_REFERENCE_ROOT to the reference source tree (the directory holding ed_mrdt/)")
     if not available():
-        raise RuntimeError("reference source tree not present")
+        raise RuntimeError(f"EDM_REFERENCE_ROOT={REF_ROOT} does not hold the reference package ed_mrdt/")
     os.environ.setdefault("NUMBA_CACHE_DIR", str(Path(tempfile.gettempdir()) / "edm_numba_cache"))
     if str(REF_ROOT) not in sys.path:
         sys.path.insert(0, str(REF_ROOT))

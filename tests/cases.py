@@ -120,3 +120,36 @@ CASES = {
 
 def get(name: str) -> dict:
     return copy.deepcopy(CASES[name]())
+
+
+def jittered_ensemble(n_replicas: int = 8, seed: int = 99, n_min: int = 400, n_max: int = 4000) -> list:
+    """Replicas drawn like the batched ensemble (particle count log-uniform,
+    box scaled to the membrane density, k_cat and K_half each jittered by
+    U(0.5, 1.5), a seed per replica), at sizes the oracle runs in seconds,
+    with the rates raised as in rich_small so that catalysis, recruitment,
+    detachment and conversions fire within tens of steps.  Every replica keeps
+    its own jitter on top of the common scaling."""
+    out = []
+    for d in W.ensemble_replicas(n_replicas, seed=seed, n_min=n_min, n_max=n_max, pixels=16):
+        for c in d["catalytic_reactions"]:
+            c["k_cat"] *= 500.0
+        for ex in d["compartment_exchanges"]:
+            ex["k_on"] *= 400.0
+            ex["k_off"] *= 2.0
+            ex["max_recruits_per_step"] = 2
+        for cv in d["unimolecular_conversions"]:
+            cv["rate"] *= 200.0
+        d["laser"]["power"] = 5.0e-4
+        out.append(d)
+    return out
+
+
+def free_diffusion(n_per_species: int = 20000, seed: int = 123) -> dict:
+    """Two species without forces or reactions (D = 1.0 and 0.05 µm^2/s) in a
+    periodic 100x100 µm^2 box at dt = 0.1 ms: the reference's MSD = 4Dt check
+    (tests/test_dynamics.py:130-213), with more particles per species."""
+    return {"name": "free diffusion", "membrane": {"size": [100.0, 100.0], "periodic": [True, True]},
+            "species": [{"name": "A", "diffusion_coefficient": 1.0, "radius": 1.0},
+                        {"name": "B", "diffusion_coefficient": 0.05, "radius": 1.0}],
+            "initial_populations": {"A": n_per_species, "B": n_per_species},
+            "bd_timestep": 1e-4, "simulation_time": 0.1, "random_seed": seed}

@@ -1,7 +1,7 @@
 """Generate tests/golden/flim_acquire.npz from the reference itself.
 
-Run in a container that has the reference source tree (EDM_REFERENCE_ROOT,
-default /root/reference):
+Run where the reference source tree is present, with EDM_REFERENCE_ROOT set to
+it (the directory holding ed_mrdt/):
 
     python tests/golden/make_flim_golden.py
 

@@ -1,7 +1,7 @@
 """Generate the golden fixtures of tests/golden/ from the reference itself.
 
-Run in a container that has the reference source tree (EDM_REFERENCE_ROOT,
-default /root/reference):
+Run where the reference source tree is present, with EDM_REFERENCE_ROOT set to
+it (the directory holding ed_mrdt/):
 
     python tests/golden/make_golden.py [name ...]   (default: every system)
 
@@ -11,10 +11,17 @@ injected (oracle/refshim.py), then one finalize_frame.  Saved per system:
 the reference's derived constants, the state after step 10 and after step
 K, the counters, the last photon batch and the finalized FLIM stack.  The
 CPU tests replay the same steps on the oracle and require bit equality.
+
+Also saved: the per-step series SimulationPipeline.run(record_subframe=True)
+records (pipeline.py:567-642), evaluated here on the reference's state and
+counters after each step with the same expressions ("sf_*"), and the frame's
+ground truth from the reference's own SimulationPipeline._extract_ground_truth
+after PhotonSimulator.update_fret_rates (pipeline.py:653-654, "gt_*").
 """
 from __future__ import annotations
 
 import sys
+import types
 import warnings
 from pathlib import Path
 
@@ -66,16 +73,53 @@ def generate(name: str) -> dict:
         "psf_sigma": np.array([vm.psf.sigma_um[k] for k in sorted(vm.psf.sigma_um)]),
         "psf_range_px": vm.scanner.psf_range_px, "sigma_irf": vm.tcspc.sigma_irf,
     }
+    sf = {k: np.zeros(STEPS, dtype=np.int64) for k in
+          ("n_complexes", "n_bindings", "n_dissociations", "n_bleached", "total_photons", "n_catalytic",
+           "n_recruited", "n_detached", "n_converted")}
+    sf["mean_fret_E"] = np.zeros(STEPS)
+    sf["species"] = np.zeros((STEPS, len(cfg.species)), dtype=np.int64)
+    names = ("n_bindings", "n_dissociations", "n_catalytic", "n_recruited", "n_detached", "n_converted")
+    prev = [getattr(eng, k) for k in names]
     for t in range(STEPS):
         dyn.step()
         batch = ph.evolve(t)
         sc.process(batch, t)
+        # the sub-frame record of pipeline.py:567-642
+        n_bound = int(np.sum(st.bond_partner[st.is_alive] >= 0) // 2)
+        sf["n_complexes"][t] = n_bound
+        cur = [getattr(eng, k) for k in names]
+        for k, a, b in zip(names, cur, prev):
+            sf[k][t] = a - b
+        prev = cur
+        sf["n_bleached"][t] = np.sum(st.is_bleached)
+        sf["total_photons"][t] = batch.n_photons
+        if cfg.fret_pairs:
+            fp = cfg.fret_pairs[0]
+            donors = st.has_dye & st.is_alive & ~st.is_bleached & (st.dye_type_id == 0)
+            n_don = int(np.sum(donors))
+            if getattr(fp, "fret_mode", "bond") == "proximity" and n_don > 0:
+                k = ps._k_fret[donors]
+                tau_d = ps._tau_all[0]
+                sf["mean_fret_E"][t] = float(np.mean(k * tau_d / (1.0 + k * tau_d)))
+            elif getattr(fp, "fret_mode", "bond") != "proximity" and n_don > 0:
+                e_const = 1.0 / (1.0 + (fp.intra_complex_distance / fp.R0) ** 6)
+                sf["mean_fret_E"][t] = e_const * n_bound / (n_bound + (n_don - n_bound))
+        for i in range(len(cfg.species)):
+            sf["species"][t, i] = np.sum((st.species_id == i) & st.is_alive)
         if t + 1 == SNAP:
             out["snap_positions"] = st.positions.copy()
             out["snap_species"] = st.species_id.copy()
             out["snap_alive"] = st.is_alive.copy()
     dyn.restore()
     frame = sc.finalize()
+    from ed_mrdt.pipeline import SimulationPipeline
+    ps.update_fret_rates()
+    gt = SimulationPipeline._extract_ground_truth(types.SimpleNamespace(_state=st, config=cfg, _photon_sim=ps))
+    out.update({f"sf_{k}": v for k, v in sf.items()})
+    out.update({"gt_fret_E": gt.fret_efficiency_exact, "gt_tau_DA": gt.donor_lifetime_exact,
+                "gt_n_complexes": gt.n_complexes, "gt_n_bleached": gt.n_bleached,
+                "gt_n_free_donors": gt.n_free_donors,
+                "gt_species_counts": np.array([gt.species_counts[sp.name] for sp in cfg.species], dtype=np.int64)})
     out.update({
         "final_positions": st.positions.copy(), "final_species": st.species_id.copy(),
         "final_alive": st.is_alive.copy(), "final_bond": st.bond_partner.copy(),

@@ -38,7 +38,7 @@ def test_library_exports_every_declared_symbol(lib):
 
 
 def test_abi_struct_sizes_match(lib):
-    assert lib.edm_abi_version() == 2
+    assert lib.edm_abi_version() == 3
     for which, cls in ((0, PR.EdmDynParams), (1, PR.EdmPhotParams), (2, PR.EdmScopeParams), (3, PR.EdmHostState),
                        (4, PR.EdmFlimParams)):
         assert lib.edm_abi_sizeof(which) == C.sizeof(cls), cls.__name__

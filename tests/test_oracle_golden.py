@@ -111,3 +111,36 @@ def test_hill_table_is_sequential_density_sum():
         rn = ratio ** 2.0
         assert tab[k] == 0.05 + (1.0 - 0.05) * (rn / (1.0 + rn))
         rho += inv_area
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_oracle_subframe_series_and_ground_truth_match_reference(name):
+    """The reference's per-step sub-frame record and frame ground truth
+    (golden sf_* / gt_*, from its own state and _extract_ground_truth) equal
+    the same expressions on the oracle's replay."""
+    from tests import census as CS
+    g = _load(name)
+    cfg, st = _build(name)
+    dp, hill, d = PR.build_dyn_params(cfg, st.N)
+    duty = min(1.0, cfg.scan.dwell_time / cfg.scan.frame_interval)
+    _, pd = PR.build_phot_params(cfg, st.N, int(st.has_dye.sum()), duty)
+    sp, _ = PR.build_scope_params(cfg)
+    orc = O.OracleSimulation(cfg, st, dp, pd, sp, duty)
+    prev = orc.counters[:6].copy()
+    for t in range(24):
+        batch = orc.bd_step()
+        row = CS.subframe_step(orc, cfg, batch[0].size, prev, pd.tau_all[0])
+        prev = orc.counters[:6].copy()
+        for k, v in row.items():
+            if k == "species":
+                assert np.array_equal(v, g["sf_species"][t]), (t, k)
+            else:
+                assert v == g[f"sf_{k}"][t], (t, k, v, g[f"sf_{k}"][t])
+    orc.finalize_frame()
+    gt = CS.ground_truth(orc, cfg, pd)
+    assert np.array_equal(gt["fret_E"], g["gt_fret_E"])
+    assert np.array_equal(gt["tau_DA"], g["gt_tau_DA"])
+    assert gt["n_complexes"] == int(g["gt_n_complexes"])
+    assert gt["n_bleached"] == int(g["gt_n_bleached"])
+    assert gt["n_free_donors"] == int(g["gt_n_free_donors"])
+    assert np.array_equal(gt["species"], g["gt_species_counts"])
