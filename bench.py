@@ -65,6 +65,7 @@ def parse():
     ap.add_argument("--flim-replicas", type=int, default=256, help="FLIM acquisition replicas (256^2 px each)")
     ap.add_argument("--no-flim", action="store_true")
     ap.add_argument("--no-large", action="store_true", help="skip the 1.3M-particle float32-vs-float64 comparison")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the fixed default launch shapes")
     return ap.parse_args()
 
 
@@ -454,6 +455,11 @@ def main():
     eng = ens.engine
     stream = torch.cuda.Stream(device=device)
     frame = 0
+    # launch shapes: timed on the first real steps of the run (untimed here), then fixed
+    shapes = eng.autotune(3, stream=stream) if not args.no_autotune else eng.launch_shapes()
+    stream.synchronize()
+    ens.upload(stream=stream)  # the timed frames start from the initial state
+    eng.set_step(0)
 
     def run_frame():
         nonlocal frame
@@ -625,6 +631,7 @@ def main():
                          "alg_bytes": dom_bytes, "alg_bytes_definition": dom_def, "kernel_ms": dom_ms,
                          "step": step_roofline, "kernels": kernel_roofline},
             "kernel_ms_per_step": groups,
+            "launch_shapes": shapes,
             "kernel_ms_sum_vs_step": {"sum_of_groups": sum(groups.values()), "graph_ms_per_bd_step": step_ms,
                                       "profiled_step_ms": prof["step"]},
             "reaction_passes_eager_ms": [[k, i, m] for k, i, m in passes],

@@ -482,8 +482,8 @@ __global__ void k_scan_down(int32_t* __restrict__ cnt, int64_t n, const int32_t*
   if (n == 0 && blockIdx.x == 0 && threadIdx.x == 0) start[0] = 0;
 }
 
-template <bool F64>
-__global__ void __launch_bounds__(kBlock) k_scatter(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk,
+template <bool F64, int BS>
+__global__ void __launch_bounds__(BS) k_scatter(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk,
                                                     DevState st) {
   const Tile t = tile_of(blk);
   const EdmDynParams& p = P[t.r];
@@ -660,8 +660,10 @@ __device__ __forceinline__ void dfield(const EdmDynParams& p, int sp, double x, 
   }
 }
 
-template <bool F64>
-__global__ void __launch_bounds__(kBlock) k_move(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk,
+// BS threads per block over tiles of BS slots; MINB resident blocks per SM
+// requested from the register allocator (1 = no constraint).
+template <bool F64, int BS, int MINB>
+__global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk,
                                                  DevState st) {
   const Tile t = tile_of(blk);
   const EdmDynParams& p = P[t.r];
@@ -876,8 +878,8 @@ struct CatLists {
   int n_cat;
 };
 
-template <bool F64>
-__global__ void __launch_bounds__(kBlock, 6) k_contacts(const EdmDynParams* __restrict__ P, DevState st, Match m,
+template <bool F64, int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) k_contacts(const EdmDynParams* __restrict__ P, DevState st, Match m,
                                                      CatLists L) {
   __shared__ int2 buf[kContactSmem];
   __shared__ int nbuf[EDM_MAX_CAT], base[EDM_MAX_CAT];

@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -58,13 +59,36 @@ int dalloc(T** p, size_t n) {
   return EDM_OK;
 }
 
-// Tiles of kBlock items per replica: (replica, first index).
-std::vector<int2> tiles(const std::vector<int64_t>& first, const std::vector<int64_t>& count) {
+// Tiles of bs items per replica: (replica, first index).
+std::vector<int2> tiles(const std::vector<int64_t>& first, const std::vector<int64_t>& count, int bs = kBlock) {
   std::vector<int2> out;
   for (size_t r = 0; r < first.size(); ++r)
-    for (int64_t i = 0; i < count[r]; i += kBlock) out.push_back(make_int2((int)r, (int)(first[r] + i)));
+    for (int64_t i = 0; i < count[r]; i += bs) out.push_back(make_int2((int)r, (int)(first[r] + i)));
   return out;
 }
+
+// ---- launch shapes of the tuned kernels -------------------------------------
+// Candidate (threads per block, minimum resident blocks per SM) of each kernel
+// the autotuner times; candidate 0 is the fixed shape used without tuning.
+struct LaunchShape {
+  int block, min_blocks;
+};
+enum TunedKernel { TK_SCATTER = 0, TK_MOVE = 1, TK_CONTACTS = 2, TK_COUNT = 3 };
+constexpr int kMaxShapes = 6;
+constexpr LaunchShape kShapes[TK_COUNT][kMaxShapes] = {
+    {{256, 1}, {128, 1}, {512, 1}, {0, 0}, {0, 0}, {0, 0}},      // k_scatter
+    {{256, 3}, {256, 4}, {128, 8}, {256, 1}, {512, 1}, {128, 5}},  // k_move
+    {{256, 6}, {256, 4}, {256, 8}, {0, 0}, {0, 0}, {0, 0}},      // k_contacts
+};
+constexpr int kNumShapes[TK_COUNT] = {3, 6, 3};
+const char* const kTunedNames[TK_COUNT] = {"k_scatter", "k_move", "k_contacts"};
+constexpr int kTileSizes[3] = {128, 256, 512};
+int tile_index(int bs) { return bs == 128 ? 0 : (bs == 256 ? 1 : 2); }
+
+// Choices of earlier tunings in this process, by (kernel, precision,
+// replicas, log2 of the slot count): later engines of the same kind reuse them.
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, int> g_tuned;
 
 }  // namespace
 
@@ -83,6 +107,14 @@ struct EdmEngine {
   uint64_t *pass_thr = nullptr, *cat_thr = nullptr;  // draw thresholds ([R][kMaxPP], [R][EDM_MAX_CAT])
   int2 *pblk = nullptr, *eblk = nullptr, *phblk = nullptr, *pxblk = nullptr;
   int npblk = 0, neblk = 0, nphblk = 0, npxblk = 0;
+  // slot tiles of 128, 256 and 512 (the 256 table is pblk) for the tuned kernels
+  int2* pblk_bs[3] = {nullptr, nullptr, nullptr};
+  int npblk_bs[3] = {0, 0, 0};
+  // launch shape of each tuned kernel (index into kShapes), tuning timings
+  int shape[TK_COUNT] = {0, 0, 0};
+  float tuned_ms[TK_COUNT] = {0, 0, 0}, default_ms[TK_COUNT] = {0, 0, 0};
+  int tune_kernel = -1;  // the kernel the autotuner is timing, with its event pair
+  cudaEvent_t tune_ev[2] = {nullptr, nullptr};
   void* pos_pre = nullptr;
   void* pos_post = nullptr;
   int32_t *cell_pre = nullptr, *cell_post = nullptr;
@@ -482,6 +514,48 @@ struct EdmEngine {
     else cudaEventRecord(prof[k], s);
   }
 
+  void tune_mark(int kernel, int k, cudaStream_t s) {
+    if (tune_kernel == kernel) cudaEventRecord(tune_ev[k], s);
+  }
+
+  template <bool F64>
+  void launch_scatter(const DevState& st, cudaStream_t s) {
+    const LaunchShape sh = kShapes[TK_SCATTER][shape[TK_SCATTER]];
+    const int t = tile_index(sh.block);
+    if (npblk_bs[t] == 0) return;
+    switch (sh.block) {
+      case 128: k_scatter<F64, 128><<<npblk_bs[t], 128, 0, s>>>(dp, pblk_bs[t], st); break;
+      case 512: k_scatter<F64, 512><<<npblk_bs[t], 512, 0, s>>>(dp, pblk_bs[t], st); break;
+      default: k_scatter<F64, 256><<<npblk_bs[t], 256, 0, s>>>(dp, pblk_bs[t], st); break;
+    }
+  }
+
+  template <bool F64>
+  void launch_move(const DevState& st, cudaStream_t s) {
+    const int v = shape[TK_MOVE];
+    const int t = tile_index(kShapes[TK_MOVE][v].block);
+    if (npblk_bs[t] == 0) return;
+    const int n = npblk_bs[t];
+    const int2* b = pblk_bs[t];
+    switch (v) {  // the rows of kShapes[TK_MOVE]
+      case 1: k_move<F64, 256, 4><<<n, 256, 0, s>>>(dp, b, st); break;
+      case 2: k_move<F64, 128, 8><<<n, 128, 0, s>>>(dp, b, st); break;
+      case 3: k_move<F64, 256, 1><<<n, 256, 0, s>>>(dp, b, st); break;
+      case 4: k_move<F64, 512, 1><<<n, 512, 0, s>>>(dp, b, st); break;
+      case 5: k_move<F64, 128, 5><<<n, 128, 0, s>>>(dp, b, st); break;
+      default: k_move<F64, 256, 3><<<n, 256, 0, s>>>(dp, b, st); break;
+    }
+  }
+
+  template <bool F64>
+  void launch_contacts(const DevState& st, const Match& m, int grid, cudaStream_t s) {
+    switch (shape[TK_CONTACTS]) {
+      case 1: k_contacts<F64, 4><<<grid, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
+      case 2: k_contacts<F64, 8><<<grid, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
+      default: k_contacts<F64, 6><<<grid, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
+    }
+  }
+
   template <bool F64>
   void enqueue_dynamics_t(cudaStream_t s) {
     const int nbs = nb_scan;
@@ -492,14 +566,18 @@ struct EdmEngine {
     mark(1, s);
     cur ^= 1;
     DevState st = dev_state();
-    k_scatter<F64><<<npblk, kBlock, 0, s>>>(dp, pblk, st);
+    tune_mark(TK_SCATTER, 0, s);
+    launch_scatter<F64>(st, s);
+    tune_mark(TK_SCATTER, 1, s);
     if (n_grid > 0) {
       cudaMemsetAsync(grid_cnt, 0, sizeof(int32_t) * n_grid, s);
       cudaMemsetAsync(grid_delta, 0, sizeof(int32_t) * n_grid, s);
     }
     cudaMemsetAsync(moved_count, 0, sizeof(int32_t) * R, s);
     mark(2, s);
-    k_move<F64><<<npblk, kBlock, 0, s>>>(dp, pblk, st);
+    tune_mark(TK_MOVE, 0, s);
+    launch_move<F64>(st, s);
+    tune_mark(TK_MOVE, 1, s);
     mark(3, s);
     const int rb = (R + 127) / 128;
     const int sgrid = (int)std::max<int64_t>(1, (N / 4 + kBlock) / kBlock);  // 4 slots per thread
@@ -515,7 +593,9 @@ struct EdmEngine {
         case P_DISSOC: k_dissociate<F64><<<sgrid, kBlock, 0, s>>>(dp, st, ps.match, ps.index); break;
         case P_CONTACTS:
           cudaMemsetAsync(contact_count, 0, sizeof(int32_t) * EDM_MAX_CAT, s);
-          k_contacts<F64><<<sgrid, kBlock, 0, s>>>(dp, st, ps.match, cat_lists);
+          tune_mark(TK_CONTACTS, 0, s);
+          launch_contacts<F64>(st, ps.match, sgrid, s);
+          tune_mark(TK_CONTACTS, 1, s);
           break;
         case P_CAT: k_catalytic<F64><<<cgrid, kBlock, 0, s>>>(dp, st, ps.index); break;
         case P_REC_APPLY:
@@ -613,6 +693,12 @@ struct EdmEngine {
     if (has_phot && neblk > 0) k_census_emitters<<<neblk, kBlock, 0, s>>>(pp, eblk, st, ph, base, cap, with_cls ? 1 : 0);
   }
 
+  std::tuple<int, int, int, int> tune_key(int kernel) const {
+    int lg = 0;
+    while ((int64_t(1) << (lg + 1)) <= N) ++lg;
+    return std::make_tuple(kernel, precision, R, lg);
+  }
+
   void drop_graphs() {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     graphs.clear();
@@ -625,6 +711,8 @@ struct EdmEngine {
   bool read_pending = false;
 
   ~EdmEngine() {
+    for (auto& ev : tune_ev)
+      if (ev) cudaEventDestroy(ev);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
     if (side_stream) cudaStreamDestroy(side_stream);
@@ -857,10 +945,22 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
     ALLOC(E->chunk_rep, cr.size());
     CUDA_TRY(cudaMemcpy(E->chunk_rep, cr.data(), sizeof(int32_t) * cr.size(), cudaMemcpyHostToDevice));
   }
-  std::vector<int2> pt = tiles(pfirst, pcount);
-  E->npblk = (int)pt.size();
-  ALLOC(E->pblk, pt.size());
-  if (!pt.empty()) CUDA_TRY(cudaMemcpy(E->pblk, pt.data(), sizeof(int2) * pt.size(), cudaMemcpyHostToDevice));
+  for (int t = 0; t < 3; ++t) {
+    std::vector<int2> pt = tiles(pfirst, pcount, kTileSizes[t]);
+    E->npblk_bs[t] = (int)pt.size();
+    ALLOC(E->pblk_bs[t], std::max<size_t>(1, pt.size()));
+    if (!pt.empty())
+      CUDA_TRY(cudaMemcpy(E->pblk_bs[t], pt.data(), sizeof(int2) * pt.size(), cudaMemcpyHostToDevice));
+  }
+  E->pblk = E->pblk_bs[1];
+  E->npblk = E->npblk_bs[1];
+  {  // launch shapes chosen by an earlier tuning of an engine of this kind
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    for (int k = 0; k < TK_COUNT; ++k) {
+      auto it = g_tuned.find(E->tune_key(k));
+      if (it != g_tuned.end()) E->shape[k] = it->second;
+    }
+  }
   if (E->has_phot) {
     ALLOC(E->pp, (size_t)n_replicas);
     ALLOC(E->emit_id, np);
@@ -1391,6 +1491,80 @@ int edm_ground_truth(EdmEngine* E, double* fret_E, double* tau_DA, int64_t* cens
     CUDA_TRY(cudaMemcpyAsync(census, E->gt_census, sizeof(int64_t) * E->R * EDM_CENSUS_FIELDS,
                              cudaMemcpyDeviceToHost, s));
   return EDM_OK;
+}
+
+int edm_autotune(EdmEngine* E, int32_t steps_per_shape, int32_t retune, void* stream) {
+  if (!E || steps_per_shape <= 0) return fail(EDM_EINVAL, "edm_autotune: bad argument");
+  CUDA_TRY(cudaSetDevice(E->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  for (int k = 0; k < 2; ++k)
+    if (!E->tune_ev[k]) CUDA_TRY(cudaEventCreate(&E->tune_ev[k]));
+  bool has_contacts = false;
+  for (const Pass& ps : E->passes) has_contacts |= ps.kind == P_CONTACTS;
+  cudaError_t ce = cudaSuccess;
+  for (int k = 0; k < TK_COUNT && ce == cudaSuccess; ++k) {
+    if (E->npblk == 0 || (k == TK_CONTACTS && !has_contacts)) continue;
+    const auto key = E->tune_key(k);
+    if (!retune) {
+      std::lock_guard<std::mutex> lock(g_tune_mu);
+      auto it = g_tuned.find(key);
+      if (it != g_tuned.end()) {
+        E->shape[k] = it->second;
+        continue;
+      }
+    }
+    // Each candidate runs real steps (every shape computes the same state),
+    // one untimed, then steps_per_shape timed around the kernel alone.
+    double best = 1e30;
+    int best_v = 0;
+    for (int v = 0; v < kNumShapes[k] && ce == cudaSuccess; ++v) {
+      E->shape[k] = v;
+      E->tune_kernel = -1;
+      E->enqueue_dynamics(s);
+      double acc = 0.0;
+      for (int i = 0; i < steps_per_shape && ce == cudaSuccess; ++i) {
+        E->tune_kernel = k;
+        E->enqueue_dynamics(s);
+        E->tune_kernel = -1;
+        ce = cudaEventSynchronize(E->tune_ev[1]);
+        float t = 0.f;
+        if (ce == cudaSuccess) ce = cudaEventElapsedTime(&t, E->tune_ev[0], E->tune_ev[1]);
+        acc += t;
+      }
+      const double ms = acc / steps_per_shape;
+      if (v == 0) E->default_ms[k] = (float)ms;
+      if (ms < best) {
+        best = ms;
+        best_v = v;
+      }
+    }
+    E->shape[k] = best_v;
+    E->tuned_ms[k] = (float)best;
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tuned[key] = best_v;
+  }
+  E->tune_kernel = -1;
+  E->drop_graphs();  // captured chunks hold the previous shapes
+  if (ce != cudaSuccess) return fail(EDM_ECUDA, std::string("edm_autotune: ") + cudaGetErrorString(ce));
+  CUDA_TRY(cudaGetLastError());
+  return EDM_OK;
+}
+
+int edm_launch_shapes(EdmEngine* E, int32_t* shapes, float* ms) {
+  if (!E) return fail(EDM_EINVAL, "edm_launch_shapes: null engine");
+  for (int k = 0; k < TK_COUNT; ++k) {
+    const LaunchShape sh = kShapes[k][E->shape[k]];
+    if (shapes) {
+      shapes[3 * k] = sh.block;
+      shapes[3 * k + 1] = sh.min_blocks;
+      shapes[3 * k + 2] = kNumShapes[k];
+    }
+    if (ms) {
+      ms[2 * k] = E->default_ms[k];
+      ms[2 * k + 1] = E->tuned_ms[k];
+    }
+  }
+  return TK_COUNT;
 }
 
 int edm_launches_per_step(EdmEngine* E, int32_t with_photons) {

@@ -72,6 +72,8 @@ def load_library():
     L.edm_profile_steps.argtypes = [vp, i32, i32, vp, vp]
     L.edm_profile_passes.argtypes = [vp, i32, vp, vp, i32, vp]
     L.edm_launches_per_step.argtypes = [vp, i32]
+    L.edm_autotune.argtypes = [vp, i32, i32, vp]
+    L.edm_launch_shapes.argtypes = [vp, vp, vp]
     L.edm_record_enable.argtypes = [vp, i32]
     L.edm_record_read.argtypes = [vp, i64, i32, vp, vp]
     L.edm_ground_truth.argtypes = [vp, vp, vp, vp, vp]
@@ -236,6 +238,26 @@ class Engine:
         n_pass = _check(self.L.edm_profile_passes(self.handle, int(n), _ptr(out), _ptr(kinds), cap,
                                                   _stream_handle(stream)), "edm_profile_passes")
         return [(self.PASS_KINDS[kinds[k] // 100], int(kinds[k] % 100), float(out[k])) for k in range(n_pass)]
+
+    # ---- launch-shape autotuner ---------------------------------------------
+    TUNED_KERNELS = ("k_scatter", "k_move", "k_contacts")
+
+    def autotune(self, steps_per_shape: int = 3, retune: bool = False, stream=None) -> dict:
+        """Time every candidate launch shape of the tuned kernels on real
+        dynamics steps and keep the fastest (edm_autotune); returns
+        launch_shapes()."""
+        _check(self.L.edm_autotune(self.handle, int(steps_per_shape), int(bool(retune)), _stream_handle(stream)),
+               "edm_autotune")
+        return self.launch_shapes()
+
+    def launch_shapes(self) -> dict:
+        """{kernel: {block, min_blocks_per_sm, candidates, default_ms, tuned_ms}}."""
+        shp = np.zeros((3, 3), dtype=np.int32)
+        ms = np.zeros((3, 2), dtype=np.float32)
+        n = _check(self.L.edm_launch_shapes(self.handle, _ptr(shp), _ptr(ms)), "edm_launch_shapes")
+        return {self.TUNED_KERNELS[k]: {"block": int(shp[k, 0]), "min_blocks_per_sm": int(shp[k, 1]),
+                                        "candidates": int(shp[k, 2]), "default_ms": float(ms[k, 0]),
+                                        "tuned_ms": float(ms[k, 1])} for k in range(n)}
 
     # ---- census: sub-frame recorder and per-frame ground truth --------------
     def record_enable(self, capacity_steps: int) -> None:

@@ -377,6 +377,23 @@ int edm_record_read(EdmEngine* eng, int64_t first_step, int32_t n_steps,
 int edm_ground_truth(EdmEngine* eng, double* fret_E, double* tau_DA,
                      int64_t* census, void* stream);
 
+/* ---- launch-shape autotuner ------------------------------------------------
+ * No reference counterpart.  For each tuned kernel (k_scatter, k_move,
+ * k_contacts, in that order) runs every candidate launch shape (threads per
+ * block, minimum resident blocks per SM, which bounds registers per thread)
+ * for 1 + steps_per_shape eager dynamics steps, times the kernel alone with
+ * CUDA events on `stream` and keeps the fastest.  The steps are real steps:
+ * every shape computes the same state, so tuning is simply the first steps
+ * of a run.  Choices are cached per (kernel, precision, replicas, log2 of the
+ * particle count) for the rest of the process and applied to later engines
+ * of the same kind, unless retune != 0.  Drops the engine's captured graphs. */
+int edm_autotune(EdmEngine* eng, int32_t steps_per_shape, int32_t retune, void* stream);
+/* The launch shape in use per tuned kernel: shapes[k][3] = (threads per block,
+ * minimum blocks per SM, candidates), ms[k][2] = (time of the default shape,
+ * time of the chosen shape) from the last tuning (0 if not tuned).  Either
+ * pointer may be NULL.  Returns the number of tuned kernels (3). */
+int edm_launch_shapes(EdmEngine* eng, int32_t* shapes, float* ms);
+
 /* Counters [n_replicas][EDM_NCOUNTERS] and the sticky status word. */
 int edm_get_counters(EdmEngine* eng, int64_t* out, void* stream);
 int edm_get_status(EdmEngine* eng, uint32_t* status, void* stream);
