@@ -369,6 +369,7 @@ def flim_bench(args, device: int, rank: int, world: int, stream):
     stream.synchronize()
     ro_ms = statistics.mean(rev[2 * k].elapsed_time(rev[2 * k + 1]) for k in range(args.steps))
     ro_bytes = R * 65536 * (256 * 4 + 6 * 8)
+    keep_tau = ro_out[1].view(R, 65536) if world > 1 else None  # mean-arrival-time maps, for the collection
     del ro_out
     proj = [ev[3 * k].elapsed_time(ev[3 * k + 1]) for k in range(args.steps)]
     hist = [ev[3 * k + 1].elapsed_time(ev[3 * k + 2]) for k in range(args.steps)]
@@ -424,6 +425,7 @@ def flim_bench(args, device: int, rank: int, world: int, stream):
                                  "traffic": ro_traffic, "alg_bytes_per_px": 256 * 4 + 6 * 8}},
         "gpu_launches": 5 * args.steps, "error_word": err, "clocks": clk.summary(),
         "l2": "histograms 17 GB per acquisition >> 126 MB L2",
+        "_tau_maps": keep_tau,
     }
 
 
@@ -594,6 +596,34 @@ def main():
     if not args.no_flim:
         flim = flim_bench(args, device, rank, world, stream)
 
+    # ---- end-of-run collection over ranks (untimed): per-replica counters, ----
+    # lifetime maps and the pooled TCSPC decay of one more frame
+    collect = None
+    tau_maps = flim.pop("_tau_maps", None) if flim is not None else None
+    if world > 1:
+        from flim_microscopy_simulator_with_causal_inference_b200 import gather as G
+        from flim_microscopy_simulator_with_causal_inference_b200 import readouts as RD
+        eng.pipeline_steps(STEPS_PER_FRAME, True, STEPS_PER_FRAME, stream=stream)
+        eng.finalize(frame, stream=stream)
+        stream.synchronize()
+        ptr, _, nb = RD.engine_stack(eng, 0)
+        stacks = G.device_view(ptr, eng.flim_elems(), np.int32).view(-1, nb)  # counts < 2^31
+        decay = torch.sum(stacks, dim=0, dtype=torch.int64)
+        eng.reset_flim(stream=stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+        c0 = time.perf_counter()
+        got = G.collect_ensemble(eng.counters(stream=stream), tau_maps, decay, device="cuda")
+        torch.cuda.synchronize()
+        collect = {"ms": 1e3 * max_over_ranks(time.perf_counter() - c0, world, "cuda"),
+                   "replicas": int(got["counters"].shape[0]),
+                   "tau_map_bytes": int(got["tau_maps"].numel() * 8) if "tau_maps" in got else 0,
+                   "pooled_decay_counts": int(got["decay"].sum().item()),
+                   "note": "NCCL all-gather of per-replica counters and lifetime maps, all-reduce of the pooled "
+                           "decay; outside the timed region"}
+    elif flim is not None:
+        flim.pop("_tau_maps", None)
+
     # ---- CPU baseline (oracle) on a bounded sample ---------------------------
     cpu = None
     if not args.no_cpu_baseline and rank == 0:
@@ -644,6 +674,7 @@ def main():
             "flim": flim,
             "gpu_launches": launches,
             "status_word": status,
+            "collect": collect,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
