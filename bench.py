@@ -538,14 +538,14 @@ def main():
         "k_scatter": (groups["scatter"], 38 * N, "38 B per slot: slot record read + written, inverse map"),
         "k_move": (groups["move"], 29 * N, "29 B per slot: 17 B pre-move slot read, 12 B position + cell written"),
     }
-    eager_rx = sum(ms for _, _, ms in passes)
+    eager_rx = sum(pm for _, _, pm in passes)
     scale_rx = groups["reactions"] / eager_rx if eager_rx > 0 else 1.0
-    for kind, idx, ms in passes:
+    for kind, idx, pm in passes:
         if kind == "contacts":
-            cand["k_contacts"] = (ms * scale_rx, 22 * N, "22 B per slot: flag sweep + every slot's cell, flags, "
+            cand["k_contacts"] = (pm * scale_rx, 22 * N, "22 B per slot: flag sweep + every slot's cell, flags, "
                                                          "pre- and post-move position read once")
         elif kind == "pass_draws":
-            cand["k_pass_draws"] = (ms * scale_rx, 1 * N, "1 B per slot: flag sweep")
+            cand["k_pass_draws"] = (pm * scale_rx, 1 * N, "1 B per slot: flag sweep")
     dom = max(cand, key=lambda k: cand[k][0])
     dom_ms, dom_bytes, dom_def = cand[dom]
     peak, peak_kind = peaks()

@@ -17,10 +17,10 @@
 //      I_free[p] h_free[b] yield_free + I_bound[p] h_bound[b] yield_bound,
 //      h the bin probabilities of an exponential decay convolved with the
 //      Gaussian IRF, negative times folded into bin 0 and times past the last
-//      bin lost (the TCSPC rule of microscope.py:716-803), in float64.  Each
-//      bin's count is drawn as its own Poisson variate.  The expected mean
-//      arrival time of each pixel follows in float64 from its two
-//      intensities and the bin sums.
+//      bin lost (the TCSPC rule of microscope.py:716-803), in float64.  The
+//      counts are drawn as Poisson in-window totals per component followed
+//      by alias-table photons.  The expected mean arrival time of each pixel
+//      follows in float64 from its two intensities and the bin sums.
 // Photon yields and lifetimes are host inputs (the reference's per-pulse
 // chain, photophysics.py:218-331).  This path has no reference counterpart:
 // the reference only has the photon-by-photon microscope (edm_phot.cuh).
@@ -259,10 +259,12 @@ __device__ double exgauss_sf(double t, double tau, double s) {
 // h[c][b] (float64), the sums S_c = sum_b h[c][b] yield_c (expected in-window
 // photons per unit intensity) and T_c = sum_b t_b h[c][b] yield_c with t_b the
 // bin centre, so that a pixel's expected mean arrival time is
-// (A T_free + B T_bound) / (A S_free + B S_bound).  One block of 256 threads.
+// (A T_free + B T_bound) / (A S_free + B S_bound), and the alias tables of
+// h[c][.] / sum h[c][.].  One block of 256 threads.
 __global__ void k_bins(EdmFlimParams p, double* h /*[2][n_bins]*/,
-                       double* sums /*[T_free, S_free, T_bound, S_bound]*/) {
-  __shared__ double ts[256], ss[256];
+                       double* sums /*[T_free, S_free, T_bound, S_bound]*/, int2* alias /*[2][n_bins]*/) {
+  __shared__ double ts[256], ss[256], q[256];
+  __shared__ int small[256], large[256];
   const int b = threadIdx.x;
   const double w = p.bin_width_ns, s = p.sigma_irf_ns;
   for (int c = 0; c < 2; ++c) {
@@ -285,6 +287,32 @@ __global__ void k_bins(EdmFlimParams p, double* h /*[2][n_bins]*/,
       }
       sums[2 * c] = T;
       sums[2 * c + 1] = S;
+      // Alias table of the in-window bin distribution ss[i] / S (Vose's
+      // method, M. D. Vose, IEEE Trans. Softw. Eng. 17 (1991) 972-975):
+      // cell i keeps bin i with probability thr / 2^24, else gives `alias`.
+      const int n = p.n_bins;
+      int ns = 0, nl = 0;
+      for (int i = 0; i < n; ++i) {
+        q[i] = S > 0.0 ? ss[i] / S * n : 1.0;
+        if (q[i] < 1.0) small[ns++] = i;
+        else large[nl++] = i;
+      }
+      int2* tab = alias + c * n;
+      while (ns > 0 && nl > 0) {
+        const int l = small[--ns], g = large[--nl];
+        tab[l] = make_int2((int)fmin(16777216.0, rint(q[l] * 16777216.0)), g);
+        q[g] = (q[g] + q[l]) - 1.0;
+        if (q[g] < 1.0) small[ns++] = g;
+        else large[nl++] = g;
+      }
+      while (nl > 0) {
+        const int g = large[--nl];
+        tab[g] = make_int2(16777216, g);
+      }
+      while (ns > 0) {  // leftovers of rounding: probability one
+        const int l = small[--ns];
+        tab[l] = make_int2(16777216, l);
+      }
     }
     __syncthreads();
   }
@@ -432,45 +460,91 @@ __device__ __forceinline__ uint32_t poisson(float mu, Rng& rng) {
   return mu < 10.0f ? poisson_small(mu, rng.uniform()) : poisson_ptrs(mu, rng);
 }
 
-// A warp takes one pixel at a time (grid-stride over every replica's
-// pixels).  Bin b of the pixel has mean mu_b = A w_free[b] + B w_bound[b]
-// (A, B the pixel's free and bound intensities; w = the float64 exGaussian
-// bin probability times the component's quantum yield), and its count is an
-// independent Poisson(mu_b) draw: the detection model itself, sampled per bin
-// (inversion below a mean of 10, PTRS above) with no per-photon work and no
-// shared-memory histogram.  Lane l draws bins l, l + 32, ...: the decay is
-// smooth over 32 bins, so the lanes of a round take the same sampler branch
-// with similar cost, and every round stores 128 contiguous bytes.  Each
-// lane has its own xoshiro128** stream per (pixel, lane).
+// A warp takes 32 consecutive pixels at a time (grid-stride).  The counts
+// n_b ~ Poisson(mu_b), mu_b = A h_free[b] y_free + B h_bound[b] y_bound, are
+// drawn through the identity "Poisson total, then independent categorical
+// photons":
+//   1. lane l draws, for pixel l of the group, the in-window totals
+//      N_c ~ Poisson(A_c S_c) of both components (stream (pixel, 32)) and
+//      writes its expected mean arrival time;
+//   2. pixel by pixel, the warp places the pixel's N_free + N_bound photons:
+//      each picks its bin from its component's alias table with one 32-bit
+//      word of its lane's stream (stream (pixel, lane)), four per lane per
+//      round so table loads and shared-memory atomics overlap, and the
+//      pixel's histogram leaves in 512-byte coalesced stores.
 __global__ void __launch_bounds__(256, 4) k_hist(EdmFlimParams p, const float* __restrict__ I /*[R][2][256*256]*/,
-                                                 const double* __restrict__ h /*[2][n_bins]*/,
-                                                 const double* __restrict__ sums, uint32_t* __restrict__ hist,
-                                                 double* __restrict__ tau_expected) {
-  __shared__ float w[2][256];
+                                                 const int2* __restrict__ alias, const double* __restrict__ sums,
+                                                 uint32_t* __restrict__ hist, double* __restrict__ tau_expected) {
+  __shared__ int2 tab[2][256];
+  __shared__ __align__(16) uint32_t wh[8][256];
   const int nb = p.n_bins;
-  for (int i = threadIdx.x; i < 2 * nb; i += blockDim.x)
-    w[i / nb][i % nb] = (float)(h[i] * (i < nb ? p.yield_free : p.yield_bound));
+  for (int i = threadIdx.x; i < 2 * nb; i += blockDim.x) tab[i / nb][i % nb] = alias[i];
   __syncthreads();
   const double Tf = sums[0], Sf = sums[1], Tb = sums[2], Sb = sums[3];
-  const int lane = threadIdx.x & 31;
+  const unsigned FULL = 0xffffffffu;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int shift = nb == 256 ? 24 : 25;  // top bits of a word pick the cell
+  uint32_t* h = wh[warp];
   const uint32_t npx = (uint32_t)kDim * kDim;
   const uint32_t total = npx * (uint32_t)p.n_replicas;
-  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
   // pixel index over all replicas: at most 4096 x 2^16 = 2^28, so 32 bits
-  // hold it and the replica / pixel split is a shift and a mask
+  // hold it and the replica / pixel split is a shift and a mask; a group of
+  // 32 aligned pixels never straddles two replicas
   static_assert(kDim * kDim == 1 << 16, "pixel split assumes 2^16 pixels per replica");
-  for (uint32_t g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < total; g += warps) {
-    const uint32_t r = g >> 16, px = g & 0xFFFFu;
-    const float A = I[((size_t)r * 2 + 0) * npx + px];
-    const float B = I[((size_t)r * 2 + 1) * npx + px];
-    if (lane == 0 && tau_expected != nullptr) {
-      const double den = (double)A * Sf + (double)B * Sb;
-      tau_expected[g] = den > 0.0 ? ((double)A * Tf + (double)B * Tb) / den : 0.0;
+  for (uint32_t g0 = (blockIdx.x * 8u + (uint32_t)warp) * 32u; g0 < total; g0 += gridDim.x * 8u * 32u) {
+    const uint32_t r = g0 >> 16;
+    const uint64_t seed = edm_flim_replica_seed(p.seed, (int32_t)r);
+    // ---- 1. this lane's pixel of the group: totals and expected lifetime
+    int n_free = 0, n_all = 0;
+    {
+      const uint32_t gl = g0 + (uint32_t)lane;
+      if (gl < total) {
+        const uint32_t px = gl & 0xFFFFu;
+        const float A = I[((size_t)r * 2 + 0) * npx + px];
+        const float B = I[((size_t)r * 2 + 1) * npx + px];
+        LaneRng trng(seed, r, px, 32u);
+        n_free = (int)poisson(fmaxf(0.0f, A) * (float)Sf, trng);
+        n_all = n_free + (int)poisson(fmaxf(0.0f, B) * (float)Sb, trng);
+        if (tau_expected != nullptr) {
+          const double den = (double)A * Sf + (double)B * Sb;
+          tau_expected[gl] = den > 0.0 ? ((double)A * Tf + (double)B * Tb) / den : 0.0;
+        }
+      }
     }
-    const float a = fmaxf(0.0f, A), b = fmaxf(0.0f, B);
-    LaneRng rng(edm_flim_replica_seed(p.seed, (int32_t)r), r, px, (uint32_t)lane);
-    uint32_t* out = hist + (size_t)g * (size_t)nb;
-    for (int k = lane; k < nb; k += 32) out[k] = poisson(a * w[0][k] + b * w[1][k], rng);
+    // ---- 2. the photons of each pixel of the group
+    const int np = total - g0 < 32u ? (int)(total - g0) : 32;
+    for (int q = 0; q < np; ++q) {
+      const uint32_t gpx = g0 + (uint32_t)q;
+      const uint32_t px = gpx & 0xFFFFu;
+      const int nf = __shfl_sync(FULL, n_free, q), na = __shfl_sync(FULL, n_all, q);
+      {
+        uint4* z = (uint4*)h;
+        for (int i = lane; i < nb / 4; i += 32) z[i] = make_uint4(0u, 0u, 0u, 0u);
+      }
+      __syncwarp();
+      LaneRng rng(seed, r, px, (uint32_t)lane);
+      int i = lane;
+      for (; i + 96 < na; i += 128) {
+        uint32_t w[4];
+        int2 e[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) w[k] = rng.next();
+#pragma unroll
+        for (int k = 0; k < 4; ++k) e[k] = tab[i + 32 * k < nf ? 0 : 1][w[k] >> shift];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          atomicAdd(&h[(int)(w[k] & 0xFFFFFFu) < e[k].x ? (int)(w[k] >> shift) : e[k].y], 1u);
+      }
+      for (; i < na; i += 32) {
+        const uint32_t w = rng.next();
+        const int2 e = tab[i < nf ? 0 : 1][w >> shift];
+        atomicAdd(&h[(int)(w & 0xFFFFFFu) < e.x ? (int)(w >> shift) : e.y], 1u);
+      }
+      __syncwarp();
+      uint4* out = (uint4*)(hist + (size_t)gpx * (size_t)nb);
+      for (int i2 = lane; i2 < nb / 4; i2 += 32) out[i2] = ((const uint4*)h)[i2];
+      __syncwarp();
+    }
   }
 }
 
@@ -510,6 +584,7 @@ struct EdmFlim {
   __nv_bfloat16 *maps = nullptr, *g1 = nullptr, *a2 = nullptr, *b2 = nullptr;
   float* I = nullptr;
   double *h = nullptr, *tau = nullptr, *sums = nullptr;
+  int2* alias = nullptr;
   uint32_t* hist = nullptr;
   uint32_t* err = nullptr;
   CUtensorMap mA1, mB1, mA2, mB2;
@@ -571,6 +646,7 @@ int edm_flim_create(const EdmFlimParams* params, int32_t device, EdmFlim** out) 
   FA(F->I, R * 2 * npx);
   FA(F->h, 2 * (size_t)params->n_bins);
   FA(F->sums, 4);
+  FA(F->alias, 2 * (size_t)params->n_bins);
   FA(F->tau, R * npx);
   FA(F->hist, R * npx * params->n_bins);
   FA(F->err, 1);
@@ -590,7 +666,7 @@ int edm_flim_create(const EdmFlimParams* params, int32_t device, EdmFlim** out) 
     if (e == cudaSuccess) F->hist_blocks = std::max(1, sms * std::max(1, per_sm));
   }
   if (e == cudaSuccess) {
-    k_bins<<<1, 256>>>(*params, F->h, F->sums);
+    k_bins<<<1, 256>>>(*params, F->h, F->sums, F->alias);
     k_band<<<kDim, kDim>>>(*params, F->g1, F->a2);
     e = cudaGetLastError();
   }
@@ -652,8 +728,8 @@ int edm_flim_histograms(EdmFlim* F, int32_t with_tau, void* stream) {
   FL_TRY(cudaSetDevice(F->device));
   const EdmFlimParams& p = F->p;
   const size_t total_px = (size_t)p.n_replicas * kDim * kDim;
-  const unsigned blocks = (unsigned)std::min<size_t>((total_px + 7) / 8, (size_t)F->hist_blocks);  // 8 warps a block
-  k_hist<<<blocks, 256, 0, (cudaStream_t)stream>>>(p, F->I, F->h, F->sums, F->hist, with_tau ? F->tau : nullptr);
+  const unsigned blocks = (unsigned)std::min<size_t>((total_px + 7) / 8, (size_t)F->hist_blocks);
+  k_hist<<<blocks, 256, 0, (cudaStream_t)stream>>>(p, F->I, F->alias, F->sums, F->hist, with_tau ? F->tau : nullptr);
   FL_TRY(cudaGetLastError());
   return EDM_OK;
 }
