@@ -40,6 +40,10 @@ constexpr int kBindCap = 512;
 struct DevState {
   void* pos_pre;      // double2 (f64) or float2 (f32 offsets), slot order, before the move
   void* pos_post;     // same, after the move
+  // f32 path: the float32 remainder of each offset (offset = hi + lo, hi in
+  // pos_*); range tests read hi alone, exact arithmetic reads both
+  float2* lo_pre;
+  float2* lo_post;
   int32_t* cell_pre;  // reference cell of each slot, before the move
   int32_t* cell_post;
   const uint8_t* flags_old;
@@ -190,20 +194,32 @@ __device__ __forceinline__ void split_cell(int c, const Geo& g, int& cx, int& cy
   cy = r;
 }
 
-// Absolute position of a slot (float64).
+// float32 path: a cell offset o (float64) is stored as hi = its float32
+// rounding, clamped into [0, cell side), and lo = the float32 rounding of
+// o - hi, so hi + lo keeps about 48 bits of o.
+__device__ __forceinline__ void split_offset(double o, float side_f, float& hi, float& lo) {
+  float h = (float)o;
+  if (!(h >= 0.0f)) h = 0.0f;
+  else if (h >= side_f) h = __int_as_float(__float_as_int(side_f) - 1);  // largest float below the side
+  hi = h;
+  lo = (float)(o - (double)h);
+}
+
+// Absolute position of a slot (float64); lo is the f32 path's remainder array.
 template <bool F64>
-__device__ __forceinline__ void abs_pos(const void* pos, const int32_t* cell, int64_t s, const Geo& g,
-                                        double& x, double& y) {
+__device__ __forceinline__ void abs_pos(const void* pos, const float2* lo, const int32_t* cell, int64_t s,
+                                        const Geo& g, double& x, double& y) {
   if constexpr (F64) {
     const double2 v = ((const double2*)pos)[s];
     x = v.x;
     y = v.y;
   } else {
     const float2 v = ((const float2*)pos)[s];
+    const float2 l = lo[s];
     int cx, cy;
     split_cell(cell[s], g, cx, cy);
-    x = __dadd_rn(__dmul_rn((double)cx, g.sx), (double)v.x);
-    y = __dadd_rn(__dmul_rn((double)cy, g.sy), (double)v.y);
+    x = __dadd_rn(__dmul_rn((double)cx, g.sx), __dadd_rn((double)v.x, (double)l.x));
+    y = __dadd_rn(__dmul_rn((double)cy, g.sy), __dadd_rn((double)v.y, (double)l.y));
   }
 }
 
@@ -498,6 +514,7 @@ __global__ void __launch_bounds__(BS) k_scatter(const EdmDynParams* __restrict__
     ((double2*)st.pos_pre)[d] = ((const double2*)st.pos_post)[t.s];
   } else {
     ((float2*)st.pos_pre)[d] = ((const float2*)st.pos_post)[t.s];
+    st.lo_pre[d] = st.lo_post[t.s];
   }
   st.cell_pre[d] = c;
   st.flags[d] = f;
@@ -562,8 +579,9 @@ __device__ __forceinline__ void for_each_force_term(const EdmDynParams& p, const
         const float fdy = -(float)dcy * g.syf + (oi.y - oj.y);
         const float fdsq = fdx * fdx + fdy * fdy;
         if (!(fdsq < range_sqf)) return;
-        dx = (double)(-dcx) * g.sx + ((double)oi.x - (double)oj.x);
-        dy = (double)(-dcy) * g.sy + ((double)oi.y - (double)oj.y);
+        const float2 li = st.lo_pre[s], lj = st.lo_pre[j];
+        dx = (double)(-dcx) * g.sx + (((double)oi.x - (double)oj.x) + ((double)li.x - (double)lj.x));
+        dy = (double)(-dcy) * g.sy + (((double)oi.y - (double)oj.y) + ((double)li.y - (double)lj.y));
         dsq = dx * dx + dy * dy;
         if (!(dsq < range_sq)) return;
       }
@@ -677,6 +695,7 @@ __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restric
       ((double2*)st.pos_post)[s] = ((const double2*)st.pos_pre)[s];
     } else {
       ((float2*)st.pos_post)[s] = ((const float2*)st.pos_pre)[s];
+      st.lo_post[s] = st.lo_pre[s];
     }
     st.cell_post[s] = c;
     atomic_inc_aggregated(&st.cnt_next[g.cbase + g.grave]);
@@ -732,7 +751,7 @@ __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restric
   }
 
   double x, y;
-  abs_pos<F64>(st.pos_pre, st.cell_pre, s, g, x, y);
+  abs_pos<F64>(st.pos_pre, st.lo_pre, st.cell_pre, s, g, x, y);
   double Di, gDx, gDy;
   dfield(p, sp, x, y, Di, gDx, gDy);
   const double dt = p.dt;
@@ -788,68 +807,52 @@ __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restric
         ddy *= scale;
       }
     }
-    float2 o = ((const float2*)st.pos_pre)[s];
+    // the new offset in float64 from hi + lo, carried into the next cell
+    // against the float64 cell side, then stored as hi + lo again
+    const float2 oh = ((const float2*)st.pos_pre)[s], ol = st.lo_pre[s];
     int cx, cy;
     split_cell(c, g, cx, cy);
-    // new offset; a move that leaves the cell is renormalised in float64
-    // against the float64 cell side (subtracting the float32 side would
-    // shift the point by their difference at every crossing)
-    const float ox1 = o.x + (float)ddx, oy1 = o.y + (float)ddy;
-    if (ox1 >= 0.0f && ox1 < g.sxf) {
-      o.x = ox1;
-    } else {
-      const double ax = (double)o.x + ddx;
+    double ax = ((double)oh.x + (double)ol.x) + ddx;
+    double ay = ((double)oh.y + (double)ol.y) + ddy;
+    if (!(ax >= 0.0 && ax < g.sx)) {
       const int k = (int)floor(ax / g.sx);
       cx += k;
-      o.x = (float)(ax - (double)k * g.sx);
+      ax -= (double)k * g.sx;
     }
-    if (oy1 >= 0.0f && oy1 < g.syf) {
-      o.y = oy1;
-    } else {
-      const double ay = (double)o.y + ddy;
+    if (!(ay >= 0.0 && ay < g.sy)) {
       const int k = (int)floor(ay / g.sy);
       cy += k;
-      o.y = (float)(ay - (double)k * g.sy);
-    }
-    // a remainder within rounding of the cell side rounds to it: the point is
-    // the next cell's origin (not this cell's, a cell away)
-    if (o.x >= g.sxf) {
-      o.x = 0.0f;
-      ++cx;
-    } else if (o.x < 0.0f) {
-      o.x = 0.0f;
-    }
-    if (o.y >= g.syf) {
-      o.y = 0.0f;
-      ++cy;
-    } else if (o.y < 0.0f) {
-      o.y = 0.0f;
+      ay -= (double)k * g.sy;
     }
     if (g.px) {  // |cx| stays within 64 cells of the box: a few wraps at most
       while (cx >= g.nx) cx -= g.nx;
       while (cx < 0) cx += g.nx;
     } else if (cx < 0 || cx >= g.nx) {  // reflecting wall, in float64
-      double ax = (double)cx * g.sx + (double)o.x;
-      if (ax < 0.0) ax = -ax;
-      else if (ax >= g.Lx) ax = 2.0 * g.Lx - ax;
-      cx = cell_index(ax, g.sx, g.nx);
-      o.x = (float)(ax - (double)cx * g.sx);
+      double bx = (double)cx * g.sx + ax;
+      if (bx < 0.0) bx = -bx;
+      else if (bx >= g.Lx) bx = 2.0 * g.Lx - bx;
+      cx = cell_index(bx, g.sx, g.nx);
+      ax = bx - (double)cx * g.sx;
     }
     if (g.py) {
       while (cy >= g.ny) cy -= g.ny;
       while (cy < 0) cy += g.ny;
     } else if (cy < 0 || cy >= g.ny) {
-      double ay = (double)cy * g.sy + (double)o.y;
-      if (ay < 0.0) ay = -ay;
-      else if (ay >= g.Ly) ay = 2.0 * g.Ly - ay;
-      cy = cell_index(ay, g.sy, g.ny);
-      o.y = (float)(ay - (double)cy * g.sy);
+      double by = (double)cy * g.sy + ay;
+      if (by < 0.0) by = -by;
+      else if (by >= g.Ly) by = 2.0 * g.Ly - by;
+      cy = cell_index(by, g.sy, g.ny);
+      ay = by - (double)cy * g.sy;
     }
-    if (!isfinite(o.x) || !isfinite(o.y)) set_status(st.status, EDM_STATUS_NONFINITE);
+    if (!isfinite(ax) || !isfinite(ay)) set_status(st.status, EDM_STATUS_NONFINITE);
+    float2 o, l;
+    split_offset(ax, g.sxf, o.x, l.x);
+    split_offset(ay, g.syf, o.y, l.y);
     ((float2*)st.pos_post)[s] = o;
+    st.lo_post[s] = l;
     newc = cx * g.ny + cy;
-    x = (double)cx * g.sx + (double)o.x;
-    y = (double)cy * g.sy + (double)o.y;
+    x = (double)cx * g.sx + ax;
+    y = (double)cy * g.sy + ay;
   }
   st.cell_post[s] = newc;
   atomicAdd(&st.cnt_next[g.cbase + newc], 1);  // result unused: a fire-and-forget reduction
@@ -971,7 +974,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_catalytic(const EdmDynParams* __r
     if (m >= st.cat_thr[(int64_t)r * EDM_MAX_CAT + cidx]) continue;
     const double u = __dmul_rn(__ull2double_rn(m), 0x1p-53);
     double xs, ys;
-    abs_pos<F64>(st.pos_post, st.cell_post, es.y, g, xs, ys);
+    abs_pos<F64>(st.pos_post, st.lo_post, st.cell_post, es.y, g, xs, ys);
     double peff = C.prob;
     if (C.rule >= 0) peff = C.prob * rule_factor(p, C.rule, st, xs, ys);
     if (C.rule >= 0 && ((p.adapt_cat_mask >> cidx) & 1)) peff = peff * adapt_factor(p, st.adapt_w, C.rule, xs, ys);
@@ -1080,7 +1083,11 @@ __global__ void k_recruit_apply(const EdmDynParams* __restrict__ P, int n_rep, D
     if constexpr (F64) {
       ((double2*)st.pos_post)[slot] = make_double2(x, y);
     } else {
-      ((float2*)st.pos_post)[slot] = make_float2((float)(x - (double)cxn * g.sx), (float)(y - (double)cyn * g.sy));
+      float2 o, l;
+      split_offset(x - (double)cxn * g.sx, g.sxf, o.x, l.x);
+      split_offset(y - (double)cyn * g.sy, g.syf, o.y, l.y);
+      ((float2*)st.pos_post)[slot] = o;
+      st.lo_post[slot] = l;
     }
     st.cell_post[slot] = newc;
     rebucket(st, g, g.grave, newc);
@@ -1148,7 +1155,7 @@ struct LazyPos {
   bool have = false;
   double x = 0.0, y = 0.0;
   __device__ __forceinline__ void get(const DevState& st, int64_t s, const Geo& g) {
-    if (!have) abs_pos<F64>(st.pos_post, st.cell_post, s, g, x, y);
+    if (!have) abs_pos<F64>(st.pos_post, st.lo_post, st.cell_post, s, g, x, y);
     have = true;
   }
 };
@@ -1329,8 +1336,8 @@ __global__ void k_bind_apply(const EdmDynParams* __restrict__ P, int n_rep, DevS
     if (st.bond[g.poff + a] >= 0 || st.bond[g.poff + bb] >= 0) continue;
     if (fl_species(fa) != B.ra || fl_species(fb) != B.rb) continue;
     double xa, ya, xb, yb;
-    abs_pos<F64>(st.pos_post, st.cell_post, sa, g, xa, ya);
-    abs_pos<F64>(st.pos_post, st.cell_post, sb, g, xb, yb);
+    abs_pos<F64>(st.pos_post, st.lo_post, st.cell_post, sa, g, xa, ya);
+    abs_pos<F64>(st.pos_post, st.lo_post, st.cell_post, sb, g, xb, yb);
     st.flags[sa] = fl_make(B.product, true);
     st.flags[sb] = fl_make(B.rb, false);
     rebucket(st, g, st.cell_post[sb], g.grave);
@@ -1358,7 +1365,7 @@ __global__ void __launch_bounds__(kBlock) k_dissociate(const EdmDynParams* __res
     if (!(u < B.prob_dissoc)) return;
     const int64_t sj = st.slot_of_id[partner];
     double x, y;
-    abs_pos<F64>(st.pos_post, st.cell_post, s, g, x, y);
+    abs_pos<F64>(st.pos_post, st.lo_post, st.cell_post, s, g, x, y);
     const uint8_t fj = st.flags[sj];
     st.flags[s] = fl_make(B.ra, true);
     st.flags[sj] = fl_make(B.rb, true);
@@ -1367,6 +1374,7 @@ __global__ void __launch_bounds__(kBlock) k_dissociate(const EdmDynParams* __res
       ((double2*)st.pos_post)[sj] = ((const double2*)st.pos_post)[s];
     } else {
       ((float2*)st.pos_post)[sj] = ((const float2*)st.pos_post)[s];
+      st.lo_post[sj] = st.lo_post[s];
     }
     rebucket(st, g, fl_alive(fj) ? st.cell_post[sj] : g.grave, newc);
     st.cell_post[sj] = newc;

@@ -117,6 +117,7 @@ struct EdmEngine {
   cudaEvent_t tune_ev[2] = {nullptr, nullptr};
   void* pos_pre = nullptr;
   void* pos_post = nullptr;
+  float2 *lo_pre = nullptr, *lo_post = nullptr;
   int32_t *cell_pre = nullptr, *cell_post = nullptr;
   uint8_t* flags[2] = {nullptr, nullptr};
   int32_t* ids[2] = {nullptr, nullptr};
@@ -183,6 +184,8 @@ struct EdmEngine {
     DevState s;
     s.pos_pre = pos_pre;
     s.pos_post = pos_post;
+    s.lo_pre = lo_pre;
+    s.lo_post = lo_post;
     s.cell_pre = cell_pre;
     s.cell_post = cell_post;
     s.flags_old = flags[cur ^ 1];
@@ -878,6 +881,10 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
   ALLOC(pp1, psz * np);
   E->pos_pre = pp0;
   E->pos_post = pp1;
+  if (!E->f64) {  // float32 remainders of the offsets
+    ALLOC(E->lo_pre, np);
+    ALLOC(E->lo_post, np);
+  }
   ALLOC(E->cell_pre, np);
   ALLOC(E->cell_post, np);
   ALLOC(E->flags[0], np + 4);
@@ -1016,8 +1023,8 @@ namespace {
 
 template <bool F64>
 __global__ void k_set_state(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk, const double* pos,
-                            const int32_t* species, const uint8_t* alive, void* pos_post, int32_t* cell_post,
-                            uint8_t* flags, int32_t* ids, int32_t* slot_of_id, int32_t* cnt) {
+                            const int32_t* species, const uint8_t* alive, void* pos_post, float2* lo_post,
+                            int32_t* cell_post, uint8_t* flags, int32_t* ids, int32_t* slot_of_id, int32_t* cnt) {
   const Tile t = tile_of(blk);
   const EdmDynParams& p = P[t.r];
   const int64_t s = t.s;
@@ -1028,7 +1035,11 @@ __global__ void k_set_state(const EdmDynParams* __restrict__ P, const int2* __re
   if constexpr (F64) {
     ((double2*)pos_post)[s] = make_double2(x, y);
   } else {
-    ((float2*)pos_post)[s] = make_float2((float)(x - (double)cx * g.sx), (float)(y - (double)cy * g.sy));
+    float2 o, l;
+    split_offset(x - (double)cx * g.sx, g.sxf, o.x, l.x);
+    split_offset(y - (double)cy * g.sy, g.syf, o.y, l.y);
+    ((float2*)pos_post)[s] = o;
+    lo_post[s] = l;
   }
   const int c = cx * g.ny + cy;
   cell_post[s] = c;
@@ -1040,7 +1051,7 @@ __global__ void k_set_state(const EdmDynParams* __restrict__ P, const int2* __re
 
 template <bool F64>
 __global__ void k_get_state(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk, const void* pos_post,
-                            const int32_t* cell_post, const uint8_t* flags, const int32_t* slot_of_id,
+                            const float2* lo_post, const int32_t* cell_post, const uint8_t* flags, const int32_t* slot_of_id,
                             const int32_t* bond, double* pos, int32_t* species, uint8_t* alive, int32_t* bond_local) {
   const Tile t = tile_of(blk);
   const EdmDynParams& p = P[t.r];
@@ -1049,7 +1060,7 @@ __global__ void k_get_state(const EdmDynParams* __restrict__ P, const int2* __re
   const Geo g(p);
   const int64_t s = slot_of_id[id];
   double x, y;
-  abs_pos<F64>(pos_post, cell_post, s, g, x, y);
+  abs_pos<F64>(pos_post, lo_post, cell_post, s, g, x, y);
   pos[2 * id] = x;
   pos[2 * id + 1] = y;
   const uint8_t f = flags[s];
@@ -1097,11 +1108,11 @@ int edm_set_state(EdmEngine* E, const EdmHostState* st, void* stream) {
   CUDA_TRY(cudaMemsetAsync(E->cnt, 0, sizeof(int32_t) * (E->n_cells > 0 ? E->n_cells : 1), s));
   if (E->npblk > 0) {
     if (E->f64)
-      k_set_state<true><<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, dpos, E->st_sp, E->st_alive, E->pos_post,
+      k_set_state<true><<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, dpos, E->st_sp, E->st_alive, E->pos_post, E->lo_post,
                                                     E->cell_post, E->flags[E->cur], E->ids[E->cur], E->slot_of_id,
                                                     E->cnt);
     else
-      k_set_state<false><<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, dpos, E->st_sp, E->st_alive, E->pos_post,
+      k_set_state<false><<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, dpos, E->st_sp, E->st_alive, E->pos_post, E->lo_post,
                                                      E->cell_post, E->flags[E->cur], E->ids[E->cur], E->slot_of_id,
                                                      E->cnt);
     k_bond_to_global<<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, E->bond);
@@ -1169,11 +1180,11 @@ int edm_get_state(EdmEngine* E, EdmHostState* st, void* stream) {
   const int64_t N = E->N;
   if (E->npblk > 0) {
     if (E->f64)
-      k_get_state<true><<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, E->pos_post, E->cell_post, E->flags[E->cur],
+      k_get_state<true><<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, E->pos_post, E->lo_post, E->cell_post, E->flags[E->cur],
                                                     E->slot_of_id, E->bond, E->st_pos, E->st_sp, E->st_alive,
                                                     E->st_bond);
     else
-      k_get_state<false><<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, E->pos_post, E->cell_post, E->flags[E->cur],
+      k_get_state<false><<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, E->pos_post, E->lo_post, E->cell_post, E->flags[E->cur],
                                                      E->slot_of_id, E->bond, E->st_pos, E->st_sp, E->st_alive,
                                                      E->st_bond);
   }

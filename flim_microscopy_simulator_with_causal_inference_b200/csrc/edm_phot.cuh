@@ -108,12 +108,12 @@ __device__ int fret_class(const EdmDynParams& p, const EdmPhotParams& pp, const 
       // the replica is tested.
       const Geo g(p);
       double xi, yi;
-      abs_pos<F64>(st.pos_post, st.cell_post, slot, g, xi, yi);
+      abs_pos<F64>(st.pos_post, st.lo_post, st.cell_post, slot, g, xi, yi);
       auto near = [&](int64_t j) {
         const uint8_t fj = st.flags[j];
         if (j == slot || !fl_alive(fj) || fl_species(fj) != F.target_species) return false;
         double xj, yj;
-        abs_pos<F64>(st.pos_post, st.cell_post, j, g, xj, yj);
+        abs_pos<F64>(st.pos_post, st.lo_post, st.cell_post, j, g, xj, yj);
         double dx = xj - xi, dy = yj - yi;
         if (g.px) {
           if (dx > g.Lx / 2.0) dx -= g.Lx;
@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(kBlock) k_scope(const EdmDynParams* __restrict
   const Geo g(p);
   const int64_t slot = st.slot_of_id[g.poff + pid];
   double x, y;
-  abs_pos<F64>(st.pos_post, st.cell_post, slot, g, x, y);
+  abs_pos<F64>(st.pos_post, st.lo_post, st.cell_post, slot, g, x, y);
   int ch = ph.ph_ch[o];
   int chs = ch;
   if (chs < 0) chs = 0;
