@@ -213,6 +213,7 @@ __device__ __forceinline__ int cell_index(double x, double s, int n) {
 // the reference expression evaluated on the device with the exact density.
 __device__ __forceinline__ double hill_of(const EdmRule& R, const double* __restrict__ hill, int k,
                                           uint32_t* status) {
+  if (k < 0) k = 0;  // counts are never negative in a consistent state
   if (k < R.table_len) return hill[R.table_offset + k];
   set_status(status, EDM_STATUS_HILL_RANGE);
   double rho = 0.0;

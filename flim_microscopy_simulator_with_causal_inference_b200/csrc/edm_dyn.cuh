@@ -340,9 +340,20 @@ __device__ __forceinline__ void for_neighbour_slots(const Geo& g, const DevState
 }
 
 // ---- density grids -----------------------------------------------------------
+// int(x / s) as the reference computes it (a rounded float64 quotient,
+// truncated), without the division when it cannot matter: the product x * inv
+// lies within a few ulps of the quotient, so when it is farther than 1e-6
+// from an integer both truncate to the same value; closer than that (about
+// one call in 10^6) the quotient itself is taken.
+__device__ __forceinline__ int grid_index(double x, double s, double inv) {
+  const double q = x * inv;
+  const double f = q - floor(q);
+  return (f > 1e-6 && f < 1.0 - 1e-6) ? (int)q : (int)__ddiv_rn(x, s);
+}
+
 __device__ __forceinline__ int64_t grid_cell_of(const EdmGrid& G, double x, double y) {
-  const int gx = clampi((int)__ddiv_rn(x, G.sx), G.nx);
-  const int gy = clampi((int)__ddiv_rn(y, G.sy), G.ny);
+  const int gx = clampi(grid_index(x, G.sx, G.inv_sx), G.nx);
+  const int gy = clampi(grid_index(y, G.sy, G.inv_sy), G.ny);
   return G.offset + (int64_t)gx * G.ny + gy;
 }
 
@@ -362,8 +373,8 @@ __device__ __forceinline__ double kfold_density(int k, double inv_area) {
 __device__ __forceinline__ double adapt_factor(const EdmDynParams& p, const double* __restrict__ w_all, int rule,
                                                double x, double y) {
   const EdmGrid& G = p.grid[p.rule[rule].grid];
-  const int gx = clampi((int)__ddiv_rn(x, G.sx), G.nx);
-  const int gy = clampi((int)__ddiv_rn(y, G.sy), G.ny);
+  const int gx = clampi(grid_index(x, G.sx, G.inv_sx), G.nx);
+  const int gy = clampi(grid_index(y, G.sy, G.inv_sy), G.ny);
   double w = 0.0;
   if (p.adapt_grid >= 0) {
     const EdmGrid& A = p.grid[p.adapt_grid];
@@ -462,7 +473,18 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int& total) {
   return base + x - v;
 }
 
-__global__ void k_scan_reduce(const int32_t* __restrict__ cnt, int64_t n, int32_t* __restrict__ bsum) {
+// Buffers the step clears before its kernels use them (density grids and
+// their deltas, the placed-after-sort and contact counters, the draw list
+// length): cleared by the first scan kernel instead of one memset each.
+struct StepZero {
+  int32_t* p[5];
+  int64_t n[5];
+};
+
+__global__ void k_scan_reduce(const int32_t* __restrict__ cnt, int64_t n, int32_t* __restrict__ bsum, StepZero z) {
+  for (int k = 0; k < 5; ++k)
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < z.n[k]; i += (int64_t)gridDim.x * blockDim.x)
+      z.p[k][i] = 0;
   const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
   const int4 c = load4(cnt, base, n);
   const int v = c.x + c.y + c.z + c.w;
@@ -558,7 +580,7 @@ __device__ __forceinline__ void for_each_force_term(const EdmDynParams& p, const
     ox = (double)oi.x;
     oy = (double)oi.y;
   }
-  const double reach = sqrt(range_sq) * 1.0001 + 1e-9;
+  const double reach = p.force_reach;  // sqrt(range_sq) * 1.0001 + 1e-9, from the host
   const int dxlo = ox < reach ? -1 : 0, dxhi = ox > g.sx - reach ? 1 : 0;
   const int dylo = oy < reach ? -1 : 0, dyhi = oy > g.sy - reach ? 1 : 0;
   for_neighbour_slots_box(g, st, c_pre, dxlo, dxhi, dylo, dyhi, [&](int j, int ordinal, int dcx, int dcy) {

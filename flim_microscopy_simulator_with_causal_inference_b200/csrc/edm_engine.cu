@@ -563,7 +563,13 @@ struct EdmEngine {
   void enqueue_dynamics_t(cudaStream_t s) {
     const int nbs = nb_scan;
     mark(0, s);
-    k_scan_reduce<<<nbs, kScanThreads, 0, s>>>(cnt, n_cells, bsum);
+    StepZero z{};
+    z.p[0] = grid_cnt, z.n[0] = grid_cnt ? n_grid : 0;
+    z.p[1] = grid_delta, z.n[1] = grid_delta ? n_grid : 0;
+    z.p[2] = moved_count, z.n[2] = R;
+    z.p[3] = contact_count, z.n[3] = contact_count ? EDM_MAX_CAT : 0;
+    z.p[4] = pl_count, z.n[4] = pl_count ? 1 : 0;
+    k_scan_reduce<<<nbs, kScanThreads, 0, s>>>(cnt, n_cells, bsum, z);
     k_scan_bsum<<<1, 1024, 0, s>>>(bsum, nbs);
     k_scan_down<<<nbs, kScanThreads, 0, s>>>(cnt, n_cells, bsum, cell_start, cursor);
     mark(1, s);
@@ -572,11 +578,6 @@ struct EdmEngine {
     tune_mark(TK_SCATTER, 0, s);
     launch_scatter<F64>(st, s);
     tune_mark(TK_SCATTER, 1, s);
-    if (n_grid > 0) {
-      cudaMemsetAsync(grid_cnt, 0, sizeof(int32_t) * n_grid, s);
-      cudaMemsetAsync(grid_delta, 0, sizeof(int32_t) * n_grid, s);
-    }
-    cudaMemsetAsync(moved_count, 0, sizeof(int32_t) * R, s);
     mark(2, s);
     tune_mark(TK_MOVE, 0, s);
     launch_move<F64>(st, s);
@@ -595,7 +596,6 @@ struct EdmEngine {
         case P_BIND_APPLY: k_bind_apply<F64><<<rb, 128, 0, s>>>(dp, R, st, ps.index); break;
         case P_DISSOC: k_dissociate<F64><<<sgrid, kBlock, 0, s>>>(dp, st, ps.match, ps.index); break;
         case P_CONTACTS:
-          cudaMemsetAsync(contact_count, 0, sizeof(int32_t) * EDM_MAX_CAT, s);
           tune_mark(TK_CONTACTS, 0, s);
           launch_contacts<F64>(st, ps.match, sgrid, s);
           tune_mark(TK_CONTACTS, 1, s);
@@ -613,7 +613,6 @@ struct EdmEngine {
             cudaStreamWaitEvent(side_stream, ev_fork, 0);
             ds = side_stream;
           }
-          cudaMemsetAsync(pl_count, 0, sizeof(int32_t), ds);
           k_pass_draws<<<sgrid, kBlock, 0, ds>>>(dp, st, d_draw, draw.any);
           if (fork) {
             cudaEventRecord(ev_join, side_stream);

@@ -52,7 +52,8 @@ DFIELD_NONE, DFIELD_REGIONS, DFIELD_SINE_X = 0, 1, 2
 # ----------------------------------------------------------------------------
 class EdmGrid(C.Structure):
     _fields_ = [("sensor", C.c_int32), ("nx", C.c_int32), ("ny", C.c_int32), ("pad", C.c_int32),
-                ("sx", C.c_double), ("sy", C.c_double), ("offset", C.c_int64)]
+                ("sx", C.c_double), ("sy", C.c_double), ("offset", C.c_int64),
+                ("inv_sx", C.c_double), ("inv_sy", C.c_double)]
 
 
 class EdmRule(C.Structure):
@@ -91,6 +92,7 @@ class EdmDynParams(C.Structure):
         ("particle_offset", C.c_int64), ("n_particles", C.c_int64),
         ("cell_offset", C.c_int64), ("grid_cells", C.c_int64),
         ("max_disp", C.c_double), ("max_disp_sq", C.c_double), ("force_range_sq", C.c_double),
+        ("force_reach", C.c_double),
         ("use_wca", C.c_int32), ("use_harmonic", C.c_int32), ("n_species", C.c_int32),
         ("dfield", C.c_int32),
         ("D_base", C.c_double * MAX_SPECIES),
@@ -505,6 +507,7 @@ def build_dyn_params(config: SimulationConfig, n_particles: int, seed: Optional[
     P.max_disp = d.max_displacement
     P.max_disp_sq = d.max_displacement * d.max_displacement
     P.force_range_sq = force_range_sq(d)
+    P.force_reach = math.sqrt(min(P.force_range_sq, P.cutoff_sq)) * 1.0001 + 1e-9
     P.use_wca, P.use_harmonic, P.n_species = int(d.use_wca), int(d.use_harmonic), config.n_species
     for i, s in enumerate(config.species):
         P.D_base[i] = s.diffusion_coefficient
@@ -560,6 +563,7 @@ def build_dyn_params(config: SimulationConfig, n_particles: int, seed: Optional[
     for k, (sensor, nxg, nyg, sx, sy) in enumerate(d.grids):
         g = P.grid[k]
         g.sensor, g.nx, g.ny, g.sx, g.sy, g.offset = sensor, nxg, nyg, sx, sy, goff
+        g.inv_sx, g.inv_sy = 1.0 / sx, 1.0 / sy
         goff += nxg * nyg
     P.grid_cells = goff - grid_offset
     tlen = int(hill_len) if hill_len is not None else n_particles + 1

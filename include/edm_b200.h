@@ -90,6 +90,7 @@ typedef struct {
   int32_t pad;
   double sx, sy;         /* cell sizes L/n                                    */
   int64_t offset;        /* start of this grid in the global count array      */
+  double inv_sx, inv_sy; /* 1/sx, 1/sy (division-free cell index, f32 path)   */
 } EdmGrid;
 
 typedef struct {
@@ -141,6 +142,7 @@ typedef struct {
   /* BD (dynamics.py:323-406, 1837-1864) */
   double max_disp, max_disp_sq;
   double force_range_sq; /* max over species pairs of the squared force range */
+  double force_reach;    /* sqrt(min(force_range_sq, cutoff_sq)) * 1.0001 + 1e-9 */
   int32_t use_wca, use_harmonic, n_species, dfield;
   double D_base[EDM_MAX_SPECIES];
   double sigma[EDM_MAX_SPECIES * EDM_MAX_SPECIES];
