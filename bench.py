@@ -535,8 +535,10 @@ def main():
     # the reactions group's in-graph time.
     cand = {
         "k_scan (3 launches)": (groups["cell_scan"], 20 * n_buckets, "20 B per sort bucket"),
-        "k_scatter": (groups["scatter"], 38 * N, "38 B per slot: slot record read + written, inverse map"),
-        "k_move": (groups["move"], 29 * N, "29 B per slot: 17 B pre-move slot read, 12 B position + cell written"),
+        "k_scatter": (groups["scatter"], 54 * N, "54 B per slot: 25 B slot record (offset hi + lo, cell, flags, id) "
+                                                 "read + written, 4 B inverse map"),
+        "k_move": (groups["move"], 45 * N, "45 B per slot: 25 B pre-move slot read (offset hi + lo, cell, flags, "
+                                           "id), 20 B offset hi + lo and cell written"),
     }
     eager_rx = sum(pm for _, _, pm in passes)
     scale_rx = groups["reactions"] / eager_rx if eager_rx > 0 else 1.0

@@ -46,6 +46,12 @@ struct DevState {
   float2* lo_post;
   int32_t* cell_pre;  // reference cell of each slot, before the move
   int32_t* cell_post;
+  // the previous sort (double-buffered with cell_pre / cell_start): a slot's
+  // bucket there, and the bucket starts, for the stable scatter
+  const int32_t* cell_pre_old;
+  const int32_t* cell_start_old;
+  int32_t* back;        // per bucket: particles placed from its end this sort
+  int32_t* fresh;       // 1 after edm_set_state: the next sort has no previous order
   const uint8_t* flags_old;
   uint8_t* flags;     // slot flags of the current step
   const int32_t* ids_old;
@@ -506,7 +512,7 @@ __global__ void k_scan_bsum(int32_t* __restrict__ bsum, int nb) {
 }
 
 __global__ void k_scan_down(int32_t* __restrict__ cnt, int64_t n, const int32_t* __restrict__ bsum,
-                            int32_t* __restrict__ start, int32_t* __restrict__ cursor) {
+                            int32_t* __restrict__ start, int32_t* __restrict__ cursor, int32_t* __restrict__ back) {
   const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
   const int4 c = load4(cnt, base, n);
   int total;
@@ -515,23 +521,53 @@ __global__ void k_scan_down(int32_t* __restrict__ cnt, int64_t n, const int32_t*
   store4(start, base, n, st4);
   store4(cursor, base, n, st4);
   store4(cnt, base, n, make_int4(0, 0, 0, 0));
+  store4(back, base, n, make_int4(0, 0, 0, 0));
   // the thread holding element n-1 writes the sentinel start[n]
   if (base < n && base + kScanItems >= n) start[n] = run + c.x + c.y + c.z + c.w;
   if (n == 0 && blockIdx.x == 0 && threadIdx.x == 0) start[0] = 0;
 }
 
+// Sort of the slots by bucket, stable for the particles that stay in their
+// bucket: slots are already grouped by the previous step's buckets, and most
+// particles keep theirs (a cell side is many mean steps).  A particle that
+// keeps an alive cell goes to the new bucket start plus the number of such
+// particles before it in its old run (no atomic); one that keeps the
+// non-alive bucket takes a warp-aggregated cursor from the bucket's start;
+// one that changed bucket takes an atomic slot from the bucket's end.  The
+// two ends meet exactly because the bucket counts are exact.  Right after
+// edm_set_state there is no previous order and every particle takes a cursor.
 template <bool F64, int BS>
 __global__ void __launch_bounds__(BS) k_scatter(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk,
-                                                    DevState st) {
+                                                DevState st) {
   const Tile t = tile_of(blk);
   const EdmDynParams& p = P[t.r];
   if (t.s >= p.particle_offset + p.n_particles) return;
   const int c = st.cell_post[t.s];
   const uint8_t f = st.flags_old[t.s];
-  // alive particles mostly have a cell to themselves: a plain atomic; the
-  // non-alive ones all share their replica's last bucket: aggregated per warp
-  const int d = fl_alive(f) ? atomicAdd(&st.cell_cursor[p.cell_offset + c], 1)
-                            : atomic_inc_aggregated(&st.cell_cursor[p.cell_offset + p.nx * p.ny]);
+  const int grave = p.nx * p.ny;
+  const int nb = fl_alive(f) ? c : grave;
+  const int32_t* cs = st.cell_start + p.cell_offset;
+  int d;
+  if (*st.fresh) {
+    d = fl_alive(f) ? atomicAdd(&st.cell_cursor[p.cell_offset + c], 1)
+                    : atomic_inc_aggregated(&st.cell_cursor[p.cell_offset + grave]);
+  } else {
+    const int32_t* os = st.cell_start_old + p.cell_offset;
+    const int ob = t.s >= os[grave] ? grave : st.cell_pre_old[t.s];
+    if (nb != ob) {
+      d = cs[nb + 1] - 1 - atomicAdd(&st.back[p.cell_offset + nb], 1);
+    } else if (nb == grave) {
+      d = atomic_inc_aggregated(&st.cell_cursor[p.cell_offset + grave]);
+    } else {
+      int rank = 0;
+      for (int64_t j = os[ob]; j < t.s; ++j) rank += (fl_alive(st.flags_old[j]) && st.cell_post[j] == ob) ? 1 : 0;
+      d = cs[nb] + rank;
+    }
+    if (d < cs[nb] || d >= cs[nb + 1]) {  // inconsistent counts: never write outside the bucket
+      set_status(st.status, EDM_STATUS_SORT);
+      return;
+    }
+  }
   if constexpr (F64) {
     ((double2*)st.pos_pre)[d] = ((const double2*)st.pos_post)[t.s];
   } else {
@@ -706,6 +742,7 @@ template <bool F64, int BS, int MINB>
 __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk,
                                                  DevState st) {
   const Tile t = tile_of(blk);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *st.fresh = 0;  // this step's sort has run
   const EdmDynParams& p = P[t.r];
   const int64_t s = t.s;
   if (s >= p.particle_offset + p.n_particles) return;
