@@ -908,6 +908,7 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
   ALLOC(E->cell_start_buf[1], nc + 1);
   ALLOC(E->back, nc);
   ALLOC(E->d_fresh, 1);
+  CUDA_TRY(cudaMemset(E->d_fresh, 1, sizeof(int32_t)));  // no previous sort yet
   ALLOC(E->cursor, nc);
   ALLOC(E->cnt, nc);
   E->nb_scan = (int)((nc + kScanTile - 1) / kScanTile);
