@@ -46,12 +46,6 @@ struct DevState {
   float2* lo_post;
   int32_t* cell_pre;  // reference cell of each slot, before the move
   int32_t* cell_post;
-  // the previous sort (double-buffered with cell_pre / cell_start): a slot's
-  // bucket there, and the bucket starts, for the stable scatter
-  const int32_t* cell_pre_old;
-  const int32_t* cell_start_old;
-  int32_t* back;        // per bucket: particles placed from its end this sort
-  int32_t* fresh;       // 1 after edm_set_state: the next sort has no previous order
   const uint8_t* flags_old;
   uint8_t* flags;     // slot flags of the current step
   const int32_t* ids_old;
@@ -512,7 +506,7 @@ __global__ void k_scan_bsum(int32_t* __restrict__ bsum, int nb) {
 }
 
 __global__ void k_scan_down(int32_t* __restrict__ cnt, int64_t n, const int32_t* __restrict__ bsum,
-                            int32_t* __restrict__ start, int32_t* __restrict__ cursor, int32_t* __restrict__ back) {
+                            int32_t* __restrict__ start, int32_t* __restrict__ cursor) {
   const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
   const int4 c = load4(cnt, base, n);
   int total;
@@ -521,53 +515,23 @@ __global__ void k_scan_down(int32_t* __restrict__ cnt, int64_t n, const int32_t*
   store4(start, base, n, st4);
   store4(cursor, base, n, st4);
   store4(cnt, base, n, make_int4(0, 0, 0, 0));
-  store4(back, base, n, make_int4(0, 0, 0, 0));
   // the thread holding element n-1 writes the sentinel start[n]
   if (base < n && base + kScanItems >= n) start[n] = run + c.x + c.y + c.z + c.w;
   if (n == 0 && blockIdx.x == 0 && threadIdx.x == 0) start[0] = 0;
 }
 
-// Sort of the slots by bucket, stable for the particles that stay in their
-// bucket: slots are already grouped by the previous step's buckets, and most
-// particles keep theirs (a cell side is many mean steps).  A particle that
-// keeps an alive cell goes to the new bucket start plus the number of such
-// particles before it in its old run (no atomic); one that keeps the
-// non-alive bucket takes a warp-aggregated cursor from the bucket's start;
-// one that changed bucket takes an atomic slot from the bucket's end.  The
-// two ends meet exactly because the bucket counts are exact.  Right after
-// edm_set_state there is no previous order and every particle takes a cursor.
 template <bool F64, int BS>
 __global__ void __launch_bounds__(BS) k_scatter(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk,
-                                                DevState st) {
+                                                    DevState st) {
   const Tile t = tile_of(blk);
   const EdmDynParams& p = P[t.r];
   if (t.s >= p.particle_offset + p.n_particles) return;
   const int c = st.cell_post[t.s];
   const uint8_t f = st.flags_old[t.s];
-  const int grave = p.nx * p.ny;
-  const int nb = fl_alive(f) ? c : grave;
-  const int32_t* cs = st.cell_start + p.cell_offset;
-  int d;
-  if (*st.fresh) {
-    d = fl_alive(f) ? atomicAdd(&st.cell_cursor[p.cell_offset + c], 1)
-                    : atomic_inc_aggregated(&st.cell_cursor[p.cell_offset + grave]);
-  } else {
-    const int32_t* os = st.cell_start_old + p.cell_offset;
-    const int ob = t.s >= os[grave] ? grave : st.cell_pre_old[t.s];
-    if (nb != ob) {
-      d = cs[nb + 1] - 1 - atomicAdd(&st.back[p.cell_offset + nb], 1);
-    } else if (nb == grave) {
-      d = atomic_inc_aggregated(&st.cell_cursor[p.cell_offset + grave]);
-    } else {
-      int rank = 0;
-      for (int64_t j = os[ob]; j < t.s; ++j) rank += (fl_alive(st.flags_old[j]) && st.cell_post[j] == ob) ? 1 : 0;
-      d = cs[nb] + rank;
-    }
-    if (d < cs[nb] || d >= cs[nb + 1]) {  // inconsistent counts: never write outside the bucket
-      set_status(st.status, EDM_STATUS_SORT);
-      return;
-    }
-  }
+  // alive particles mostly have a cell to themselves: a plain atomic; the
+  // non-alive ones all share their replica's last bucket: aggregated per warp
+  const int d = fl_alive(f) ? atomicAdd(&st.cell_cursor[p.cell_offset + c], 1)
+                            : atomic_inc_aggregated(&st.cell_cursor[p.cell_offset + p.nx * p.ny]);
   if constexpr (F64) {
     ((double2*)st.pos_pre)[d] = ((const double2*)st.pos_post)[t.s];
   } else {
@@ -742,7 +706,6 @@ template <bool F64, int BS, int MINB>
 __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk,
                                                  DevState st) {
   const Tile t = tile_of(blk);
-  if (blockIdx.x == 0 && threadIdx.x == 0) *st.fresh = 0;  // this step's sort has run
   const EdmDynParams& p = P[t.r];
   const int64_t s = t.s;
   if (s >= p.particle_offset + p.n_particles) return;
@@ -931,7 +894,8 @@ __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restric
 // substrate by the time pass c runs (its substrate, or a species earlier
 // passes convert into it) and the pair is within c's contact radius.  Pass c
 // then reads only its own list.
-constexpr int kContactSmem = 2048;
+constexpr int kContactSmem = 2048;              // staged contacts per block
+constexpr int kWarpStage = kContactSmem / (kBlock / 32);  // per warp
 
 struct CatLists {
   uint32_t capable[EDM_MAX_CAT];          // species that can be substrate of c at pass c
@@ -943,11 +907,15 @@ struct CatLists {
 template <bool F64, int MINB>
 __global__ void __launch_bounds__(kBlock, MINB) k_contacts(const EdmDynParams* __restrict__ P, DevState st, Match m,
                                                      CatLists L) {
-  __shared__ int2 buf[kContactSmem];
-  __shared__ int nbuf[EDM_MAX_CAT], base[EDM_MAX_CAT];
-  const int per = L.n_cat > 0 ? kContactSmem / L.n_cat : kContactSmem;  // staging slots per reaction
-  if (threadIdx.x < EDM_MAX_CAT) nbuf[threadIdx.x] = 0;
-  __syncthreads();
+  // Each warp stages its contacts in its own shared-memory region and
+  // appends them to the global lists when its sweep ends (one atomic per
+  // reaction and warp), so no warp waits for the block's slowest sweep.
+  __shared__ int2 buf[kBlock / 32][kWarpStage];
+  __shared__ int nbuf[kBlock / 32][EDM_MAX_CAT], base[kBlock / 32][EDM_MAX_CAT];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int per = L.n_cat > 0 ? kWarpStage / L.n_cat : kWarpStage;  // staging slots per reaction
+  if (lane < EDM_MAX_CAT) nbuf[wid][lane] = 0;
+  __syncwarp();
   sweep4(st, m, [&](int r, int64_t s) {
     const EdmDynParams& p = P[r];
     const Geo g(p);
@@ -982,9 +950,9 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contacts(const EdmDynParams* _
       for (uint32_t bits = rmask; bits; bits &= bits - 1) {
         const int c = __ffs(bits) - 1;
         if (!((L.capable[c] >> spj) & 1u) || d2 > p.cat[c].contact_sq) continue;
-        const int k = atomicAdd(&nbuf[c], 1);
+        const int k = atomicAdd(&nbuf[wid][c], 1);
         if (k < per) {
-          buf[c * per + k] = make_int2((int)s, j);
+          buf[wid][c * per + k] = make_int2((int)s, j);
         } else {  // staging full: append directly
           const int q = atomicAdd(&st.contact_count[c], 1);
           if (q < st.contact_cap) st.contacts[(int64_t)c * st.contact_cap + q] = make_int2((int)s, j);
@@ -993,17 +961,17 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contacts(const EdmDynParams* _
       }
     });
   });
-  __syncthreads();
-  if (threadIdx.x < L.n_cat) {
-    const int n = nbuf[threadIdx.x] < per ? nbuf[threadIdx.x] : per;
-    base[threadIdx.x] = n > 0 ? atomicAdd(&st.contact_count[threadIdx.x], n) : 0;
+  __syncwarp();
+  if (lane < L.n_cat) {
+    const int n = nbuf[wid][lane] < per ? nbuf[wid][lane] : per;
+    base[wid][lane] = n > 0 ? atomicAdd(&st.contact_count[lane], n) : 0;
   }
-  __syncthreads();
+  __syncwarp();
   for (int c = 0; c < L.n_cat; ++c) {
-    const int n = nbuf[c] < per ? nbuf[c] : per;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-      const int64_t q = (int64_t)base[c] + k;
-      if (q < st.contact_cap) st.contacts[(int64_t)c * st.contact_cap + q] = buf[c * per + k];
+    const int n = nbuf[wid][c] < per ? nbuf[wid][c] : per;
+    for (int k = lane; k < n; k += 32) {
+      const int64_t q = (int64_t)base[wid][c] + k;
+      if (q < st.contact_cap) st.contacts[(int64_t)c * st.contact_cap + q] = buf[wid][c * per + k];
       else set_status(st.status, EDM_STATUS_CONTACT_CAP);
     }
   }

@@ -118,17 +118,14 @@ struct EdmEngine {
   void* pos_pre = nullptr;
   void* pos_post = nullptr;
   float2 *lo_pre = nullptr, *lo_post = nullptr;
-  int32_t* cell_post = nullptr;
-  int32_t* cell_pre_buf[2] = {nullptr, nullptr};       // by slot parity `cur`, like flags and ids
+  int32_t *cell_pre = nullptr, *cell_post = nullptr;
   uint8_t* flags[2] = {nullptr, nullptr};
   int32_t* ids[2] = {nullptr, nullptr};
   int cur = 0;
   int32_t *slot_of_id = nullptr, *bond = nullptr;
   uint8_t *has_dye = nullptr, *bleached = nullptr;
   int8_t *dye = nullptr, *ctmc = nullptr;
-  int32_t *cursor = nullptr, *cnt = nullptr, *bsum = nullptr;
-  int32_t* cell_start_buf[2] = {nullptr, nullptr};     // sort-bucket starts, by slot parity `cur`
-  int32_t *back = nullptr, *d_fresh = nullptr;
+  int32_t *cell_start = nullptr, *cursor = nullptr, *cnt = nullptr, *bsum = nullptr;
   int nb_scan = 0;
   int32_t *grid_cnt = nullptr, *grid_delta = nullptr;
   int64_t* counters = nullptr;
@@ -189,11 +186,7 @@ struct EdmEngine {
     s.pos_post = pos_post;
     s.lo_pre = lo_pre;
     s.lo_post = lo_post;
-    s.cell_pre = cell_pre_buf[cur];
-    s.cell_pre_old = cell_pre_buf[cur ^ 1];
-    s.cell_start_old = cell_start_buf[cur ^ 1];
-    s.back = back;
-    s.fresh = d_fresh;
+    s.cell_pre = cell_pre;
     s.cell_post = cell_post;
     s.flags_old = flags[cur ^ 1];
     s.flags = flags[cur];
@@ -201,7 +194,7 @@ struct EdmEngine {
     s.ids = ids[cur];
     s.slot_of_id = slot_of_id;
     s.bond = bond;
-    s.cell_start = cell_start_buf[cur];
+    s.cell_start = cell_start;
     s.cell_cursor = cursor;
     s.cnt_next = cnt;
     s.grid_cnt = grid_cnt;
@@ -578,7 +571,7 @@ struct EdmEngine {
     z.p[4] = pl_count, z.n[4] = pl_count ? 1 : 0;
     k_scan_reduce<<<nbs, kScanThreads, 0, s>>>(cnt, n_cells, bsum, z);
     k_scan_bsum<<<1, 1024, 0, s>>>(bsum, nbs);
-    k_scan_down<<<nbs, kScanThreads, 0, s>>>(cnt, n_cells, bsum, cell_start_buf[cur ^ 1], cursor, back);
+    k_scan_down<<<nbs, kScanThreads, 0, s>>>(cnt, n_cells, bsum, cell_start, cursor);
     mark(1, s);
     cur ^= 1;
     DevState st = dev_state();
@@ -891,8 +884,7 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
     ALLOC(E->lo_pre, np);
     ALLOC(E->lo_post, np);
   }
-  ALLOC(E->cell_pre_buf[0], np);
-  ALLOC(E->cell_pre_buf[1], np);
+  ALLOC(E->cell_pre, np);
   ALLOC(E->cell_post, np);
   ALLOC(E->flags[0], np + 4);
   ALLOC(E->flags[1], np + 4);
@@ -904,11 +896,7 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
   ALLOC(E->bleached, np);
   ALLOC(E->dye, np);
   ALLOC(E->ctmc, np);
-  ALLOC(E->cell_start_buf[0], nc + 1);
-  ALLOC(E->cell_start_buf[1], nc + 1);
-  ALLOC(E->back, nc);
-  ALLOC(E->d_fresh, 1);
-  CUDA_TRY(cudaMemset(E->d_fresh, 1, sizeof(int32_t)));  // no previous sort yet
+  ALLOC(E->cell_start, nc + 1);
   ALLOC(E->cursor, nc);
   ALLOC(E->cnt, nc);
   E->nb_scan = (int)((nc + kScanTile - 1) / kScanTile);
@@ -1117,7 +1105,6 @@ int edm_set_state(EdmEngine* E, const EdmHostState* st, void* stream) {
   CUDA_TRY(cudaMemcpyAsync(E->ctmc, st->ctmc_state, N, cudaMemcpyHostToDevice, s));
   CUDA_TRY(cudaMemcpyAsync(E->bleached, st->is_bleached, N, cudaMemcpyHostToDevice, s));
   CUDA_TRY(cudaMemsetAsync(E->cnt, 0, sizeof(int32_t) * (E->n_cells > 0 ? E->n_cells : 1), s));
-  CUDA_TRY(cudaMemsetAsync(E->d_fresh, 1, sizeof(int32_t), s));  // no previous order: the next sort uses cursors
   if (E->npblk > 0) {
     if (E->f64)
       k_set_state<true><<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, dpos, E->st_sp, E->st_alive, E->pos_post, E->lo_post,
@@ -1695,7 +1682,7 @@ int edm_get_cells(EdmEngine* E, int32_t replica, int32_t* cell_start, int32_t* m
   // reference cell each slot stores.
   cudaStream_t s = (cudaStream_t)stream;
   std::vector<int32_t> cells(p.n_particles), ids(p.n_particles);
-  CUDA_TRY(cudaMemcpyAsync(cells.data(), E->cell_pre_buf[E->cur] + p.particle_offset, sizeof(int32_t) * p.n_particles,
+  CUDA_TRY(cudaMemcpyAsync(cells.data(), E->cell_pre + p.particle_offset, sizeof(int32_t) * p.n_particles,
                            cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaMemcpyAsync(ids.data(), E->ids[E->cur] + p.particle_offset, sizeof(int32_t) * p.n_particles,
                            cudaMemcpyDeviceToHost, s));

@@ -58,7 +58,6 @@ extern "C" {
 #define EDM_STATUS_RECRUIT_CAP 0x20u   /* recruitment candidate buffer overflow                         */
 #define EDM_STATUS_POISSON_NORMAL 0x40u /* a Poisson mean >= 30 used the normal approximation            */
 #define EDM_STATUS_CONTACT_CAP 0x80u   /* catalytic contact buffer overflow (events may be missed)      */
-#define EDM_STATUS_SORT 0x100u         /* bucket counts disagreed with the sort (a slot was not placed)  */
 
 /* ---- noise streams (Philox key = seed; counter = (a, b, step, stream)) --- */
 enum EdmStream {
