@@ -147,18 +147,22 @@ __device__ __forceinline__ U2 normal2(uint64_t seed, int64_t step, int stream, u
 }
 
 // The same normal pair in float32 for the float32 engine: the same uniforms,
-// the transform in float32 (relative error ~1e-6, far below the float32
-// path's position tolerance); ln(1 - u0) as log1pf(-u0) below 1/2, where the
-// float32 difference would lose u0.
+// the transform in float32 (error ~1e-6 of a unit normal, far below the
+// float32 path's position tolerance).
 __device__ __forceinline__ void normal2_f32(uint64_t seed, int64_t step, int stream, uint64_t a, float& z0,
                                             float& z1) {
   const U2 u = uniform2(seed, step, stream, a, 0);
-  const float w = u.u0 > 0.5 ? logf((float)(1.0 - u.u0)) : log1pf(-(float)u.u0);
+  // ln(1 - u0): the float64 difference rounded to float32 loses nothing that
+  // matters unless u0 is tiny, where log1pf(-u0) keeps it (a branch one lane
+  // in a thousand takes, so the warp rarely runs both)
+  const float w = u.u0 >= 0x1p-10 ? logf((float)(1.0 - u.u0)) : log1pf(-(float)u.u0);
   const float r = sqrtf(-2.0f * w);
+  // cos / sin of 2 pi u1 from the hardware approximations on [-pi, pi):
+  // cos(2 pi u1) = -cos(2 pi u1 - pi), likewise sin (absolute error ~1e-6)
   float sf, cf;
-  sincospif(2.0f * (float)u.u1, &sf, &cf);
-  z0 = r * cf;
-  z1 = r * sf;
+  __sincosf(6.283185307179586f * (float)u.u1 - 3.14159265358979f, &sf, &cf);
+  z0 = -r * cf;
+  z1 = -r * sf;
 }
 
 // ---- particle flags: bits 0-6 species, bit 7 alive -------------------------

@@ -583,7 +583,7 @@ __device__ __forceinline__ void for_each_force_term(const EdmDynParams& p, const
   const double reach = p.force_reach;  // sqrt(range_sq) * 1.0001 + 1e-9, from the host
   const int dxlo = ox < reach ? -1 : 0, dxhi = ox > g.sx - reach ? 1 : 0;
   const int dylo = oy < reach ? -1 : 0, dyhi = oy > g.sy - reach ? 1 : 0;
-  for_neighbour_slots_box(g, st, c_pre, dxlo, dxhi, dylo, dyhi, [&](int j, int ordinal, int dcx, int dcy) {
+  auto term = [&](int j, int ordinal, int dcx, int dcy) {
     {
       if (j == s) return;
       double dx, dy, dsq;
@@ -646,7 +646,15 @@ __device__ __forceinline__ void for_each_force_term(const EdmDynParams& p, const
         }
       }
     }
-  });
+  };
+  if ((dxlo | dxhi | dylo | dyhi) == 0) {
+    // farther than the reach from every side (most particles): the own
+    // cell's run alone, ordinal 4 = (0 + 1) * 3 + (0 + 1)
+    const int j0 = st.cell_start[g.cbase + c_pre], j1 = st.cell_start[g.cbase + c_pre + 1];
+    for (int j = j0; j < j1; ++j) term(j, 4, 0, 0);
+  } else {
+    for_neighbour_slots_box(g, st, c_pre, dxlo, dxhi, dylo, dyhi, term);
+  }
 }
 
 // D(x) and grad D at an absolute position (dynamics.py:440-519; sine-x field).
@@ -894,8 +902,7 @@ __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restric
 // substrate by the time pass c runs (its substrate, or a species earlier
 // passes convert into it) and the pair is within c's contact radius.  Pass c
 // then reads only its own list.
-constexpr int kContactSmem = 2048;              // staged contacts per block
-constexpr int kWarpStage = kContactSmem / (kBlock / 32);  // per warp
+constexpr int kContactSmem = 2048;
 
 struct CatLists {
   uint32_t capable[EDM_MAX_CAT];          // species that can be substrate of c at pass c
@@ -907,15 +914,11 @@ struct CatLists {
 template <bool F64, int MINB>
 __global__ void __launch_bounds__(kBlock, MINB) k_contacts(const EdmDynParams* __restrict__ P, DevState st, Match m,
                                                      CatLists L) {
-  // Each warp stages its contacts in its own shared-memory region and
-  // appends them to the global lists when its sweep ends (one atomic per
-  // reaction and warp), so no warp waits for the block's slowest sweep.
-  __shared__ int2 buf[kBlock / 32][kWarpStage];
-  __shared__ int nbuf[kBlock / 32][EDM_MAX_CAT], base[kBlock / 32][EDM_MAX_CAT];
-  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int per = L.n_cat > 0 ? kWarpStage / L.n_cat : kWarpStage;  // staging slots per reaction
-  if (lane < EDM_MAX_CAT) nbuf[wid][lane] = 0;
-  __syncwarp();
+  __shared__ int2 buf[kContactSmem];
+  __shared__ int nbuf[EDM_MAX_CAT], base[EDM_MAX_CAT];
+  const int per = L.n_cat > 0 ? kContactSmem / L.n_cat : kContactSmem;  // staging slots per reaction
+  if (threadIdx.x < EDM_MAX_CAT) nbuf[threadIdx.x] = 0;
+  __syncthreads();
   sweep4(st, m, [&](int r, int64_t s) {
     const EdmDynParams& p = P[r];
     const Geo g(p);
@@ -950,9 +953,9 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contacts(const EdmDynParams* _
       for (uint32_t bits = rmask; bits; bits &= bits - 1) {
         const int c = __ffs(bits) - 1;
         if (!((L.capable[c] >> spj) & 1u) || d2 > p.cat[c].contact_sq) continue;
-        const int k = atomicAdd(&nbuf[wid][c], 1);
+        const int k = atomicAdd(&nbuf[c], 1);
         if (k < per) {
-          buf[wid][c * per + k] = make_int2((int)s, j);
+          buf[c * per + k] = make_int2((int)s, j);
         } else {  // staging full: append directly
           const int q = atomicAdd(&st.contact_count[c], 1);
           if (q < st.contact_cap) st.contacts[(int64_t)c * st.contact_cap + q] = make_int2((int)s, j);
@@ -961,17 +964,17 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contacts(const EdmDynParams* _
       }
     });
   });
-  __syncwarp();
-  if (lane < L.n_cat) {
-    const int n = nbuf[wid][lane] < per ? nbuf[wid][lane] : per;
-    base[wid][lane] = n > 0 ? atomicAdd(&st.contact_count[lane], n) : 0;
+  __syncthreads();
+  if (threadIdx.x < L.n_cat) {
+    const int n = nbuf[threadIdx.x] < per ? nbuf[threadIdx.x] : per;
+    base[threadIdx.x] = n > 0 ? atomicAdd(&st.contact_count[threadIdx.x], n) : 0;
   }
-  __syncwarp();
+  __syncthreads();
   for (int c = 0; c < L.n_cat; ++c) {
-    const int n = nbuf[wid][c] < per ? nbuf[wid][c] : per;
-    for (int k = lane; k < n; k += 32) {
-      const int64_t q = (int64_t)base[wid][c] + k;
-      if (q < st.contact_cap) st.contacts[(int64_t)c * st.contact_cap + q] = buf[wid][c * per + k];
+    const int n = nbuf[c] < per ? nbuf[c] : per;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      const int64_t q = (int64_t)base[c] + k;
+      if (q < st.contact_cap) st.contacts[(int64_t)c * st.contact_cap + q] = buf[c * per + k];
       else set_status(st.status, EDM_STATUS_CONTACT_CAP);
     }
   }
