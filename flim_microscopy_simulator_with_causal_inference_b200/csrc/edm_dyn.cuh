@@ -980,6 +980,104 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contacts(const EdmDynParams* _
   }
 }
 
+// The same contact search with the work spread over (enzyme, neighbour
+// column) tasks: a warp compacts its enzymes as sweep4 does, then each lane
+// takes tasks t = lane, lane + 32, ... (enzyme t / 3, column t % 3 - 1) and
+// walks that column's one or two slot runs.  A lane's loop is about three
+// candidates instead of nine, so lanes idle less while the longest run
+// finishes.  Same tests, same contact set (in another order, which the
+// catalytic passes do not depend on).
+template <bool F64, int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) k_contacts_cols(const EdmDynParams* __restrict__ P, DevState st,
+                                                              Match m, CatLists L) {
+  __shared__ int2 buf[kContactSmem];
+  __shared__ int nbuf[EDM_MAX_CAT], base[EDM_MAX_CAT];
+  __shared__ int32_t list[kBlock / 32][kSweepChunk];
+  const int per = L.n_cat > 0 ? kContactSmem / L.n_cat : kContactSmem;
+  if (threadIdx.x < EDM_MAX_CAT) nbuf[threadIdx.x] = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) * 4;
+  int n = 0, r0 = 0;
+  if (w0 < st.n_slots) {  // whole warps: compact the chunk's enzymes
+    const int64_t s0 = w0 + (int64_t)lane * 4;
+    uchar4 f4 = make_uchar4(0, 0, 0, 0);
+    if (s0 < st.n_slots) f4 = *reinterpret_cast<const uchar4*>(st.flags + s0);
+    const uint8_t fl[4] = {f4.x, f4.y, f4.z, f4.w};
+    const unsigned below = (1u << lane) - 1u;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const bool hit = s0 + k < st.n_slots && matches(fl[k], m);
+      const unsigned bits = __ballot_sync(0xffffffffu, hit);
+      if (hit) list[wid][n + __popc(bits & below)] = (int32_t)(s0 + k);
+      n += __popc(bits);
+    }
+    r0 = st.chunk_rep[w0 / kSweepChunk];
+  }
+  __syncwarp();
+  for (int t = lane; t < 3 * n; t += 32) {
+    const int q = t / 3, dcx = t - 3 * q - 1;
+    const int64_t s = list[wid][q];
+    int r = r0;
+    while (r + 1 < st.n_rep && st.rep_first[r + 1] <= s) ++r;
+    const EdmDynParams& p = P[r];
+    const Geo g(p);
+    const int sps = fl_species(st.flags[s]);
+    const uint32_t rmask = L.reactions_of[sps], pmask = L.partners_of[sps];
+    float2 oi_pre = make_float2(0.f, 0.f), oi_post = make_float2(0.f, 0.f);
+    int cxs = 0, cys = 0;
+    if constexpr (!F64) {
+      oi_pre = ((const float2*)st.pos_pre)[s];
+      oi_post = ((const float2*)st.pos_post)[s];
+      split_cell(st.cell_post[s], g, cxs, cys);
+    }
+    for_neighbour_slots_box(g, st, st.cell_pre[s], dcx, dcx, -1, 1, [&](int j, int, int dcx_, int dcy) {
+      if (j == s) return;
+      const uint8_t fj = st.flags[j];
+      const int spj = fl_species(fj);
+      if (!fl_alive(fj) || !((pmask >> spj) & 1u)) return;
+      double d2;
+      if constexpr (F64) {
+        if (!(sep_sq<F64>(st.pos_pre, st.cell_pre, s, j, g) < g.cutoff_sq)) return;
+        d2 = sep_sq<F64>(st.pos_post, st.cell_post, s, j, g);
+      } else {
+        const float2 oj = ((const float2*)st.pos_pre)[j];
+        const float fdx = -(float)dcx_ * g.sxf + (oi_pre.x - oj.x);
+        const float fdy = -(float)dcy * g.syf + (oi_pre.y - oj.y);
+        if (!((double)(fdx * fdx + fdy * fdy) < g.cutoff_sq)) return;
+        float dx, dy;
+        d2 = (double)rel_sq_f32_xy(cxs, cys, oi_post, st.cell_post[j], ((const float2*)st.pos_post)[j], g, dx, dy);
+      }
+      for (uint32_t bits = rmask; bits; bits &= bits - 1) {
+        const int c = __ffs(bits) - 1;
+        if (!((L.capable[c] >> spj) & 1u) || d2 > p.cat[c].contact_sq) continue;
+        const int k = atomicAdd(&nbuf[c], 1);
+        if (k < per) {
+          buf[c * per + k] = make_int2((int)s, j);
+        } else {
+          const int qq = atomicAdd(&st.contact_count[c], 1);
+          if (qq < st.contact_cap) st.contacts[(int64_t)c * st.contact_cap + qq] = make_int2((int)s, j);
+          else set_status(st.status, EDM_STATUS_CONTACT_CAP);
+        }
+      }
+    });
+  }
+  __syncthreads();
+  if (threadIdx.x < L.n_cat) {
+    const int nn = nbuf[threadIdx.x] < per ? nbuf[threadIdx.x] : per;
+    base[threadIdx.x] = nn > 0 ? atomicAdd(&st.contact_count[threadIdx.x], nn) : 0;
+  }
+  __syncthreads();
+  for (int c = 0; c < L.n_cat; ++c) {
+    const int nn = nbuf[c] < per ? nbuf[c] : per;
+    for (int k = threadIdx.x; k < nn; k += blockDim.x) {
+      const int64_t qq = (int64_t)base[c] + k;
+      if (qq < st.contact_cap) st.contacts[(int64_t)c * st.contact_cap + qq] = buf[c * per + k];
+      else set_status(st.status, EDM_STATUS_CONTACT_CAP);
+    }
+  }
+}
+
 // Catalytic pass c (dynamics.py:825-983) over its contact list: the set of
 // substrates with at least one accepted (enzyme, substrate) pair converts.
 // Every listed pair is alive, has the pass's enzyme and is within its contact

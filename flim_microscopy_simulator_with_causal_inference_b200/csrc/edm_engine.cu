@@ -78,9 +78,9 @@ constexpr int kMaxShapes = 6;
 constexpr LaunchShape kShapes[TK_COUNT][kMaxShapes] = {
     {{256, 1}, {128, 1}, {512, 1}, {0, 0}, {0, 0}, {0, 0}},      // k_scatter
     {{256, 3}, {256, 4}, {128, 8}, {256, 1}, {512, 1}, {128, 5}},  // k_move
-    {{256, 6}, {256, 4}, {256, 8}, {0, 0}, {0, 0}, {0, 0}},      // k_contacts
+    {{256, 6}, {256, 4}, {256, 8}, {256, 6}, {256, 4}, {0, 0}},  // k_contacts (3, 4: by neighbour column)
 };
-constexpr int kNumShapes[TK_COUNT] = {3, 6, 3};
+constexpr int kNumShapes[TK_COUNT] = {3, 6, 5};
 const char* const kTunedNames[TK_COUNT] = {"k_scatter", "k_move", "k_contacts"};
 constexpr int kTileSizes[3] = {128, 256, 512};
 int tile_index(int bs) { return bs == 128 ? 0 : (bs == 256 ? 1 : 2); }
@@ -552,9 +552,11 @@ struct EdmEngine {
 
   template <bool F64>
   void launch_contacts(const DevState& st, const Match& m, int grid, cudaStream_t s) {
-    switch (shape[TK_CONTACTS]) {
+    switch (shape[TK_CONTACTS]) {  // the rows of kShapes[TK_CONTACTS]
       case 1: k_contacts<F64, 4><<<grid, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
       case 2: k_contacts<F64, 8><<<grid, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
+      case 3: k_contacts_cols<F64, 6><<<grid, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
+      case 4: k_contacts_cols<F64, 4><<<grid, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
       default: k_contacts<F64, 6><<<grid, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
     }
   }
@@ -1565,9 +1567,10 @@ int edm_launch_shapes(EdmEngine* E, int32_t* shapes, float* ms) {
   for (int k = 0; k < TK_COUNT; ++k) {
     const LaunchShape sh = kShapes[k][E->shape[k]];
     if (shapes) {
-      shapes[3 * k] = sh.block;
-      shapes[3 * k + 1] = sh.min_blocks;
-      shapes[3 * k + 2] = kNumShapes[k];
+      shapes[4 * k] = sh.block;
+      shapes[4 * k + 1] = sh.min_blocks;
+      shapes[4 * k + 2] = kNumShapes[k];
+      shapes[4 * k + 3] = E->shape[k];
     }
     if (ms) {
       ms[2 * k] = E->default_ms[k];

@@ -252,11 +252,12 @@ class Engine:
 
     def launch_shapes(self) -> dict:
         """{kernel: {block, min_blocks_per_sm, candidates, default_ms, tuned_ms}}."""
-        shp = np.zeros((3, 3), dtype=np.int32)
+        shp = np.zeros((3, 4), dtype=np.int32)
         ms = np.zeros((3, 2), dtype=np.float32)
         n = _check(self.L.edm_launch_shapes(self.handle, _ptr(shp), _ptr(ms)), "edm_launch_shapes")
         return {self.TUNED_KERNELS[k]: {"block": int(shp[k, 0]), "min_blocks_per_sm": int(shp[k, 1]),
-                                        "candidates": int(shp[k, 2]), "default_ms": float(ms[k, 0]),
+                                        "candidates": int(shp[k, 2]), "candidate": int(shp[k, 3]),
+                                        "default_ms": float(ms[k, 0]),
                                         "tuned_ms": float(ms[k, 1])} for k in range(n)}
 
     # ---- census: sub-frame recorder and per-frame ground truth --------------

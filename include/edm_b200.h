@@ -390,8 +390,10 @@ int edm_ground_truth(EdmEngine* eng, double* fret_E, double* tau_DA,
  * particle count) for the rest of the process and applied to later engines
  * of the same kind, unless retune != 0.  Drops the engine's captured graphs. */
 int edm_autotune(EdmEngine* eng, int32_t steps_per_shape, int32_t retune, void* stream);
-/* The launch shape in use per tuned kernel: shapes[k][3] = (threads per block,
- * minimum blocks per SM, candidates), ms[k][2] = (time of the default shape,
+/* The launch shape in use per tuned kernel: shapes[k][4] = (threads per block,
+ * minimum blocks per SM, candidates, chosen candidate; k_contacts candidates
+ * 3 and 4 are the variant whose lanes take one neighbour column of an enzyme
+ * each), ms[k][2] = (time of the default shape,
  * time of the chosen shape) from the last tuning (0 if not tuned).  Either
  * pointer may be NULL.  Returns the number of tuned kernels (3). */
 int edm_launch_shapes(EdmEngine* eng, int32_t* shapes, float* ms);
