@@ -647,14 +647,7 @@ __device__ __forceinline__ void for_each_force_term(const EdmDynParams& p, const
       }
     }
   };
-  if ((dxlo | dxhi | dylo | dyhi) == 0) {
-    // farther than the reach from every side (most particles): the own
-    // cell's run alone, ordinal 4 = (0 + 1) * 3 + (0 + 1)
-    const int j0 = st.cell_start[g.cbase + c_pre], j1 = st.cell_start[g.cbase + c_pre + 1];
-    for (int j = j0; j < j1; ++j) term(j, 4, 0, 0);
-  } else {
-    for_neighbour_slots_box(g, st, c_pre, dxlo, dxhi, dylo, dyhi, term);
-  }
+  for_neighbour_slots_box(g, st, c_pre, dxlo, dxhi, dylo, dyhi, term);
 }
 
 // D(x) and grad D at an absolute position (dynamics.py:440-519; sine-x field).
