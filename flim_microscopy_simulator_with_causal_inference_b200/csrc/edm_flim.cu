@@ -469,9 +469,10 @@ __device__ __forceinline__ uint32_t poisson(float mu, Rng& rng) {
 //      writes its expected mean arrival time;
 //   2. pixel by pixel, the warp places the pixel's N_free + N_bound photons:
 //      each picks its bin from its component's alias table with one 32-bit
-//      word of its lane's stream (stream (pixel, lane)), four per lane per
-//      round so table loads and shared-memory atomics overlap, and the
-//      pixel's histogram leaves in 512-byte coalesced stores.
+//      word of its lane's stream (stream (group, lane), running through the
+//      group's pixels), four per lane per round so table loads and
+//      shared-memory atomics overlap, and the pixel's histogram leaves in
+//      512-byte coalesced stores.
 __global__ void __launch_bounds__(256, 4) k_hist(EdmFlimParams p, const float* __restrict__ I /*[R][2][256*256]*/,
                                                  const int2* __restrict__ alias, const double* __restrict__ sums,
                                                  uint32_t* __restrict__ hist, double* __restrict__ tau_expected) {
@@ -513,32 +514,39 @@ __global__ void __launch_bounds__(256, 4) k_hist(EdmFlimParams p, const float* _
     }
     // ---- 2. the photons of each pixel of the group
     const int np = total - g0 < 32u ? (int)(total - g0) : 32;
+    // each lane's photon stream runs through the group's pixels in order:
+    // one seeding per group (key: the group's first pixel and the lane)
+    LaneRng rng(seed, r, g0 & 0xFFFFu, (uint32_t)lane);
     for (int q = 0; q < np; ++q) {
       const uint32_t gpx = g0 + (uint32_t)q;
-      const uint32_t px = gpx & 0xFFFFu;
       const int nf = __shfl_sync(FULL, n_free, q), na = __shfl_sync(FULL, n_all, q);
       {
         uint4* z = (uint4*)h;
         for (int i = lane; i < nb / 4; i += 32) z[i] = make_uint4(0u, 0u, 0u, 0u);
       }
       __syncwarp();
-      LaneRng rng(seed, r, px, (uint32_t)lane);
-      int i = lane;
-      for (; i + 96 < na; i += 128) {
-        uint32_t w[4];
-        int2 e[4];
+      // the free component's photons, then the bound component's, each
+      // from its own alias table
+      for (int c = 0; c < 2; ++c) {
+        const int2* tc = tab[c];
+        const int n = c == 0 ? nf : na - nf;
+        int i = lane;
+        for (; i + 96 < n; i += 128) {
+          uint32_t w[4];
+          int2 e[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) w[k] = rng.next();
+          for (int k = 0; k < 4; ++k) w[k] = rng.next();
 #pragma unroll
-        for (int k = 0; k < 4; ++k) e[k] = tab[i + 32 * k < nf ? 0 : 1][w[k] >> shift];
+          for (int k = 0; k < 4; ++k) e[k] = tc[w[k] >> shift];
 #pragma unroll
-        for (int k = 0; k < 4; ++k)
-          atomicAdd(&h[(int)(w[k] & 0xFFFFFFu) < e[k].x ? (int)(w[k] >> shift) : e[k].y], 1u);
-      }
-      for (; i < na; i += 32) {
-        const uint32_t w = rng.next();
-        const int2 e = tab[i < nf ? 0 : 1][w >> shift];
-        atomicAdd(&h[(int)(w & 0xFFFFFFu) < e.x ? (int)(w >> shift) : e.y], 1u);
+          for (int k = 0; k < 4; ++k)
+            atomicAdd(&h[(int)(w[k] & 0xFFFFFFu) < e[k].x ? (int)(w[k] >> shift) : e[k].y], 1u);
+        }
+        for (; i < n; i += 32) {
+          const uint32_t w = rng.next();
+          const int2 e = tc[w >> shift];
+          atomicAdd(&h[(int)(w & 0xFFFFFFu) < e.x ? (int)(w >> shift) : e.y], 1u);
+        }
       }
       __syncwarp();
       uint4* out = (uint4*)(hist + (size_t)gpx * (size_t)nb);
