@@ -502,27 +502,48 @@ def main():
     state_out = {k: torch.empty((eng.N, w) if w > 1 else (eng.N,), dtype=tdt[dt]).pin_memory().numpy()
                  for k, dt, w in eng.STATE_FIELDS}
     state_bytes_in = sum(v.nbytes for v in pinned.values())
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        eng.set_state(pinned["positions"], pinned["species"], pinned["alive"], pinned["bond"], pinned["has_dye"],
-                      pinned["dye"], pinned["ctmc"], pinned["bleached"], stream=stream)
-        eng.pipeline_steps(STEPS_PER_FRAME, True, STEPS_PER_FRAME, stream=stream)
-        eng.finalize(frame, stream=stream)
-        st = eng.get_state(stream=stream, out=state_out)
-        # every replica's stacks: snapshot + clear on the stream, D2H on the engine's copy stream; the
-        # state is read first, so the two reads do not share the device-to-host link
-        eng.frame_out_begin(flim_host, stream=stream)
-        frame += 1
-    eng.frame_out_wait()
-    torch.cuda.synchronize()
-    e2e_s = max_over_ranks(time.perf_counter() - t0, world, "cuda")
-    e2e_value = job_ps / e2e_s
-    state_bytes_out = sum(v.nbytes for v in st.values())
-    h2d = state_bytes_in / STEPS_PER_FRAME
-    d2h = (flim_elems * 4 + state_bytes_out) / STEPS_PER_FRAME
+    sp_cap = max(1, flim_elems // 64)
+    sp_idx = torch.empty(sp_cap, dtype=torch.int64).pin_memory().numpy()
+    sp_cnt = torch.empty(sp_cap, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+
+    def e2e_loop(sparse: bool):
+        """Frames through the C ABI with host buffers: state H2D, 100 steps,
+        finalize, state D2H and every replica's stacks D2H (their nonzero bins
+        with edm_frame_out_sparse, or dense on the copy stream)."""
+        nonlocal frame
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        d2h_flim = 0
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            eng.set_state(pinned["positions"], pinned["species"], pinned["alive"], pinned["bond"],
+                          pinned["has_dye"], pinned["dye"], pinned["ctmc"], pinned["bleached"], stream=stream)
+            eng.pipeline_steps(STEPS_PER_FRAME, True, STEPS_PER_FRAME, stream=stream)
+            eng.finalize(frame, stream=stream)
+            st = eng.get_state(stream=stream, out=state_out)
+            done = False
+            if sparse:
+                try:
+                    nnz = eng.frame_out_sparse(sp_idx, sp_cnt, stream=stream)
+                    d2h_flim += nnz * 12
+                    done = True
+                except RuntimeError:  # a frame denser than the buffer: read it dense
+                    pass
+            if not done:
+                # snapshot + clear on the stream, D2H on the engine's copy stream, overlapping the next frame
+                eng.frame_out_begin(flim_host, stream=stream)
+                d2h_flim += flim_elems * 4
+            frame += 1
+        eng.frame_out_wait()
+        torch.cuda.synchronize()
+        e2e_s = max_over_ranks(time.perf_counter() - t0, world, "cuda")
+        state_bytes_out = sum(v.nbytes for v in st.values())
+        return job_ps / e2e_s, state_bytes_in / STEPS_PER_FRAME, \
+            (d2h_flim / args.steps + state_bytes_out) / STEPS_PER_FRAME
+
+    e2e_value, h2d, d2h = e2e_loop(sparse=True)
+    e2e_dense, _, d2h_dense = e2e_loop(sparse=False)
 
     # ---- per-kernel timing (CUDA events inside a captured graph) -------------
     prof = eng.profile_steps(20, True, stream=stream)
@@ -655,9 +676,12 @@ def main():
                        "bd_steps_per_step": STEPS_PER_FRAME, "precision": "f32 cell-relative positions",
                        "l2": "working set > 126 MB L2 (resident state ~45 B/particle)"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                    "note": "per frame: state H2D from pinned host, 100 BD steps, finalize, every FLIM stack D2H "
-                            "(edm_frame_out_begin: on a copy stream, overlapping the next frame; the timed region "
-                            "ends after the last read), state D2H; bytes are per BD step"},
+                    "note": "per frame: state H2D from pinned host, 100 BD steps, finalize, state D2H, every "
+                            "replica's FLIM stacks D2H as their nonzero bins (edm_frame_out_sparse: element index "
+                            "+ count, lossless); bytes are per BD step",
+                    "dense_stacks": {"value": e2e_dense, "d2h_bytes_per_step": int(d2h_dense),
+                                     "note": "the same loop reading the stacks dense (edm_frame_out_begin on a "
+                                             "copy stream, overlapping the next frame)"}},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "alg_bytes": dom_bytes, "alg_bytes_definition": dom_def, "kernel_ms": dom_ms,

@@ -710,6 +710,12 @@ struct EdmEngine {
 
   // overlapped frame readout (edm_frame_out_begin / _wait)
   uint32_t* flim_snap = nullptr;
+  // sparse frame readout: block counts and offsets, device output of sp_cap entries
+  int32_t* sp_bcount = nullptr;
+  int64_t* sp_off = nullptr;
+  int64_t* sp_idx = nullptr;
+  uint32_t* sp_cnt = nullptr;
+  int64_t sp_cap = 0;
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_snap = nullptr, ev_read = nullptr;
   bool read_pending = false;
@@ -1021,6 +1027,86 @@ int edm_destroy(EdmEngine* eng) {
 
 // ---- state upload / download ------------------------------------------------
 namespace {
+
+// ---- sparse frame readout ----------------------------------------------------
+// A frame's TCSPC stacks are mostly zero (about one bin in a thousand holds a
+// photon at the bench's rates), so the readout can move only the nonzero
+// bins.  Block b owns the elements [b chunk, (b + 1) chunk) of the
+// concatenated stacks; a counting pass and a scan of the block counts give
+// each block its output offset, and the writing pass emits (element index,
+// count) in index order and clears the bins it emits.
+constexpr int kSpBlocks = 148 * 8;
+constexpr int kSpThreads = 256;
+
+__device__ __forceinline__ uint4 sp_load(const uint32_t* f, int64_t i, int64_t end) {
+  if (i + 3 < end) return *reinterpret_cast<const uint4*>(f + i);
+  uint4 v = make_uint4(0u, 0u, 0u, 0u);
+  if (i < end) v.x = f[i];
+  if (i + 1 < end) v.y = f[i + 1];
+  if (i + 2 < end) v.z = f[i + 2];
+  return v;
+}
+
+__global__ void __launch_bounds__(kSpThreads) k_sp_count(const uint32_t* __restrict__ flim, int64_t n, int64_t chunk,
+                                                         int32_t* __restrict__ bcount) {
+  __shared__ int ws[kSpThreads / 32];
+  const int64_t b0 = (int64_t)blockIdx.x * chunk, b1 = b0 + chunk < n ? b0 + chunk : n;
+  int c = 0;
+  for (int64_t i = b0 + 4 * (int64_t)threadIdx.x; i < b1; i += 4 * (int64_t)blockDim.x) {
+    const uint4 v = sp_load(flim, i, b1);
+    c += (v.x != 0u) + (v.y != 0u) + (v.z != 0u) + (v.w != 0u);
+  }
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < kSpThreads / 32; ++w) t += ws[w];
+    bcount[blockIdx.x] = t;
+  }
+}
+
+// exclusive scan of the block counts (one block); off[nb] = total
+__global__ void k_sp_scan(const int32_t* __restrict__ bcount, int nb, int64_t* __restrict__ off) {
+  int64_t carry = 0;
+  for (int base = 0; base < nb; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    const int v = i < nb ? bcount[i] : 0;
+    int total;
+    const int ex = block_exclusive_scan(v, total);
+    if (i < nb) off[i] = carry + ex;
+    carry += total;
+  }
+  if (threadIdx.x == 0) off[nb] = carry;
+}
+
+// Emit and clear the nonzero bins; writes nothing (and clears nothing) when
+// the frame holds more nonzero bins than the output's capacity.
+__global__ void __launch_bounds__(kSpThreads) k_sp_write(uint32_t* __restrict__ flim, int64_t n, int64_t chunk,
+                                                         const int64_t* __restrict__ off, int nb,
+                                                         int64_t* __restrict__ idx_out, uint32_t* __restrict__ cnt_out,
+                                                         int64_t cap) {
+  if (off[nb] > cap) return;
+  const int64_t b0 = (int64_t)blockIdx.x * chunk, b1 = b0 + chunk < n ? b0 + chunk : n;
+  int64_t base = off[blockIdx.x];
+  for (int64_t t0 = b0; t0 < b1; t0 += 4 * (int64_t)blockDim.x) {  // same trip count in every thread
+    const int64_t i = t0 + 4 * (int64_t)threadIdx.x;
+    const uint4 v = sp_load(flim, i, b1);
+    const uint32_t e[4] = {v.x, v.y, v.z, v.w};
+    const int c = (v.x != 0u) + (v.y != 0u) + (v.z != 0u) + (v.w != 0u);
+    int total;
+    int q = block_exclusive_scan(c, total);
+    for (int k = 0; k < 4; ++k) {
+      if (e[k] != 0u) {
+        idx_out[base + q] = i + k;
+        cnt_out[base + q] = e[k];
+        flim[i + k] = 0u;
+        ++q;
+      }
+    }
+    base += total;
+  }
+}
 
 template <bool F64>
 __global__ void k_set_state(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk, const double* pos,
@@ -1648,6 +1734,52 @@ int edm_frame_out_begin(EdmEngine* E, uint32_t* host_out, int64_t n_elems, void*
   CUDA_TRY(cudaEventRecord(E->ev_read, E->copy_stream));
   E->read_pending = true;
   return EDM_OK;
+}
+
+int64_t edm_frame_out_sparse(EdmEngine* E, int64_t* idx_host, uint32_t* count_host, int64_t cap, void* stream) {
+  if (!E || !E->has_scope || cap < 0 || (cap > 0 && (!idx_host || !count_host)))
+    return fail(EDM_EINVAL, "edm_frame_out_sparse: bad argument");
+  CUDA_TRY(cudaSetDevice(E->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t dcap = cap < E->n_flim ? cap : E->n_flim;
+  int rc;
+  if (!E->sp_bcount) {
+    if ((rc = E->alloc(&E->sp_bcount, kSpBlocks)) != EDM_OK) return rc;
+    if ((rc = E->alloc(&E->sp_off, kSpBlocks + 1)) != EDM_OK) return rc;
+  }
+  if (dcap > E->sp_cap) {  // (re)size the device output
+    for (auto& a : E->allocs)
+      if (a == (void*)E->sp_idx || a == (void*)E->sp_cnt) a = nullptr;
+    CUDA_TRY(cudaStreamSynchronize(s));
+    cudaFree(E->sp_idx);
+    cudaFree(E->sp_cnt);
+    E->sp_idx = nullptr;
+    E->sp_cnt = nullptr;
+    E->sp_cap = 0;
+    if ((rc = E->alloc(&E->sp_idx, (size_t)std::max<int64_t>(dcap, 1))) != EDM_OK) return rc;
+    if ((rc = E->alloc(&E->sp_cnt, (size_t)std::max<int64_t>(dcap, 1))) != EDM_OK) return rc;
+    E->sp_cap = dcap;
+  }
+  const int64_t n = E->n_flim;
+  const int64_t per = (n + kSpBlocks - 1) / kSpBlocks;
+  const int64_t quantum = 4 * kSpThreads;
+  const int64_t chunk = std::max<int64_t>(quantum, (per + quantum - 1) / quantum * quantum);
+  k_sp_count<<<kSpBlocks, kSpThreads, 0, s>>>(E->flim, n, chunk, E->sp_bcount);
+  k_sp_scan<<<1, 1024, 0, s>>>(E->sp_bcount, kSpBlocks, E->sp_off);
+  k_sp_write<<<kSpBlocks, kSpThreads, 0, s>>>(E->flim, n, chunk, E->sp_off, kSpBlocks, E->sp_idx, E->sp_cnt, dcap);
+  CUDA_TRY(cudaGetLastError());
+  int64_t total = 0;
+  CUDA_TRY(cudaMemcpyAsync(&total, E->sp_off + kSpBlocks, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  if (total > dcap)
+    return fail(EDM_EINVAL, "edm_frame_out_sparse: " + std::to_string((long long)total) +
+                                " nonzero bins exceed the capacity; the stacks are left in place");
+  if (total > 0) {
+    CUDA_TRY(cudaMemcpyAsync(idx_host, E->sp_idx, sizeof(int64_t) * total, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(count_host, E->sp_cnt, sizeof(uint32_t) * total, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  return total;
 }
 
 int edm_frame_out_wait(EdmEngine* E) {

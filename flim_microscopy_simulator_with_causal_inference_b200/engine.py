@@ -84,6 +84,8 @@ def load_library():
     L.edm_flim_elems.restype = i64
     L.edm_frame_out_begin.argtypes = [vp, vp, i64, vp]
     L.edm_frame_out_wait.argtypes = [vp]
+    L.edm_frame_out_sparse.argtypes = [vp, vp, vp, i64, vp]
+    L.edm_frame_out_sparse.restype = i64
     L.edm_flim_create.argtypes = [vp, i32, C.POINTER(vp)]
     L.edm_flim_destroy.argtypes = [vp]
     L.edm_flim_set_inputs.argtypes = [vp, vp, u64, vp]
@@ -313,6 +315,24 @@ class Engine:
             raise ValueError("host_out must be a contiguous uint32 array")
         _check(self.L.edm_frame_out_begin(self.handle, _ptr(host_out), host_out.size, _stream_handle(stream)),
                "edm_frame_out_begin")
+
+    def frame_out_sparse(self, idx_out: np.ndarray, count_out: np.ndarray, stream=None) -> int:
+        """Every replica's finalized stacks as nonzero bins (element index into
+        the concatenated stacks, count) written into idx_out (int64) and
+        count_out (uint32), both of capacity len(idx_out); the emitted bins
+        are cleared.  Returns the number of nonzero bins."""
+        if idx_out.dtype != np.int64 or count_out.dtype != np.uint32 or idx_out.size != count_out.size:
+            raise ValueError("idx_out must be int64 and count_out uint32 of the same length")
+        n = self.L.edm_frame_out_sparse(self.handle, _ptr(idx_out), _ptr(count_out), idx_out.size,
+                                        _stream_handle(stream))
+        return _check(int(n), "edm_frame_out_sparse")
+
+    @staticmethod
+    def sparse_to_dense(idx: np.ndarray, count: np.ndarray, n: int, n_elems: int) -> np.ndarray:
+        """The dense concatenated stacks (uint32, n_elems long) of a sparse readout of n bins."""
+        out = np.zeros(n_elems, dtype=np.uint32)
+        out[idx[:n]] = count[:n]
+        return out
 
     def frame_out_wait(self) -> None:
         """Block until the last frame_out_begin read has landed in host memory."""

@@ -335,6 +335,18 @@ int64_t edm_flim_elems(EdmEngine* eng);
 int edm_frame_out_begin(EdmEngine* eng, uint32_t* host_out, int64_t n_elems,
                         void* stream);
 int edm_frame_out_wait(EdmEngine* eng);
+/* Every replica's finalized stacks as their nonzero bins only: element index
+ * into the concatenated stacks (edm_flim_elems() long; replica r starts at
+ * its EdmScopeParams.flim_offset) and count, in index order, copied to host
+ * memory; the emitted bins are cleared, so the stacks start the next frame
+ * at zero as with edm_frame_out_begin.  A frame's stacks hold about one
+ * photon per thousand bins at the rates of the reference's examples, so
+ * this moves a few megabytes where the dense read moves gigabytes.  Returns
+ * the number of nonzero bins; more than cap is an error and leaves the
+ * stacks untouched.  Synchronous on `stream`.  No reference counterpart
+ * (finalize_frame returns dense stacks, microscope.py:1159-1203). */
+int64_t edm_frame_out_sparse(EdmEngine* eng, int64_t* idx_host, uint32_t* count_host, int64_t cap,
+                             void* stream);
 
 /* ---- census rows: sub-frame series and per-frame ground truth -------------
  * One row of EDM_CENSUS_FIELDS int64 per replica holds what the reference's
