@@ -887,37 +887,114 @@ __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restric
 // =============================================================================
 
 // Catalytic contacts (pairs of the reference's pre-move pair list, dynamics.py
-// :219-278, in post-move contact): enzyme-capable alive particles sweep their
-// neighbour cells once per step, after the binding passes.  During the
-// catalytic passes enzymes keep their species and nobody moves or dies, so a
-// pair (enzyme s, partner j) is filed once, in the list of every catalytic
-// reaction c whose enzyme is s's species, when j's species can be c's
-// substrate by the time pass c runs (its substrate, or a species earlier
-// passes convert into it) and the pair is within c's contact radius.  Pass c
-// then reads only its own list.
+// :219-278, in post-move contact).  During the catalytic passes enzymes keep
+// their species and nobody moves or dies, so pass c needs the pairs (enzyme
+// of species E_c, partner) within c's contact radius whose partner holds c's
+// substrate S_c when pass c runs:
+// * direct pairs, whose partner holds S_c at the step start, are found by
+//   one sweep after the move, from the rarer side of each reaction: the
+//   alive particles of the sweeping species (E_c or S_c) visit their
+//   neighbour cells for the other species.  Both distance tests are
+//   symmetric in the two particles (the float32 differences change sign
+//   exactly), so either side finds the same pairs;
+// * late pairs, whose partner an earlier catalytic pass of the step turns
+//   into S_c, are few: the pass that converts a particle looks up its
+//   enzymes of the later reactions at once (late_contacts).
+// A pair can be filed twice (a partner converted away and back); the passes
+// accept a substrate once, so duplicates change nothing.
 constexpr int kContactSmem = 2048;
 
 struct CatLists {
-  uint32_t capable[EDM_MAX_CAT];          // species that can be substrate of c at pass c
-  uint32_t reactions_of[EDM_MAX_SPECIES];  // reactions whose enzyme is the species
-  uint32_t partners_of[EDM_MAX_SPECIES];   // union of capable[c] over those reactions
+  uint32_t sweep_rx[EDM_MAX_SPECIES];        // reactions whose direct pairs the species sweeps for
+  uint32_t sweep_partners[EDM_MAX_SPECIES];  // species those sweeps look for
+  int32_t other[EDM_MAX_CAT];                // species the sweeper of reaction c looks for
+  uint32_t from_enzyme;                      // reactions swept from the enzyme side
   int n_cat;
 };
+
+// One neighbour j (pre-move cell offset dcx, dcy) of sweeper s: the pair
+// tests, then stage(c, enzyme, substrate) for each reaction of rx it meets.
+// oi_pre / oi_post / (cxs, cys): the sweeper's float32 offsets and post-move
+// cell (float32 path).
+template <bool F64, typename Stage>
+__device__ __forceinline__ void contact_candidate(const EdmDynParams& p, const Geo& g, const DevState& st,
+                                                  const CatLists& L, int64_t s, int j, int dcx, int dcy,
+                                                  uint32_t rx, uint32_t pmask, float2 oi_pre, float2 oi_post,
+                                                  int cxs, int cys, Stage stage) {
+  if (j == s) return;
+  const uint8_t fj = st.flags[j];
+  const int spj = fl_species(fj);
+  if (!fl_alive(fj) || !((pmask >> spj) & 1u)) return;
+  double d2;
+  if constexpr (F64) {
+    if (!(sep_sq<F64>(st.pos_pre, st.cell_pre, s, j, g) < g.cutoff_sq)) return;
+    d2 = sep_sq<F64>(st.pos_post, st.cell_post, s, j, g);
+  } else {
+    // pre-move: j sits in the neighbour cell at (dcx, dcy)
+    const float2 oj = ((const float2*)st.pos_pre)[j];
+    const float fdx = -(float)dcx * g.sxf + (oi_pre.x - oj.x);
+    const float fdy = -(float)dcy * g.syf + (oi_pre.y - oj.y);
+    if (!((double)(fdx * fdx + fdy * fdy) < g.cutoff_sq)) return;
+    float dx, dy;
+    d2 = (double)rel_sq_f32_xy(cxs, cys, oi_post, st.cell_post[j], ((const float2*)st.pos_post)[j], g, dx, dy);
+  }
+  for (uint32_t bits = rx; bits; bits &= bits - 1) {
+    const int c = __ffs(bits) - 1;
+    if (spj != L.other[c] || d2 > p.cat[c].contact_sq) continue;
+    if ((L.from_enzyme >> c) & 1u) stage(c, (int)s, j);
+    else stage(c, j, (int)s);
+  }
+}
+
+// Shared-memory staging of a block's contact pairs, per reaction, then one
+// global append per reaction; a full stage appends directly.
+struct ContactStage {
+  int2* buf;
+  int* nbuf;
+  int per;
+  __device__ __forceinline__ void operator()(const DevState& st, int c, int e, int sub) const {
+    const int k = atomicAdd(&nbuf[c], 1);
+    if (k < per) {
+      buf[c * per + k] = make_int2(e, sub);
+    } else {
+      const int q = atomicAdd(&st.contact_count[c], 1);
+      if (q < st.contact_cap) st.contacts[(int64_t)c * st.contact_cap + q] = make_int2(e, sub);
+      else set_status(st.status, EDM_STATUS_CONTACT_CAP);
+    }
+  }
+};
+
+__device__ __forceinline__ void flush_contacts(const DevState& st, const CatLists& L, const ContactStage& S,
+                                               int* base) {
+  __syncthreads();
+  if (threadIdx.x < L.n_cat) {
+    const int n = S.nbuf[threadIdx.x] < S.per ? S.nbuf[threadIdx.x] : S.per;
+    base[threadIdx.x] = n > 0 ? atomicAdd(&st.contact_count[threadIdx.x], n) : 0;
+  }
+  __syncthreads();
+  for (int c = 0; c < L.n_cat; ++c) {
+    const int n = S.nbuf[c] < S.per ? S.nbuf[c] : S.per;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      const int64_t q = (int64_t)base[c] + k;
+      if (q < st.contact_cap) st.contacts[(int64_t)c * st.contact_cap + q] = S.buf[c * S.per + k];
+      else set_status(st.status, EDM_STATUS_CONTACT_CAP);
+    }
+  }
+}
 
 template <bool F64, int MINB>
 __global__ void __launch_bounds__(kBlock, MINB) k_contacts(const EdmDynParams* __restrict__ P, DevState st, Match m,
                                                      CatLists L) {
   __shared__ int2 buf[kContactSmem];
   __shared__ int nbuf[EDM_MAX_CAT], base[EDM_MAX_CAT];
-  const int per = L.n_cat > 0 ? kContactSmem / L.n_cat : kContactSmem;  // staging slots per reaction
+  const ContactStage S{buf, nbuf, L.n_cat > 0 ? kContactSmem / L.n_cat : kContactSmem};
   if (threadIdx.x < EDM_MAX_CAT) nbuf[threadIdx.x] = 0;
   __syncthreads();
   sweep4(st, m, [&](int r, int64_t s) {
     const EdmDynParams& p = P[r];
     const Geo g(p);
     const int sps = fl_species(st.flags[s]);
-    const uint32_t rmask = L.reactions_of[sps], pmask = L.partners_of[sps];
-    // this particle's pre- and post-move points (float32: offsets + post cell)
+    const uint32_t rx = L.sweep_rx[sps], pmask = L.sweep_partners[sps];
     float2 oi_pre = make_float2(0.f, 0.f), oi_post = make_float2(0.f, 0.f);
     int cxs = 0, cys = 0;
     if constexpr (!F64) {
@@ -926,56 +1003,16 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contacts(const EdmDynParams* _
       split_cell(st.cell_post[s], g, cxs, cys);
     }
     for_neighbour_slots(g, st, st.cell_pre[s], [&](int j, int, int dcx, int dcy) {
-      if (j == s) return;
-      const uint8_t fj = st.flags[j];
-      const int spj = fl_species(fj);
-      if (!fl_alive(fj) || !((pmask >> spj) & 1u)) return;
-      double d2;
-      if constexpr (F64) {
-        if (!(sep_sq<F64>(st.pos_pre, st.cell_pre, s, j, g) < g.cutoff_sq)) return;
-        d2 = sep_sq<F64>(st.pos_post, st.cell_post, s, j, g);
-      } else {
-        // pre-move: j sits in the neighbour cell at (dcx, dcy)
-        const float2 oj = ((const float2*)st.pos_pre)[j];
-        const float fdx = -(float)dcx * g.sxf + (oi_pre.x - oj.x);
-        const float fdy = -(float)dcy * g.syf + (oi_pre.y - oj.y);
-        if (!((double)(fdx * fdx + fdy * fdy) < g.cutoff_sq)) return;
-        float dx, dy;
-        d2 = (double)rel_sq_f32_xy(cxs, cys, oi_post, st.cell_post[j], ((const float2*)st.pos_post)[j], g, dx, dy);
-      }
-      for (uint32_t bits = rmask; bits; bits &= bits - 1) {
-        const int c = __ffs(bits) - 1;
-        if (!((L.capable[c] >> spj) & 1u) || d2 > p.cat[c].contact_sq) continue;
-        const int k = atomicAdd(&nbuf[c], 1);
-        if (k < per) {
-          buf[c * per + k] = make_int2((int)s, j);
-        } else {  // staging full: append directly
-          const int q = atomicAdd(&st.contact_count[c], 1);
-          if (q < st.contact_cap) st.contacts[(int64_t)c * st.contact_cap + q] = make_int2((int)s, j);
-          else set_status(st.status, EDM_STATUS_CONTACT_CAP);
-        }
-      }
+      contact_candidate<F64>(p, g, st, L, s, j, dcx, dcy, rx, pmask, oi_pre, oi_post, cxs, cys,
+                             [&](int c, int e, int sub) { S(st, c, e, sub); });
     });
   });
-  __syncthreads();
-  if (threadIdx.x < L.n_cat) {
-    const int n = nbuf[threadIdx.x] < per ? nbuf[threadIdx.x] : per;
-    base[threadIdx.x] = n > 0 ? atomicAdd(&st.contact_count[threadIdx.x], n) : 0;
-  }
-  __syncthreads();
-  for (int c = 0; c < L.n_cat; ++c) {
-    const int n = nbuf[c] < per ? nbuf[c] : per;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-      const int64_t q = (int64_t)base[c] + k;
-      if (q < st.contact_cap) st.contacts[(int64_t)c * st.contact_cap + q] = buf[c * per + k];
-      else set_status(st.status, EDM_STATUS_CONTACT_CAP);
-    }
-  }
+  flush_contacts(st, L, S, base);
 }
 
-// The same contact search with the work spread over (enzyme, neighbour
-// column) tasks: a warp compacts its enzymes as sweep4 does, then each lane
-// takes tasks t = lane, lane + 32, ... (enzyme t / 3, column t % 3 - 1) and
+// The same contact search with the work spread over (sweeper, neighbour
+// column) tasks: a warp compacts its sweepers as sweep4 does, then each lane
+// takes tasks t = lane, lane + 32, ... (sweeper t / 3, column t % 3 - 1) and
 // walks that column's one or two slot runs.  A lane's loop is about three
 // candidates instead of nine, so lanes idle less while the longest run
 // finishes.  Same tests, same contact set (in another order, which the
@@ -986,13 +1023,13 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contacts_cols(const EdmDynPara
   __shared__ int2 buf[kContactSmem];
   __shared__ int nbuf[EDM_MAX_CAT], base[EDM_MAX_CAT];
   __shared__ int32_t list[kBlock / 32][kSweepChunk];
-  const int per = L.n_cat > 0 ? kContactSmem / L.n_cat : kContactSmem;
+  const ContactStage S{buf, nbuf, L.n_cat > 0 ? kContactSmem / L.n_cat : kContactSmem};
   if (threadIdx.x < EDM_MAX_CAT) nbuf[threadIdx.x] = 0;
   __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) * 4;
   int n = 0, r0 = 0;
-  if (w0 < st.n_slots) {  // whole warps: compact the chunk's enzymes
+  if (w0 < st.n_slots) {  // whole warps: compact the chunk's sweepers
     const int64_t s0 = w0 + (int64_t)lane * 4;
     uchar4 f4 = make_uchar4(0, 0, 0, 0);
     if (s0 < st.n_slots) f4 = *reinterpret_cast<const uchar4*>(st.flags + s0);
@@ -1016,7 +1053,7 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contacts_cols(const EdmDynPara
     const EdmDynParams& p = P[r];
     const Geo g(p);
     const int sps = fl_species(st.flags[s]);
-    const uint32_t rmask = L.reactions_of[sps], pmask = L.partners_of[sps];
+    const uint32_t rx = L.sweep_rx[sps], pmask = L.sweep_partners[sps];
     float2 oi_pre = make_float2(0.f, 0.f), oi_post = make_float2(0.f, 0.f);
     int cxs = 0, cys = 0;
     if constexpr (!F64) {
@@ -1025,58 +1062,57 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contacts_cols(const EdmDynPara
       split_cell(st.cell_post[s], g, cxs, cys);
     }
     for_neighbour_slots_box(g, st, st.cell_pre[s], dcx, dcx, -1, 1, [&](int j, int, int dcx_, int dcy) {
-      if (j == s) return;
-      const uint8_t fj = st.flags[j];
-      const int spj = fl_species(fj);
-      if (!fl_alive(fj) || !((pmask >> spj) & 1u)) return;
-      double d2;
-      if constexpr (F64) {
-        if (!(sep_sq<F64>(st.pos_pre, st.cell_pre, s, j, g) < g.cutoff_sq)) return;
-        d2 = sep_sq<F64>(st.pos_post, st.cell_post, s, j, g);
-      } else {
-        const float2 oj = ((const float2*)st.pos_pre)[j];
-        const float fdx = -(float)dcx_ * g.sxf + (oi_pre.x - oj.x);
-        const float fdy = -(float)dcy * g.syf + (oi_pre.y - oj.y);
-        if (!((double)(fdx * fdx + fdy * fdy) < g.cutoff_sq)) return;
-        float dx, dy;
-        d2 = (double)rel_sq_f32_xy(cxs, cys, oi_post, st.cell_post[j], ((const float2*)st.pos_post)[j], g, dx, dy);
-      }
-      for (uint32_t bits = rmask; bits; bits &= bits - 1) {
-        const int c = __ffs(bits) - 1;
-        if (!((L.capable[c] >> spj) & 1u) || d2 > p.cat[c].contact_sq) continue;
-        const int k = atomicAdd(&nbuf[c], 1);
-        if (k < per) {
-          buf[c * per + k] = make_int2((int)s, j);
-        } else {
-          const int qq = atomicAdd(&st.contact_count[c], 1);
-          if (qq < st.contact_cap) st.contacts[(int64_t)c * st.contact_cap + qq] = make_int2((int)s, j);
-          else set_status(st.status, EDM_STATUS_CONTACT_CAP);
-        }
-      }
+      contact_candidate<F64>(p, g, st, L, s, j, dcx_, dcy, rx, pmask, oi_pre, oi_post, cxs, cys,
+                             [&](int c, int e, int sub) { S(st, c, e, sub); });
     });
   }
-  __syncthreads();
-  if (threadIdx.x < L.n_cat) {
-    const int nn = nbuf[threadIdx.x] < per ? nbuf[threadIdx.x] : per;
-    base[threadIdx.x] = nn > 0 ? atomicAdd(&st.contact_count[threadIdx.x], nn) : 0;
-  }
-  __syncthreads();
-  for (int c = 0; c < L.n_cat; ++c) {
-    const int nn = nbuf[c] < per ? nbuf[c] : per;
-    for (int k = threadIdx.x; k < nn; k += blockDim.x) {
-      const int64_t qq = (int64_t)base[c] + k;
-      if (qq < st.contact_cap) st.contacts[(int64_t)c * st.contact_cap + qq] = buf[c * per + k];
+  flush_contacts(st, L, S, base);
+}
+
+// Late pairs of particle j, which a catalytic pass has just turned into the
+// substrate of the later reactions `late`: its alive neighbours of those
+// reactions' enzyme species passing the tests an enzyme-side sweep makes
+// (j seen from enzyme e at the opposite cell offset, the same float32
+// expressions), appended to the reactions' lists.
+template <bool F64>
+__device__ __noinline__ void late_contacts(const EdmDynParams& p, const Geo& g, const DevState& st, int64_t j,
+                                           uint32_t late) {
+  uint32_t emask = 0;
+  for (uint32_t b = late; b; b &= b - 1) emask |= 1u << p.cat[__ffs(b) - 1].enzyme;
+  for_neighbour_slots(g, st, st.cell_pre[j], [&](int e, int, int dcx, int dcy) {
+    if (e == j) return;
+    const uint8_t fe = st.flags[e];
+    const int spe = fl_species(fe);
+    if (!fl_alive(fe) || !((emask >> spe) & 1u)) return;
+    double d2;
+    if constexpr (F64) {
+      if (!(sep_sq<F64>(st.pos_pre, st.cell_pre, e, j, g) < g.cutoff_sq)) return;
+      d2 = sep_sq<F64>(st.pos_post, st.cell_post, e, j, g);
+    } else {
+      const float2 oe = ((const float2*)st.pos_pre)[e], oj = ((const float2*)st.pos_pre)[j];
+      const float fdx = -(float)(-dcx) * g.sxf + (oe.x - oj.x);
+      const float fdy = -(float)(-dcy) * g.syf + (oe.y - oj.y);
+      if (!((double)(fdx * fdx + fdy * fdy) < g.cutoff_sq)) return;
+      d2 = sep_sq<F64>(st.pos_post, st.cell_post, e, j, g);
+    }
+    for (uint32_t b = late; b; b &= b - 1) {
+      const int c = __ffs(b) - 1;
+      if (spe != p.cat[c].enzyme || d2 > p.cat[c].contact_sq) continue;
+      const int q = atomicAdd(&st.contact_count[c], 1);
+      if (q < st.contact_cap) st.contacts[(int64_t)c * st.contact_cap + q] = make_int2(e, (int)j);
       else set_status(st.status, EDM_STATUS_CONTACT_CAP);
     }
-  }
+  });
 }
 
 // Catalytic pass c (dynamics.py:825-983) over its contact list: the set of
 // substrates with at least one accepted (enzyme, substrate) pair converts.
 // Every listed pair is alive, has the pass's enzyme and is within its contact
 // radius; only the partner's current species is left to test.
+// `late`: the later reactions whose substrate is this pass's product.
 template <bool F64>
-__global__ void __launch_bounds__(kBlock, 8) k_catalytic(const EdmDynParams* __restrict__ P, DevState st, int cidx) {
+__global__ void __launch_bounds__(kBlock, 8) k_catalytic(const EdmDynParams* __restrict__ P, DevState st, int cidx,
+                                                       uint32_t late) {
   const int n = st.contact_count[cidx];
   const int lim = (int64_t)n < st.contact_cap ? n : (int)st.contact_cap;
   const int2* list = st.contacts + (int64_t)cidx * st.contact_cap;
@@ -1103,6 +1139,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_catalytic(const EdmDynParams* __r
       if (cas_u8(&st.flags[es.y], fs, fl_make(C.product, true))) {
         atomic_add_i64(&st.counters[(int64_t)r * EDM_NCOUNTERS + EDM_C_CATALYTIC], 1);
         grid_change(p, st.grid_delta, C.substrate, true, C.product, true, xs, ys);
+        if (late) late_contacts<F64>(p, g, st, es.y, late);
       }
     }
   }

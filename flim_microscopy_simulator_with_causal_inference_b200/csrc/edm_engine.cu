@@ -162,6 +162,8 @@ struct EdmEngine {
   int64_t contact_cap = 0;
   uint32_t enzyme_mask = 0;
   CatLists cat_lists{};
+  uint32_t cat_late[EDM_MAX_CAT] = {};
+  bool contact_sides_counted = false;  // sides chosen from a state's species counts
   int64_t* rep_first = nullptr;
   int32_t* chunk_rep = nullptr;  // replica of the first slot of each 128-slot chunk
   int32_t *moved = nullptr, *moved_count = nullptr;
@@ -307,21 +309,18 @@ struct EdmEngine {
     if (p.n_cat > 0) {
       enzyme_mask = 0;
       uint32_t touched = 0;
-      cat_lists = CatLists{};
-      cat_lists.n_cat = p.n_cat;
       for (int c = 0; c < p.n_cat; ++c) {
         enzyme_mask |= 1u << p.cat[c].enzyme;
         touched |= (1u << p.cat[c].substrate) | (1u << p.cat[c].product);
-        // species that earlier passes of the step can turn into this substrate
-        uint32_t capable = 1u << p.cat[c].substrate;
-        for (int c2 = c - 1; c2 >= 0; --c2)
-          if ((capable >> p.cat[c2].product) & 1u) capable |= 1u << p.cat[c2].substrate;
-        cat_lists.capable[c] = capable;
-        cat_lists.reactions_of[p.cat[c].enzyme] |= 1u << c;
+        // the later reactions whose substrate this pass's product is: a
+        // particle it converts gets its late pairs for them at once
+        cat_late[c] = 0;
+        for (int c2 = c + 1; c2 < p.n_cat; ++c2)
+          if (p.cat[c2].substrate == p.cat[c].product) cat_late[c] |= 1u << c2;
       }
-      for (int c = 0; c < p.n_cat; ++c) cat_lists.partners_of[p.cat[c].enzyme] |= cat_lists.capable[c];
       if (enzyme_mask & touched) return fail(EDM_EUNSUP, "an enzyme species is also a catalytic substrate/product");
-      passes.push_back({P_CONTACTS, 0, Match{{0u, enzyme_mask}}});
+      passes.push_back({P_CONTACTS, 0, Match{{0u, 0u}}});
+      set_contact_sides(nullptr);
     }
     // A pass whose probability is zero in every replica changes nothing (its
     // keyed draws feed no other pass), so it is not scheduled.
@@ -357,6 +356,29 @@ struct EdmEngine {
       writes({p.conv[v].from, p.conv[v].to});
     }
     return fuse_particle_passes();
+  }
+
+  // Which side of each catalytic reaction sweeps for its direct contact
+  // pairs: the species with fewer alive particles (count[sp], summed over
+  // the replicas; the enzyme side without counts).  Both sides find the same
+  // pairs, so this choice changes only the work.
+  void set_contact_sides(const int64_t* count) {
+    const EdmDynParams& p = hdp[0];
+    cat_lists = CatLists{};
+    cat_lists.n_cat = p.n_cat;
+    uint32_t sweepers = 0;
+    for (int c = 0; c < p.n_cat; ++c) {
+      const int e = p.cat[c].enzyme, sub = p.cat[c].substrate;
+      const bool from_enzyme = !count || count[e] <= count[sub];
+      const int sw = from_enzyme ? e : sub, other = from_enzyme ? sub : e;
+      if (from_enzyme) cat_lists.from_enzyme |= 1u << c;
+      cat_lists.other[c] = other;
+      cat_lists.sweep_rx[sw] |= 1u << c;
+      cat_lists.sweep_partners[sw] |= 1u << other;
+      sweepers |= 1u << sw;
+    }
+    for (Pass& ps : passes)
+      if (ps.kind == P_CONTACTS) ps.match = Match{{0u, sweepers}};
   }
 
   // The per-particle passes (recruitment candidates, detachments,
@@ -602,7 +624,7 @@ struct EdmEngine {
           launch_contacts<F64>(st, ps.match, sgrid, s);
           tune_mark(TK_CONTACTS, 1, s);
           break;
-        case P_CAT: k_catalytic<F64><<<cgrid, kBlock, 0, s>>>(dp, st, ps.index); break;
+        case P_CAT: k_catalytic<F64><<<cgrid, kBlock, 0, s>>>(dp, st, ps.index, cat_late[ps.index]); break;
         case P_REC_APPLY:
           k_recruit_apply<F64><<<rb, 128, 0, s>>>(dp, R, st, ps.index, d_draw, rec_after[ps.index]);
           break;
@@ -1193,6 +1215,17 @@ int edm_set_state(EdmEngine* E, const EdmHostState* st, void* stream) {
   CUDA_TRY(cudaMemcpyAsync(E->ctmc, st->ctmc_state, N, cudaMemcpyHostToDevice, s));
   CUDA_TRY(cudaMemcpyAsync(E->bleached, st->is_bleached, N, cudaMemcpyHostToDevice, s));
   CUDA_TRY(cudaMemsetAsync(E->cnt, 0, sizeof(int32_t) * (E->n_cells > 0 ? E->n_cells : 1), s));
+  if (!E->contact_sides_counted && E->hdp[0].n_cat > 0) {
+    // the contact sweep's sides from the first state's alive species counts
+    int64_t count[EDM_MAX_SPECIES] = {};
+    for (int64_t i = 0; i < N; ++i) {
+      const int32_t sp = st->species_id[i];
+      if (st->is_alive[i] && sp >= 0 && sp < EDM_MAX_SPECIES) ++count[sp];
+    }
+    E->set_contact_sides(count);
+    E->drop_graphs();
+    E->contact_sides_counted = true;
+  }
   if (E->npblk > 0) {
     if (E->f64)
       k_set_state<true><<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, dpos, E->st_sp, E->st_alive, E->pos_post, E->lo_post,
