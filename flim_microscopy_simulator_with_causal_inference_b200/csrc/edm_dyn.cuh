@@ -900,8 +900,12 @@ __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restric
 // * late pairs, whose partner an earlier catalytic pass of the step turns
 //   into S_c, are few: the pass that converts a particle looks up its
 //   enzymes of the later reactions at once (late_contacts).
-// A pair can be filed twice (a partner converted away and back); the passes
-// accept a substrate once, so duplicates change nothing.
+// A late pair is filed only when its keyed draw for the pass lies below the
+// pass's threshold (the pass rejects it otherwise); the sweep files every
+// direct pair and leaves the draws to the passes (a Philox per pair inside
+// the sweep measured slower).  A pair can be filed twice (a partner converted
+// away and back); the passes accept a substrate once, so duplicates change
+// nothing.
 constexpr int kContactSmem = 2048;
 
 struct CatLists {
@@ -912,6 +916,15 @@ struct CatLists {
   int n_cat;
 };
 
+// Whether pass c's keyed draw for the pair of local ids (a, b) of replica r
+// lies below the pass's threshold.  The pass rejects the pair otherwise,
+// whatever the state, so a pair whose draw fails is not filed.
+__device__ __forceinline__ bool cat_draw_passes(const EdmDynParams& p, const DevState& st, int r, int c, int a,
+                                                int b, int64_t step) {
+  const uint32_t lo = a < b ? a : b, hi = a < b ? b : a;
+  return draw_u53(p.seed, step, EDM_S_CAT + c, lo, hi) < st.cat_thr[(int64_t)r * EDM_MAX_CAT + c];
+}
+
 // One neighbour j (pre-move cell offset dcx, dcy) of sweeper s: the pair
 // tests, then stage(c, enzyme, substrate) for each reaction of rx it meets.
 // oi_pre / oi_post / (cxs, cys): the sweeper's float32 offsets and post-move
@@ -919,8 +932,8 @@ struct CatLists {
 template <bool F64, typename Stage>
 __device__ __forceinline__ void contact_candidate(const EdmDynParams& p, const Geo& g, const DevState& st,
                                                   const CatLists& L, int64_t s, int j, int dcx, int dcy,
-                                                  uint32_t rx, uint32_t pmask, float2 oi_pre, float2 oi_post,
-                                                  int cxs, int cys, Stage stage) {
+                                                  uint32_t rx, uint32_t pmask,
+                                                  float2 oi_pre, float2 oi_post, int cxs, int cys, Stage stage) {
   if (j == s) return;
   const uint8_t fj = st.flags[j];
   const int spj = fl_species(fj);
@@ -1075,8 +1088,8 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contacts_cols(const EdmDynPara
 // (j seen from enzyme e at the opposite cell offset, the same float32
 // expressions), appended to the reactions' lists.
 template <bool F64>
-__device__ __noinline__ void late_contacts(const EdmDynParams& p, const Geo& g, const DevState& st, int64_t j,
-                                           uint32_t late) {
+__device__ __forceinline__ void late_contacts(const EdmDynParams& p, const Geo& g, const DevState& st, int r,
+                                           int64_t j, int id_j, int64_t step, uint32_t late) {
   uint32_t emask = 0;
   for (uint32_t b = late; b; b &= b - 1) emask |= 1u << p.cat[__ffs(b) - 1].enzyme;
   for_neighbour_slots(g, st, st.cell_pre[j], [&](int e, int, int dcx, int dcy) {
@@ -1098,6 +1111,7 @@ __device__ __noinline__ void late_contacts(const EdmDynParams& p, const Geo& g, 
     for (uint32_t b = late; b; b &= b - 1) {
       const int c = __ffs(b) - 1;
       if (spe != p.cat[c].enzyme || d2 > p.cat[c].contact_sq) continue;
+      if (!cat_draw_passes(p, st, r, c, st.ids[e] - (int)g.poff, id_j, step)) continue;
       const int q = atomicAdd(&st.contact_count[c], 1);
       if (q < st.contact_cap) st.contacts[(int64_t)c * st.contact_cap + q] = make_int2(e, (int)j);
       else set_status(st.status, EDM_STATUS_CONTACT_CAP);
@@ -1111,7 +1125,7 @@ __device__ __noinline__ void late_contacts(const EdmDynParams& p, const Geo& g, 
 // radius; only the partner's current species is left to test.
 // `late`: the later reactions whose substrate is this pass's product.
 template <bool F64>
-__global__ void __launch_bounds__(kBlock, 8) k_catalytic(const EdmDynParams* __restrict__ P, DevState st, int cidx,
+__global__ void __launch_bounds__(kBlock, 4) k_catalytic(const EdmDynParams* __restrict__ P, DevState st, int cidx,
                                                        uint32_t late) {
   const int n = st.contact_count[cidx];
   const int lim = (int64_t)n < st.contact_cap ? n : (int)st.contact_cap;
@@ -1139,7 +1153,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_catalytic(const EdmDynParams* __r
       if (cas_u8(&st.flags[es.y], fs, fl_make(C.product, true))) {
         atomic_add_i64(&st.counters[(int64_t)r * EDM_NCOUNTERS + EDM_C_CATALYTIC], 1);
         grid_change(p, st.grid_delta, C.substrate, true, C.product, true, xs, ys);
-        if (late) late_contacts<F64>(p, g, st, es.y, late);
+        if (late) late_contacts<F64>(p, g, st, r, es.y, ids, *st.d_step, late);
       }
     }
   }
