@@ -88,6 +88,9 @@ struct DevState {
   int4* pl;
   int32_t* pl_count;
   int32_t* pl_index;
+  // the contact search's sweepers of this step (k_sweep_list), block by block
+  int32_t* sw_list;
+  int32_t* sw_count;
   // per global grid cell: the adaptation field w (float64, on the adaptation
   // grid's cells) and the local-recruitment CDF (on a feedback grid's cells)
   double* adapt_w;
@@ -477,12 +480,12 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int& total) {
 // their deltas, the placed-after-sort and contact counters, the draw list
 // length): cleared by the first scan kernel instead of one memset each.
 struct StepZero {
-  int32_t* p[5];
-  int64_t n[5];
+  int32_t* p[6];
+  int64_t n[6];
 };
 
 __global__ void k_scan_reduce(const int32_t* __restrict__ cnt, int64_t n, int32_t* __restrict__ bsum, StepZero z) {
-  for (int k = 0; k < 5; ++k)
+  for (int k = 0; k < 6; ++k)
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < z.n[k]; i += (int64_t)gridDim.x * blockDim.x)
       z.p[k][i] = 0;
   const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
@@ -1023,13 +1026,37 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contacts(const EdmDynParams* _
   flush_contacts(st, L, S, base);
 }
 
+// The per-sweeper work of the column-task contact search: sweeper s, its
+// neighbour column dcx (-1, 0, 1); r0 is a replica at or before s's.
+template <bool F64, typename Stage>
+__device__ __forceinline__ void contact_column_task(const EdmDynParams* __restrict__ P, const DevState& st,
+                                                    const CatLists& L, int64_t s, int dcx, int r0, Stage stage) {
+  int r = r0;
+  while (r + 1 < st.n_rep && st.rep_first[r + 1] <= s) ++r;
+  const EdmDynParams& p = P[r];
+  const Geo g(p);
+  const int sps = fl_species(st.flags[s]);
+  const uint32_t rx = L.sweep_rx[sps], pmask = L.sweep_partners[sps];
+  float2 oi_pre = make_float2(0.f, 0.f), oi_post = make_float2(0.f, 0.f);
+  int cxs = 0, cys = 0;
+  if constexpr (!F64) {
+    oi_pre = ((const float2*)st.pos_pre)[s];
+    oi_post = ((const float2*)st.pos_post)[s];
+    split_cell(st.cell_post[s], g, cxs, cys);
+  }
+  for_neighbour_slots_box(g, st, st.cell_pre[s], dcx, dcx, -1, 1, [&](int j, int, int dcx_, int dcy) {
+    contact_candidate<F64>(p, g, st, L, s, j, dcx_, dcy, rx, pmask, oi_pre, oi_post, cxs, cys, stage);
+  });
+}
+
 // The same contact search with the work spread over (sweeper, neighbour
-// column) tasks: a warp compacts its sweepers as sweep4 does, then each lane
-// takes tasks t = lane, lane + 32, ... (sweeper t / 3, column t % 3 - 1) and
-// walks that column's one or two slot runs.  A lane's loop is about three
-// candidates instead of nine, so lanes idle less while the longest run
-// finishes.  Same tests, same contact set (in another order, which the
-// catalytic passes do not depend on).
+// column) tasks: a warp compacts the sweepers of its kSweepChunk slots in
+// shared memory (as sweep4 does), then each lane takes tasks t = lane,
+// lane + 32, ... (sweeper t / 3, column t % 3 - 1) and walks that column's
+// one or two slot runs.  A lane's loop is about three candidates instead of
+// nine, so lanes idle less while the longest run finishes.  Same tests, same
+// contact set (in another order, which the catalytic passes do not depend
+// on).
 template <bool F64, int MINB>
 __global__ void __launch_bounds__(kBlock, MINB) k_contacts_cols(const EdmDynParams* __restrict__ P, DevState st,
                                                               Match m, CatLists L) {
@@ -1059,25 +1086,118 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contacts_cols(const EdmDynPara
   }
   __syncwarp();
   for (int t = lane; t < 3 * n; t += 32) {
-    const int q = t / 3, dcx = t - 3 * q - 1;
-    const int64_t s = list[wid][q];
-    int r = r0;
-    while (r + 1 < st.n_rep && st.rep_first[r + 1] <= s) ++r;
-    const EdmDynParams& p = P[r];
-    const Geo g(p);
-    const int sps = fl_species(st.flags[s]);
-    const uint32_t rx = L.sweep_rx[sps], pmask = L.sweep_partners[sps];
-    float2 oi_pre = make_float2(0.f, 0.f), oi_post = make_float2(0.f, 0.f);
-    int cxs = 0, cys = 0;
-    if constexpr (!F64) {
-      oi_pre = ((const float2*)st.pos_pre)[s];
-      oi_post = ((const float2*)st.pos_post)[s];
-      split_cell(st.cell_post[s], g, cxs, cys);
-    }
-    for_neighbour_slots_box(g, st, st.cell_pre[s], dcx, dcx, -1, 1, [&](int j, int, int dcx_, int dcy) {
-      contact_candidate<F64>(p, g, st, L, s, j, dcx_, dcy, rx, pmask, oi_pre, oi_post, cxs, cys,
+    const int q = t / 3;
+    contact_column_task<F64>(P, st, L, list[wid][q], t - 3 * q - 1, r0,
                              [&](int c, int e, int sub) { S(st, c, e, sub); });
-    });
+  }
+  flush_contacts(st, L, S, base);
+}
+
+// Block compaction of the slots matching m among the block's kBlock * SPT
+// slots from b0 (SPT per thread, in slot order per thread): writes them to
+// list (kBlock * SPT entries of shared memory) and returns their number.
+// Every thread of the block calls it.
+template <int SPT>
+__device__ __forceinline__ int block_compact(const DevState& st, const Match& m, int64_t b0, int32_t* list,
+                                             int* woff) {
+  static_assert(SPT == 4 || SPT == 16, "4 or 16 slots per thread");
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int64_t s0 = b0 + (int64_t)threadIdx.x * SPT;
+  uint8_t fl[SPT];
+  if (s0 + SPT <= st.n_slots) {  // s0 and SPT are multiples of SPT bytes: aligned
+    if constexpr (SPT == 16) {
+      const uint4 v = *reinterpret_cast<const uint4*>(st.flags + s0);
+      const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int k = 0; k < 16; ++k) fl[k] = (uint8_t)(w[k >> 2] >> (8 * (k & 3)));
+    } else {
+      const uchar4 f4 = *reinterpret_cast<const uchar4*>(st.flags + s0);
+      fl[0] = f4.x, fl[1] = f4.y, fl[2] = f4.z, fl[3] = f4.w;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < SPT; ++k) fl[k] = s0 + k < st.n_slots ? st.flags[s0 + k] : (uint8_t)0;
+  }
+  unsigned hits = 0;  // bit k: slot s0 + k matches
+#pragma unroll
+  for (int k = 0; k < SPT; ++k)
+    if (s0 + k < st.n_slots && matches(fl[k], m)) hits |= 1u << k;
+  int wn = 0;
+#pragma unroll
+  for (int k = 0; k < SPT; ++k) wn += __popc(__ballot_sync(0xffffffffu, (hits >> k) & 1u));
+  if (lane == 0) woff[wid + 1] = wn;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    woff[0] = 0;
+    for (int w = 1; w <= kBlock / 32; ++w) woff[w] += woff[w - 1];
+  }
+  __syncthreads();
+  const unsigned below = (1u << lane) - 1u;
+  int at = woff[wid];
+#pragma unroll
+  for (int k = 0; k < SPT; ++k) {
+    const bool hit = (hits >> k) & 1u;
+    const unsigned bits = __ballot_sync(0xffffffffu, hit);
+    if (hit) list[at + __popc(bits & below)] = (int32_t)(s0 + k);
+    at += __popc(bits);
+  }
+  __syncthreads();
+  return woff[kBlock / 32];
+}
+
+// The contact search's sweepers as one global list: each block compacts its
+// kBlock * 16 slots and appends them with one atomic (launch with
+// ceil(n_slots / (16 kBlock)) blocks of kBlock).
+__global__ void __launch_bounds__(kBlock) k_sweep_list(DevState st, Match m) {
+  __shared__ int32_t list[kBlock * 16];
+  __shared__ int woff[kBlock / 32 + 1];
+  __shared__ int at;
+  const int n = block_compact<16>(st, m, (int64_t)blockIdx.x * kBlock * 16, list, woff);
+  if (threadIdx.x == 0) at = n > 0 ? atomicAdd(st.sw_count, n) : 0;
+  __syncthreads();
+  for (int k = threadIdx.x; k < n; k += blockDim.x) st.sw_list[at + k] = list[k];
+}
+
+// The column tasks over the global sweeper list, one wave of blocks walking
+// the tasks grid-stride: every lane has a task however the sweepers cluster.
+template <bool F64, int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) k_contacts_list(const EdmDynParams* __restrict__ P, DevState st,
+                                                              CatLists L) {
+  __shared__ int2 buf[kContactSmem];
+  __shared__ int nbuf[EDM_MAX_CAT], base[EDM_MAX_CAT];
+  const ContactStage S{buf, nbuf, L.n_cat > 0 ? kContactSmem / L.n_cat : kContactSmem};
+  if (threadIdx.x < EDM_MAX_CAT) nbuf[threadIdx.x] = 0;
+  __syncthreads();
+  const int64_t tasks = 3 * (int64_t)*st.sw_count;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < tasks; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t q = t / 3;
+    const int64_t s = st.sw_list[q];
+    contact_column_task<F64>(P, st, L, s, (int)(t - 3 * q) - 1, st.chunk_rep[s / kSweepChunk],
+                             [&](int c, int e, int sub) { S(st, c, e, sub); });
+  }
+  flush_contacts(st, L, S, base);
+}
+
+// The column tasks balanced over the whole block: the block compacts the
+// sweepers of its kBlock * SPT slots (SPT per thread) into one shared list,
+// so a warp whose slots hold a cluster of sweepers shares them with the
+// block's other warps instead of keeping the block waiting.
+template <bool F64, int MINB, int SPT>
+__global__ void __launch_bounds__(kBlock, MINB) k_contacts_block(const EdmDynParams* __restrict__ P, DevState st,
+                                                               Match m, CatLists L) {
+  __shared__ int2 buf[kContactSmem];
+  __shared__ int nbuf[EDM_MAX_CAT], base[EDM_MAX_CAT];
+  __shared__ int32_t list[kBlock * SPT];
+  __shared__ int woff[kBlock / 32 + 1];
+  const ContactStage S{buf, nbuf, L.n_cat > 0 ? kContactSmem / L.n_cat : kContactSmem};
+  if (threadIdx.x < EDM_MAX_CAT) nbuf[threadIdx.x] = 0;
+  const int64_t b0 = (int64_t)blockIdx.x * blockDim.x * SPT;
+  const int n = block_compact<SPT>(st, m, b0, list, woff);  // its barriers also publish nbuf
+  const int r0 = n > 0 ? st.chunk_rep[b0 / kSweepChunk] : 0;
+  for (int t = threadIdx.x; t < 3 * n; t += blockDim.x) {
+    const int q = t / 3;
+    contact_column_task<F64>(P, st, L, list[q], t - 3 * q - 1, r0,
+                             [&](int c, int e, int sub) { S(st, c, e, sub); });
   }
   flush_contacts(st, L, S, base);
 }

@@ -74,13 +74,18 @@ struct LaunchShape {
   int block, min_blocks;
 };
 enum TunedKernel { TK_SCATTER = 0, TK_MOVE = 1, TK_CONTACTS = 2, TK_COUNT = 3 };
-constexpr int kMaxShapes = 6;
+constexpr int kMaxShapes = 8;
 constexpr LaunchShape kShapes[TK_COUNT][kMaxShapes] = {
-    {{256, 1}, {128, 1}, {512, 1}, {0, 0}, {0, 0}, {0, 0}},      // k_scatter
-    {{256, 3}, {256, 4}, {128, 8}, {256, 1}, {512, 1}, {128, 5}},  // k_move
-    {{256, 6}, {256, 4}, {256, 8}, {256, 6}, {256, 4}, {0, 0}},  // k_contacts (3, 4: by neighbour column)
+    {{256, 1}, {128, 1}, {512, 1}},                                // k_scatter
+    // k_move: the second number bounds its registers (80 at 256 x 3 down to 32
+    // at 128 x 16, with spills below 64): occupancy pays more than the spills
+    {{256, 3}, {256, 4}, {128, 8}, {128, 10}, {128, 12}, {128, 16}, {256, 6}, {256, 8}},
+    // k_contacts: 0 by sweeper; 1-2 by (sweeper, neighbour column) per warp;
+    // 3-5 the same tasks balanced over the block (16, 16, 4 slots per
+    // thread); 6-7 over a global sweeper list (k_sweep_list), one wave
+    {{256, 6}, {256, 6}, {256, 4}, {256, 6}, {256, 4}, {256, 6}, {256, 6}, {256, 8}},
 };
-constexpr int kNumShapes[TK_COUNT] = {3, 6, 5};
+constexpr int kNumShapes[TK_COUNT] = {3, 8, 8};
 const char* const kTunedNames[TK_COUNT] = {"k_scatter", "k_move", "k_contacts"};
 constexpr int kTileSizes[3] = {128, 256, 512};
 int tile_index(int bs) { return bs == 128 ? 0 : (bs == 256 ? 1 : 2); }
@@ -169,6 +174,7 @@ struct EdmEngine {
   int32_t *moved = nullptr, *moved_count = nullptr;
   int4* pl = nullptr;  // listed particles of the per-particle passes: (slot, pass bits, replica, id)
   int32_t *pl_count = nullptr, *pl_index = nullptr;
+  int32_t *sw_list = nullptr, *sw_count = nullptr;  // the contact search's sweeper list
   double *adapt_w = nullptr, *local_cdf = nullptr;  // per global grid cell
   std::vector<int32_t> emit_host;  // emitter list last uploaded
   std::vector<uint8_t> has_dye_host;  // has_dye of the last edm_set_state
@@ -223,6 +229,8 @@ struct EdmEngine {
     s.pl = pl;
     s.pl_count = pl_count;
     s.pl_index = pl_index;
+    s.sw_list = sw_list;
+    s.sw_count = sw_count;
     s.adapt_w = adapt_w;
     s.local_cdf = local_cdf;
     s.n_rep = R;
@@ -565,20 +573,31 @@ struct EdmEngine {
     switch (v) {  // the rows of kShapes[TK_MOVE]
       case 1: k_move<F64, 256, 4><<<n, 256, 0, s>>>(dp, b, st); break;
       case 2: k_move<F64, 128, 8><<<n, 128, 0, s>>>(dp, b, st); break;
-      case 3: k_move<F64, 256, 1><<<n, 256, 0, s>>>(dp, b, st); break;
-      case 4: k_move<F64, 512, 1><<<n, 512, 0, s>>>(dp, b, st); break;
-      case 5: k_move<F64, 128, 5><<<n, 128, 0, s>>>(dp, b, st); break;
+      case 3: k_move<F64, 128, 10><<<n, 128, 0, s>>>(dp, b, st); break;
+      case 4: k_move<F64, 128, 12><<<n, 128, 0, s>>>(dp, b, st); break;
+      case 5: k_move<F64, 128, 16><<<n, 128, 0, s>>>(dp, b, st); break;
+      case 6: k_move<F64, 256, 6><<<n, 256, 0, s>>>(dp, b, st); break;
+      case 7: k_move<F64, 256, 8><<<n, 256, 0, s>>>(dp, b, st); break;
       default: k_move<F64, 256, 3><<<n, 256, 0, s>>>(dp, b, st); break;
     }
   }
 
   template <bool F64>
   void launch_contacts(const DevState& st, const Match& m, int grid, cudaStream_t s) {
+    const int grid16 = (int)((N + 16 * kBlock - 1) / (16 * kBlock));  // 16 slots per thread
+    if (grid16 == 0) return;
     switch (shape[TK_CONTACTS]) {  // the rows of kShapes[TK_CONTACTS]
-      case 1: k_contacts<F64, 4><<<grid, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
-      case 2: k_contacts<F64, 8><<<grid, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
-      case 3: k_contacts_cols<F64, 6><<<grid, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
-      case 4: k_contacts_cols<F64, 4><<<grid, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
+      case 1: k_contacts_cols<F64, 6><<<grid, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
+      case 2: k_contacts_cols<F64, 4><<<grid, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
+      case 3: k_contacts_block<F64, 6, 16><<<grid16, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
+      case 4: k_contacts_block<F64, 4, 16><<<grid16, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
+      case 5: k_contacts_block<F64, 6, 4><<<grid, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
+      case 6:
+      case 7:
+        k_sweep_list<<<grid16, kBlock, 0, s>>>(st, m);
+        if (shape[TK_CONTACTS] == 6) k_contacts_list<F64, 6><<<148 * 6, kBlock, 0, s>>>(dp, st, cat_lists);
+        else k_contacts_list<F64, 8><<<148 * 8, kBlock, 0, s>>>(dp, st, cat_lists);
+        break;
       default: k_contacts<F64, 6><<<grid, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
     }
   }
@@ -593,6 +612,7 @@ struct EdmEngine {
     z.p[2] = moved_count, z.n[2] = R;
     z.p[3] = contact_count, z.n[3] = contact_count ? EDM_MAX_CAT : 0;
     z.p[4] = pl_count, z.n[4] = pl_count ? 1 : 0;
+    z.p[5] = sw_count, z.n[5] = sw_count ? 1 : 0;
     k_scan_reduce<<<nbs, kScanThreads, 0, s>>>(cnt, n_cells, bsum, z);
     k_scan_bsum<<<1, 1024, 0, s>>>(bsum, nbs);
     k_scan_down<<<nbs, kScanThreads, 0, s>>>(cnt, n_cells, bsum, cell_start, cursor);
@@ -667,6 +687,8 @@ struct EdmEngine {
 
   int launches_per_step(bool with_photons) const {
     int n = 3 + 1 + 1 + (int)passes.size() + 1;
+    for (const Pass& ps : passes)  // the sweeper-list contact shapes launch two kernels
+      if (ps.kind == P_CONTACTS && shape[TK_CONTACTS] >= 6) ++n;
     if (with_photons) n += (neblk > 0 ? 3 : 1) + 1 + (nphblk > 0 ? 1 : 0) + 1;
     if (rec_cap > 0) n += 2 + ((has_phot && neblk > 0) ? 1 : 0);
     return n;
@@ -962,6 +984,8 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
   ALLOC(E->pl, (size_t)np);
   ALLOC(E->pl_count, 1);
   ALLOC(E->pl_index, (size_t)np);
+  ALLOC(E->sw_list, (size_t)np);
+  ALLOC(E->sw_count, 1);
   ALLOC(E->adapt_w, (size_t)std::max<int64_t>(ng, 1));
   ALLOC(E->local_cdf, (size_t)std::max<int64_t>(ng, 1));
   CUDA_TRY(cudaMemset(E->pl_index, 0xFF, sizeof(int32_t) * np));

@@ -21,7 +21,9 @@ def test_autotuned_engine_matches_default_shapes_bitwise():
     shapes = tuned.eng.autotune(2, retune=True, stream=s)
     s.synchronize()
     steps = tuned.eng.get_step()
-    assert steps == (3 + 6 + 5) * 3  # candidates of k_scatter, k_move, k_contacts x (1 + 2 timed) steps
+    # candidates of k_scatter, k_move, k_contacts (by sweeper, by neighbour column,
+    # over the move's sweeper list: no binding pass here) x (1 + 2 timed) steps
+    assert steps == (3 + 8 + 8) * 3
     for k, v in shapes.items():
         assert v["block"] in (128, 256, 512) and v["candidates"] >= 3, (k, v)
         assert 0.0 < v["tuned_ms"] <= v["default_ms"], (k, v)
