@@ -66,6 +66,9 @@ def parse():
     ap.add_argument("--no-flim", action="store_true")
     ap.add_argument("--no-large", action="store_true", help="skip the 1.3M-particle float32-vs-float64 comparison")
     ap.add_argument("--no-autotune", action="store_true", help="keep the fixed default launch shapes")
+    ap.add_argument("--shapes", default=None,
+                    help="launch-shape candidates of k_scatter,k_move,k_contacts instead of tuning (e.g. 1,5,7: "
+                         "a profiler run replays the shapes a plain run tuned)")
     return ap.parse_args()
 
 
@@ -286,7 +289,9 @@ def large_membrane_bench(device: int, stream) -> dict:
     ens = {prec: Ensemble([raw], precision=prec, photons=True, device=device) for prec in (32, 64)}
     n_mem = ens[32].total_membrane
     rates, counts = {}, {}
+    shapes = {}
     for prec, e in ens.items():
+        shapes[prec] = {k: v["candidate"] for k, v in e.engine.autotune(3, stream=stream).items()}
         e.engine.pipeline_steps(100, True, 100, stream=stream)  # capture + warm
         stream.synchronize()
         e.upload(stream=stream)  # back to the initial state, step 0
@@ -326,7 +331,8 @@ def large_membrane_bench(device: int, stream) -> dict:
             "lockstep_max_position_error_um": worst, "lockstep_event_sets_identical": same_events,
             "reaction_count_rel_deviation_100_steps": dev,
             "reaction_counts_100_steps": {"fp32": counts[32][2:6].tolist(), "fp64": counts[64][2:6].tolist(),
-                                          "fields": ["catalytic", "recruited", "detached", "converted"]}}
+                                          "fields": ["catalytic", "recruited", "detached", "converted"]},
+            "launch_shapes": {"fp32": shapes[32], "fp64": shapes[64]}}
 
 
 def flim_bench(args, device: int, rank: int, world: int, stream):
@@ -458,7 +464,12 @@ def main():
     stream = torch.cuda.Stream(device=device)
     frame = 0
     # launch shapes: timed on the first real steps of the run (untimed here), then fixed
-    shapes = eng.autotune(3, stream=stream) if not args.no_autotune else eng.launch_shapes()
+    if args.shapes:
+        shapes = eng.set_launch_shapes([int(x) for x in args.shapes.split(",")])
+    elif not args.no_autotune:
+        shapes = eng.autotune(3, stream=stream)
+    else:
+        shapes = eng.launch_shapes()
     stream.synchronize()
     ens.upload(stream=stream)  # the timed frames start from the initial state
     eng.set_step(0)

@@ -370,14 +370,16 @@ struct EdmEngine {
   // pairs: the species with fewer alive particles (count[sp], summed over
   // the replicas; the enzyme side without counts).  Both sides find the same
   // pairs, so this choice changes only the work.
-  void set_contact_sides(const int64_t* count) {
+  // force_mask >= 0: bit c set = reaction c from the enzyme side, whatever
+  // the counts.
+  void set_contact_sides(const int64_t* count, int32_t force_mask = -1) {
     const EdmDynParams& p = hdp[0];
     cat_lists = CatLists{};
     cat_lists.n_cat = p.n_cat;
     uint32_t sweepers = 0;
     for (int c = 0; c < p.n_cat; ++c) {
       const int e = p.cat[c].enzyme, sub = p.cat[c].substrate;
-      const bool from_enzyme = !count || count[e] <= count[sub];
+      const bool from_enzyme = force_mask >= 0 ? ((force_mask >> c) & 1) != 0 : (!count || count[e] <= count[sub]);
       const int sw = from_enzyme ? e : sub, other = from_enzyme ? sub : e;
       if (from_enzyme) cat_lists.from_enzyme |= 1u << c;
       cat_lists.other[c] = other;
@@ -1703,6 +1705,27 @@ int edm_autotune(EdmEngine* E, int32_t steps_per_shape, int32_t retune, void* st
   if (ce != cudaSuccess) return fail(EDM_ECUDA, std::string("edm_autotune: ") + cudaGetErrorString(ce));
   CUDA_TRY(cudaGetLastError());
   return EDM_OK;
+}
+
+int edm_set_launch_shapes(EdmEngine* E, const int32_t* candidate) {
+  if (!E || !candidate) return fail(EDM_EINVAL, "edm_set_launch_shapes: bad argument");
+  for (int k = 0; k < TK_COUNT; ++k)
+    if (candidate[k] < -1 || candidate[k] >= kNumShapes[k])
+      return fail(EDM_EINVAL, "edm_set_launch_shapes: no such candidate");
+  for (int k = 0; k < TK_COUNT; ++k)
+    if (candidate[k] >= 0) E->shape[k] = candidate[k];
+  E->drop_graphs();
+  return EDM_OK;
+}
+
+int edm_contact_sides(EdmEngine* E, int32_t force_mask) {
+  if (!E) return fail(EDM_EINVAL, "edm_contact_sides: null engine");
+  if (force_mask >= 0 && E->hdp[0].n_cat > 0) {
+    E->set_contact_sides(nullptr, force_mask);
+    E->contact_sides_counted = true;
+    E->drop_graphs();
+  }
+  return (int)(E->cat_lists.from_enzyme & 0x7FFFFFFFu);
 }
 
 int edm_launch_shapes(EdmEngine* E, int32_t* shapes, float* ms) {

@@ -74,6 +74,8 @@ def load_library():
     L.edm_launches_per_step.argtypes = [vp, i32]
     L.edm_autotune.argtypes = [vp, i32, i32, vp]
     L.edm_launch_shapes.argtypes = [vp, vp, vp]
+    L.edm_contact_sides.argtypes = [vp, i32]
+    L.edm_set_launch_shapes.argtypes = [vp, vp]
     L.edm_record_enable.argtypes = [vp, i32]
     L.edm_record_read.argtypes = [vp, i64, i32, vp, vp]
     L.edm_ground_truth.argtypes = [vp, vp, vp, vp, vp]
@@ -261,6 +263,22 @@ class Engine:
                                         "candidates": int(shp[k, 2]), "candidate": int(shp[k, 3]),
                                         "default_ms": float(ms[k, 0]),
                                         "tuned_ms": float(ms[k, 1])} for k in range(n)}
+
+    def set_launch_shapes(self, candidates: Sequence[int]) -> dict:
+        """Sets each tuned kernel's launch shape (edm_set_launch_shapes):
+        candidates[k] for TUNED_KERNELS[k], -1 keeps it; returns
+        launch_shapes()."""
+        c = np.full(len(self.TUNED_KERNELS), -1, dtype=np.int32)
+        c[: len(candidates)] = np.asarray(candidates, dtype=np.int32)
+        _check(self.L.edm_set_launch_shapes(self.handle, _ptr(c)), "edm_set_launch_shapes")
+        return self.launch_shapes()
+
+    def contact_sides(self, force_mask: Optional[int] = None) -> int:
+        """Sides of the catalytic contact sweep (edm_contact_sides): bit c set
+        = reaction c swept from its enzyme species, clear = from its substrate
+        species.  force_mask sets them; returns the mask in use."""
+        return _check(self.L.edm_contact_sides(self.handle, -1 if force_mask is None else int(force_mask)),
+                      "edm_contact_sides")
 
     # ---- census: sub-frame recorder and per-frame ground truth --------------
     def record_enable(self, capacity_steps: int) -> None:

@@ -403,12 +403,28 @@ int edm_ground_truth(EdmEngine* eng, double* fret_E, double* tau_DA,
  * of the same kind, unless retune != 0.  Drops the engine's captured graphs. */
 int edm_autotune(EdmEngine* eng, int32_t steps_per_shape, int32_t retune, void* stream);
 /* The launch shape in use per tuned kernel: shapes[k][4] = (threads per block,
- * minimum blocks per SM, candidates, chosen candidate; k_contacts candidates
- * 3 and 4 are the variant whose lanes take one neighbour column of an enzyme
- * each), ms[k][2] = (time of the default shape,
- * time of the chosen shape) from the last tuning (0 if not tuned).  Either
- * pointer may be NULL.  Returns the number of tuned kernels (3). */
+ * minimum blocks per SM, candidates, chosen candidate; k_contacts candidate 0
+ * gives a thread a whole sweeper, 1-2 give each lane one neighbour column of
+ * a sweeper within a warp, 3-5 within a block, 6-7 over a global sweeper
+ * list), ms[k][2] = (time of the default shape, time of the chosen shape) from
+ * the last tuning (0 if not tuned).  Either pointer may be NULL.  Returns the
+ * number of tuned kernels (3). */
 int edm_launch_shapes(EdmEngine* eng, int32_t* shapes, float* ms);
+/* Sets the launch shape of each tuned kernel: candidate[k] in
+ * [0, candidates of k), or -1 to keep it (a profiler run, where timings mean
+ * nothing, replays the shapes a plain run tuned).  Drops the captured graphs. */
+int edm_set_launch_shapes(EdmEngine* eng, const int32_t* candidate);
+
+/* Sides of the catalytic contact sweep.  No reference counterpart.  The
+ * pairs (enzyme, partner holding the substrate at the step start) of each
+ * catalytic reaction are found by sweeping from one side: bit c of the mask
+ * set = from the enzyme species, clear = from the substrate species (both
+ * find the same pairs; the choice changes only the work).  The first
+ * edm_set_state picks the side with fewer alive particles per reaction.
+ * force_mask >= 0 sets the sides (bits at or above the reaction count are
+ * ignored; later states do not change them) and drops the captured graphs;
+ * force_mask < 0 changes nothing.  Returns the mask in use. */
+int edm_contact_sides(EdmEngine* eng, int32_t force_mask);
 
 /* Counters [n_replicas][EDM_NCOUNTERS] and the sticky status word. */
 int edm_get_counters(EdmEngine* eng, int64_t* out, void* stream);
