@@ -176,8 +176,12 @@ struct Geo {
   __device__ __forceinline__ explicit Geo(const EdmDynParams& p)
       : nx(p.nx), ny(p.ny), px(p.periodic_x), py(p.periodic_y), Lx(p.Lx), Ly(p.Ly),
         sx(p.cell_sx), sy(p.cell_sy), cutoff_sq(p.cutoff_sq), sxf((float)p.cell_sx),
-        syf((float)p.cell_sy), inv_ny(1.0f / (float)p.ny), cbase(p.cell_offset), poff(p.particle_offset),
-        grave(p.nx * p.ny) {}
+        syf((float)p.cell_sy), inv_ny(0.0f), cbase(p.cell_offset), poff(p.particle_offset),
+        grave(p.nx * p.ny) {
+#ifdef __CUDA_ARCH__  // device-only intrinsic: the reciprocal without a division's slow path
+    inv_ny = __frcp_rn((float)p.ny);
+#endif
+  }
 };
 
 // Cell key c = cx * ny + cy -> (cx, cy) without an integer division: the
@@ -771,13 +775,14 @@ __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restric
         first = false;
       }
     }
-  } else {
+  } else if (nterms > 0) {  // most particles have no partner in force range
     Fx = (double)qx * 0x1p-20;
     Fy = (double)qy * 0x1p-20;
   }
 
-  double x, y;
-  abs_pos<F64>(st.pos_pre, st.lo_pre, st.cell_pre, s, g, x, y);
+  double x = 0.0, y = 0.0;
+  // the float32 path needs the absolute position here only for a D(x) field
+  if (F64 || p.dfield != EDM_DFIELD_NONE) abs_pos<F64>(st.pos_pre, st.lo_pre, st.cell_pre, s, g, x, y);
   double Di, gDx, gDy;
   dfield(p, sp, x, y, Di, gDx, gDy);
   const double dt = p.dt;
@@ -816,7 +821,7 @@ __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restric
     float dyt = (float)gDy * dtf + sn * z1 + Dif * (float)Fy * dtf;
     const float dr2 = dxt * dxt + dyt * dyt;
     double ddx = (double)dxt, ddy = (double)dyt;
-    if ((double)dr2 > p.max_disp_sq * 0.999) {
+    if (dr2 > (float)(p.max_disp_sq * 0.999)) {
       // at (or within rounding of) the displacement cap the move keeps only
       // its direction: form and cap it in float64 as dynamics.py:378-385 do
       ddx = gDx * dt;
