@@ -160,7 +160,7 @@ __device__ __forceinline__ void normal2_f32(uint64_t seed, int64_t step, int str
   // cos / sin of 2 pi u1 from the hardware approximations on [-pi, pi):
   // cos(2 pi u1) = -cos(2 pi u1 - pi), likewise sin (absolute error ~1e-6)
   float sf, cf;
-  __sincosf(6.283185307179586f * (float)u.u1 - 3.14159265358979f, &sf, &cf);
+  __sincosf(__fmaf_rn(6.283185307179586f, (float)u.u1, -3.14159265358979f), &sf, &cf);
   z0 = -r * cf;
   z1 = -r * sf;
 }

@@ -261,9 +261,9 @@ __device__ __forceinline__ float rel_sq_f32_xy(int cxi, int cyi, float2 oi, int 
     if (2 * dcy > g.ny) dcy -= g.ny;
     else if (2 * dcy < -g.ny) dcy += g.ny;
   }
-  dx = (float)dcx * g.sxf + (oi.x - oj.x);
-  dy = (float)dcy * g.syf + (oi.y - oj.y);
-  return dx * dx + dy * dy;
+  dx = __fmaf_rn((float)dcx, g.sxf, oi.x - oj.x);
+  dy = __fmaf_rn((float)dcy, g.syf, oi.y - oj.y);
+  return __fmaf_rn(dx, dx, dy * dy);
 }
 
 // float32 separation of two cell-relative points (cells ci, cj).
@@ -604,9 +604,9 @@ __device__ __forceinline__ void for_each_force_term(const EdmDynParams& p, const
         // from (cell, offset): the float32 sum below rounds at the ulp of a
         // cell side, a large fraction of |dx| for nearly coincident pairs
         const float2 oj = ((const float2*)st.pos_pre)[j];
-        const float fdx = -(float)dcx * g.sxf + (oi.x - oj.x);
-        const float fdy = -(float)dcy * g.syf + (oi.y - oj.y);
-        const float fdsq = fdx * fdx + fdy * fdy;
+        const float fdx = __fmaf_rn(-(float)dcx, g.sxf, oi.x - oj.x);
+        const float fdy = __fmaf_rn(-(float)dcy, g.syf, oi.y - oj.y);
+        const float fdsq = __fmaf_rn(fdx, fdx, fdy * fdy);
         if (!(fdsq < range_sqf)) return;
         const float2 li = st.lo_pre[s], lj = st.lo_pre[j];
         dx = (double)(-dcx) * g.sx + (((double)oi.x - (double)oj.x) + ((double)li.x - (double)lj.x));
@@ -817,9 +817,9 @@ __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restric
     normal2_f32(p.seed, step, EDM_S_BD_NORMAL, (uint64_t)id, z0, z1);
     const float Dif = (float)Di, dtf = (float)dt;
     const float sn = sqrtf(2.0f * Dif * dtf);
-    float dxt = (float)gDx * dtf + sn * z0 + Dif * (float)Fx * dtf;
-    float dyt = (float)gDy * dtf + sn * z1 + Dif * (float)Fy * dtf;
-    const float dr2 = dxt * dxt + dyt * dyt;
+    float dxt = __fmaf_rn(sn, z0, __fmaf_rn((float)gDx, dtf, Dif * (float)Fx * dtf));
+    float dyt = __fmaf_rn(sn, z1, __fmaf_rn((float)gDy, dtf, Dif * (float)Fy * dtf));
+    const float dr2 = __fmaf_rn(dxt, dxt, dyt * dyt);
     double ddx = (double)dxt, ddy = (double)dyt;
     if (dr2 > (float)(p.max_disp_sq * 0.999)) {
       // at (or within rounding of) the displacement cap the move keeps only
@@ -953,9 +953,9 @@ __device__ __forceinline__ void contact_candidate(const EdmDynParams& p, const G
   } else {
     // pre-move: j sits in the neighbour cell at (dcx, dcy)
     const float2 oj = ((const float2*)st.pos_pre)[j];
-    const float fdx = -(float)dcx * g.sxf + (oi_pre.x - oj.x);
-    const float fdy = -(float)dcy * g.syf + (oi_pre.y - oj.y);
-    if (!((double)(fdx * fdx + fdy * fdy) < g.cutoff_sq)) return;
+    const float fdx = __fmaf_rn(-(float)dcx, g.sxf, oi_pre.x - oj.x);
+    const float fdy = __fmaf_rn(-(float)dcy, g.syf, oi_pre.y - oj.y);
+    if (!((double)__fmaf_rn(fdx, fdx, fdy * fdy) < g.cutoff_sq)) return;
     float dx, dy;
     d2 = (double)rel_sq_f32_xy(cxs, cys, oi_post, st.cell_post[j], ((const float2*)st.pos_post)[j], g, dx, dy);
   }
@@ -1228,9 +1228,9 @@ __device__ __forceinline__ void late_contacts(const EdmDynParams& p, const Geo& 
       d2 = sep_sq<F64>(st.pos_post, st.cell_post, e, j, g);
     } else {
       const float2 oe = ((const float2*)st.pos_pre)[e], oj = ((const float2*)st.pos_pre)[j];
-      const float fdx = -(float)(-dcx) * g.sxf + (oe.x - oj.x);
-      const float fdy = -(float)(-dcy) * g.syf + (oe.y - oj.y);
-      if (!((double)(fdx * fdx + fdy * fdy) < g.cutoff_sq)) return;
+      const float fdx = __fmaf_rn(-(float)(-dcx), g.sxf, oe.x - oj.x);
+      const float fdy = __fmaf_rn(-(float)(-dcy), g.syf, oe.y - oj.y);
+      if (!((double)__fmaf_rn(fdx, fdx, fdy * fdy) < g.cutoff_sq)) return;
       d2 = sep_sq<F64>(st.pos_post, st.cell_post, e, j, g);
     }
     for (uint32_t b = late; b; b &= b - 1) {
