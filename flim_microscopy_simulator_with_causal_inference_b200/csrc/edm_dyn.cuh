@@ -167,16 +167,23 @@ __device__ __forceinline__ int atomic_inc_aggregated(int32_t* addr) {
 }
 
 // ---- replica geometry --------------------------------------------------------
+// The box side and the pair-list cutoff are read from the parameter block
+// where they are used (rare branches), so they hold no registers meanwhile.
+// Slot, particle and bucket offsets fit 32 bits (slot indices are int32).
 struct Geo {
+  const EdmDynParams* prm;
   int nx, ny, px, py;
-  double Lx, Ly, sx, sy, cutoff_sq;
+  double sx, sy;
   float sxf, syf, inv_ny;
-  int64_t cbase, poff;
+  int cbase, poff;
   int grave;  // bucket of non-alive particles
+  __device__ __forceinline__ double Lx() const { return prm->Lx; }
+  __device__ __forceinline__ double Ly() const { return prm->Ly; }
+  __device__ __forceinline__ double cutoff_sq() const { return prm->cutoff_sq; }
   __device__ __forceinline__ explicit Geo(const EdmDynParams& p)
-      : nx(p.nx), ny(p.ny), px(p.periodic_x), py(p.periodic_y), Lx(p.Lx), Ly(p.Ly),
-        sx(p.cell_sx), sy(p.cell_sy), cutoff_sq(p.cutoff_sq), sxf((float)p.cell_sx),
-        syf((float)p.cell_sy), inv_ny(0.0f), cbase(p.cell_offset), poff(p.particle_offset),
+      : prm(&p), nx(p.nx), ny(p.ny), px(p.periodic_x), py(p.periodic_y),
+        sx(p.cell_sx), sy(p.cell_sy), sxf((float)p.cell_sx),
+        syf((float)p.cell_sy), inv_ny(0.0f), cbase((int)p.cell_offset), poff((int)p.particle_offset),
         grave(p.nx * p.ny) {
 #ifdef __CUDA_ARCH__  // device-only intrinsic: the reciprocal without a division's slow path
     inv_ny = __frcp_rn((float)p.ny);
@@ -236,12 +243,12 @@ __device__ __forceinline__ double min_image_sq(double x1, double y1, double x2, 
   dx = x1 - x2;
   dy = y1 - y2;
   if (g.px) {
-    if (dx > 0.5 * g.Lx) dx -= g.Lx;
-    else if (dx < -0.5 * g.Lx) dx += g.Lx;
+    if (dx > 0.5 * g.Lx()) dx -= g.Lx();
+    else if (dx < -0.5 * g.Lx()) dx += g.Lx();
   }
   if (g.py) {
-    if (dy > 0.5 * g.Ly) dy -= g.Ly;
-    else if (dy < -0.5 * g.Ly) dy += g.Ly;
+    if (dy > 0.5 * g.Ly()) dy -= g.Ly();
+    else if (dy < -0.5 * g.Ly()) dy += g.Ly();
   }
   return dx * dx + dy * dy;
 }
@@ -570,7 +577,7 @@ __device__ __forceinline__ void for_each_force_term(const EdmDynParams& p, const
     oi = ((const float2*)st.pos_pre)[s];
   }
   // pairs beyond both the pair-list cutoff and every potential's range carry no force
-  const double range_sq = p.force_range_sq < g.cutoff_sq ? p.force_range_sq : g.cutoff_sq;
+  const double range_sq = p.force_range_sq < g.cutoff_sq() ? p.force_range_sq : g.cutoff_sq();
   const float range_sqf = (float)range_sq * 1.0001f;
   // Only neighbour cells within that range of the particle can hold a force
   // partner (a partner in a skipped column or row is farther than its offset
@@ -803,12 +810,12 @@ __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restric
     }
     x += dxt;
     y += dyt;
-    if (g.px) x = py_fmod(x, g.Lx);
+    if (g.px) x = py_fmod(x, g.Lx());
     else if (x < 0.0) x = -x;
-    else if (x >= g.Lx) x = 2.0 * g.Lx - x;
-    if (g.py) y = py_fmod(y, g.Ly);
+    else if (x >= g.Lx()) x = 2.0 * g.Lx() - x;
+    if (g.py) y = py_fmod(y, g.Ly());
     else if (y < 0.0) y = -y;
-    else if (y >= g.Ly) y = 2.0 * g.Ly - y;
+    else if (y >= g.Ly()) y = 2.0 * g.Ly() - y;
     if (!isfinite(x) || !isfinite(y)) set_status(st.status, EDM_STATUS_NONFINITE);
     ((double2*)st.pos_post)[s] = make_double2(x, y);
     newc = cell_index(x, g.sx, g.nx) * g.ny + cell_index(y, g.sy, g.ny);
@@ -861,7 +868,7 @@ __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restric
     } else if (cx < 0 || cx >= g.nx) {  // reflecting wall, in float64
       double bx = (double)cx * g.sx + ax;
       if (bx < 0.0) bx = -bx;
-      else if (bx >= g.Lx) bx = 2.0 * g.Lx - bx;
+      else if (bx >= g.Lx()) bx = 2.0 * g.Lx() - bx;
       cx = cell_index(bx, g.sx, g.nx);
       ax = bx - (double)cx * g.sx;
     }
@@ -871,7 +878,7 @@ __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restric
     } else if (cy < 0 || cy >= g.ny) {
       double by = (double)cy * g.sy + ay;
       if (by < 0.0) by = -by;
-      else if (by >= g.Ly) by = 2.0 * g.Ly - by;
+      else if (by >= g.Ly()) by = 2.0 * g.Ly() - by;
       cy = cell_index(by, g.sy, g.ny);
       ay = by - (double)cy * g.sy;
     }
@@ -948,14 +955,14 @@ __device__ __forceinline__ void contact_candidate(const EdmDynParams& p, const G
   if (!fl_alive(fj) || !((pmask >> spj) & 1u)) return;
   double d2;
   if constexpr (F64) {
-    if (!(sep_sq<F64>(st.pos_pre, st.cell_pre, s, j, g) < g.cutoff_sq)) return;
+    if (!(sep_sq<F64>(st.pos_pre, st.cell_pre, s, j, g) < g.cutoff_sq())) return;
     d2 = sep_sq<F64>(st.pos_post, st.cell_post, s, j, g);
   } else {
     // pre-move: j sits in the neighbour cell at (dcx, dcy)
     const float2 oj = ((const float2*)st.pos_pre)[j];
     const float fdx = __fmaf_rn(-(float)dcx, g.sxf, oi_pre.x - oj.x);
     const float fdy = __fmaf_rn(-(float)dcy, g.syf, oi_pre.y - oj.y);
-    if (!((double)__fmaf_rn(fdx, fdx, fdy * fdy) < g.cutoff_sq)) return;
+    if (!((double)__fmaf_rn(fdx, fdx, fdy * fdy) < g.cutoff_sq())) return;
     float dx, dy;
     d2 = (double)rel_sq_f32_xy(cxs, cys, oi_post, st.cell_post[j], ((const float2*)st.pos_post)[j], g, dx, dy);
   }
@@ -1224,13 +1231,13 @@ __device__ __forceinline__ void late_contacts(const EdmDynParams& p, const Geo& 
     if (!fl_alive(fe) || !((emask >> spe) & 1u)) return;
     double d2;
     if constexpr (F64) {
-      if (!(sep_sq<F64>(st.pos_pre, st.cell_pre, e, j, g) < g.cutoff_sq)) return;
+      if (!(sep_sq<F64>(st.pos_pre, st.cell_pre, e, j, g) < g.cutoff_sq())) return;
       d2 = sep_sq<F64>(st.pos_post, st.cell_post, e, j, g);
     } else {
       const float2 oe = ((const float2*)st.pos_pre)[e], oj = ((const float2*)st.pos_pre)[j];
       const float fdx = __fmaf_rn(-(float)(-dcx), g.sxf, oe.x - oj.x);
       const float fdy = __fmaf_rn(-(float)(-dcy), g.syf, oe.y - oj.y);
-      if (!((double)__fmaf_rn(fdx, fdx, fdy * fdy) < g.cutoff_sq)) return;
+      if (!((double)__fmaf_rn(fdx, fdx, fdy * fdy) < g.cutoff_sq())) return;
       d2 = sep_sq<F64>(st.pos_post, st.cell_post, e, j, g);
     }
     for (uint32_t b = late; b; b &= b - 1) {
@@ -1578,7 +1585,7 @@ __global__ void __launch_bounds__(kBlock) k_bind_candidates(const EdmDynParams* 
         } else {
           return;
         }
-        if (!(sep_sq<F64>(st.pos_pre, st.cell_pre, s, j, g) < g.cutoff_sq)) return;
+        if (!(sep_sq<F64>(st.pos_pre, st.cell_pre, s, j, g) < g.cutoff_sq())) return;
         if (sep_sq<F64>(st.pos_post, st.cell_post, s, j, g) > B.contact_sq) return;
         const double u = uniform1(p.seed, step, EDM_S_BIND + 2 * b, (uint64_t)id, (uint64_t)idj);
         if (!(u < B.prob_bind)) return;

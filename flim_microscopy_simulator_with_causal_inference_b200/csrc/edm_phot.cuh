@@ -116,12 +116,12 @@ __device__ int fret_class(const EdmDynParams& p, const EdmPhotParams& pp, const 
         abs_pos<F64>(st.pos_post, st.lo_post, st.cell_post, j, g, xj, yj);
         double dx = xj - xi, dy = yj - yi;
         if (g.px) {
-          if (dx > g.Lx / 2.0) dx -= g.Lx;
-          else if (dx < -g.Lx / 2.0) dx += g.Lx;
+          if (dx > g.Lx() / 2.0) dx -= g.Lx();
+          else if (dx < -g.Lx() / 2.0) dx += g.Lx();
         }
         if (g.py) {
-          if (dy > g.Ly / 2.0) dy -= g.Ly;
-          else if (dy < -g.Ly / 2.0) dy += g.Ly;
+          if (dy > g.Ly() / 2.0) dy -= g.Ly();
+          else if (dy < -g.Ly() / 2.0) dy += g.Ly();
         }
         return dx * dx + dy * dy < F.prox_radius_sq;
       };
