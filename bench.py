@@ -517,22 +517,30 @@ def main():
     sp_idx = torch.empty(sp_cap, dtype=torch.int64).pin_memory().numpy()
     sp_cnt = torch.empty(sp_cap, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
 
+    state_outs = [state_out, {k: torch.empty((eng.N, w) if w > 1 else (eng.N,), dtype=tdt[dt]).pin_memory().numpy()
+                              for k, dt, w in eng.STATE_FIELDS}]
+
     def e2e_loop(sparse: bool):
-        """Frames through the C ABI with host buffers: state H2D, 100 steps,
-        finalize, state D2H and every replica's stacks D2H (their nonzero bins
-        with edm_frame_out_sparse, or dense on the copy stream)."""
+        """Frames through the C ABI with pinned host buffers, the transfers
+        overlapped with the computation: every frame uploads its state
+        (edm_set_state_async: the next frame's upload runs while this frame
+        computes), runs 100 steps, finalizes, downloads the state
+        (edm_get_state_async: while the next frame computes) and reads every
+        replica's stacks (their nonzero bins with edm_frame_out_sparse, or
+        dense on the copy stream)."""
         nonlocal frame
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
         d2h_flim = 0
         t0 = time.perf_counter()
-        for _ in range(args.steps):
-            eng.set_state(pinned["positions"], pinned["species"], pinned["alive"], pinned["bond"],
-                          pinned["has_dye"], pinned["dye"], pinned["ctmc"], pinned["bleached"], stream=stream)
+        eng.set_state_async(pinned, stream=stream)
+        for k in range(args.steps):
             eng.pipeline_steps(STEPS_PER_FRAME, True, STEPS_PER_FRAME, stream=stream)
             eng.finalize(frame, stream=stream)
-            st = eng.get_state(stream=stream, out=state_out)
+            st = eng.get_state_async(state_outs[k % 2], stream=stream)
+            if k + 1 < args.steps:  # the next frame's state goes up while this frame's reads finish
+                eng.set_state_async(pinned, stream=stream)
             done = False
             if sparse:
                 try:
@@ -547,6 +555,7 @@ def main():
                 d2h_flim += flim_elems * 4
             frame += 1
         eng.frame_out_wait()
+        eng.transfers_wait()
         torch.cuda.synchronize()
         e2e_s = max_over_ranks(time.perf_counter() - t0, world, "cuda")
         state_bytes_out = sum(v.nbytes for v in st.values())
@@ -687,9 +696,11 @@ def main():
                        "bd_steps_per_step": STEPS_PER_FRAME, "precision": "f32 cell-relative positions",
                        "l2": "working set > 126 MB L2 (resident state ~45 B/particle)"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                    "note": "per frame: state H2D from pinned host, 100 BD steps, finalize, state D2H, every "
-                            "replica's FLIM stacks D2H as their nonzero bins (edm_frame_out_sparse: element index "
-                            "+ count, lossless); bytes are per BD step",
+                    "note": "per frame: state H2D from pinned host (edm_set_state_async: uploaded while the "
+                            "previous frame computes), 100 BD steps, finalize, state D2H (edm_get_state_async: "
+                            "downloaded while the next frame computes), every replica's FLIM stacks D2H as their "
+                            "nonzero bins (edm_frame_out_sparse: element index + count, lossless); bytes are per "
+                            "BD step",
                     "dense_stacks": {"value": e2e_dense, "d2h_bytes_per_step": int(d2h_dense),
                                      "note": "the same loop reading the stacks dense (edm_frame_out_begin on a "
                                              "copy stream, overlapping the next frame)"}},

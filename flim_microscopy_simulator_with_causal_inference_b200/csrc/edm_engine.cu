@@ -766,6 +766,37 @@ struct EdmEngine {
   cudaEvent_t ev_snap = nullptr, ev_read = nullptr;
   bool read_pending = false;
 
+  // asynchronous state transfers (edm_set_state_async / edm_get_state_async):
+  // the host arrays land in (leave from) device staging of their own, on an
+  // upload (download) stream, so the link works while `stream` computes
+  struct Xfer {
+    double* pos = nullptr;
+    int32_t *sp = nullptr, *bond = nullptr, *dye = nullptr;
+    uint8_t *alive = nullptr, *has_dye = nullptr, *bleached = nullptr;
+    int8_t* ctmc = nullptr;
+  } in, out;
+  cudaStream_t up_stream = nullptr, down_stream = nullptr;
+  cudaEvent_t ev_staged = nullptr, ev_in_free = nullptr, ev_out_ready = nullptr, ev_out_free = nullptr;
+  bool in_used = false, out_used = false;
+
+  int xfer_setup() {
+    if (up_stream) return EDM_OK;
+    int rc;
+    const size_t n = (size_t)std::max<int64_t>(N, 1);
+    for (Xfer* x : {&in, &out}) {
+      if ((rc = alloc(&x->pos, 2 * n)) != EDM_OK || (rc = alloc(&x->sp, n)) != EDM_OK ||
+          (rc = alloc(&x->bond, n)) != EDM_OK || (rc = alloc(&x->dye, n)) != EDM_OK ||
+          (rc = alloc(&x->alive, n)) != EDM_OK || (rc = alloc(&x->has_dye, n)) != EDM_OK ||
+          (rc = alloc(&x->bleached, n)) != EDM_OK || (rc = alloc(&x->ctmc, n)) != EDM_OK)
+        return rc;
+    }
+    CUDA_TRY(cudaStreamCreateWithFlags(&up_stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaStreamCreateWithFlags(&down_stream, cudaStreamNonBlocking));
+    for (cudaEvent_t* ev : {&ev_staged, &ev_in_free, &ev_out_ready, &ev_out_free})
+      CUDA_TRY(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+    return EDM_OK;
+  }
+
   ~EdmEngine() {
     for (auto& ev : tune_ev)
       if (ev) cudaEventDestroy(ev);
@@ -775,6 +806,10 @@ struct EdmEngine {
     if (ev_snap) cudaEventDestroy(ev_snap);
     if (ev_read) cudaEventDestroy(ev_read);
     if (copy_stream) cudaStreamDestroy(copy_stream);
+    if (up_stream) cudaStreamDestroy(up_stream);
+    if (down_stream) cudaStreamDestroy(down_stream);
+    for (cudaEvent_t ev : {ev_staged, ev_in_free, ev_out_ready, ev_out_free})
+      if (ev) cudaEventDestroy(ev);
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     for (void* p : allocs) cudaFree(p);
   }
@@ -1343,6 +1378,100 @@ int edm_get_state(EdmEngine* E, EdmHostState* st, void* stream) {
   if (st->is_bleached) CUDA_TRY(cudaMemcpyAsync(st->is_bleached, E->bleached, N, cudaMemcpyDeviceToHost, s));
   if (st->has_dye) CUDA_TRY(cudaMemcpyAsync(st->has_dye, E->has_dye, N, cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
+  return EDM_OK;
+}
+
+int edm_set_state_async(EdmEngine* E, const EdmHostState* st, void* stream) {
+  if (!E || !st || st->n != E->N) return fail(EDM_EINVAL, "edm_set_state_async: size mismatch");
+  // new dye carriers rebuild the emitter list on the host: the synchronous path
+  if (E->has_phot && !(E->has_dye_host.size() == (size_t)E->N &&
+                       std::memcmp(E->has_dye_host.data(), st->has_dye, (size_t)E->N) == 0))
+    return edm_set_state(E, st, stream);
+  CUDA_TRY(cudaSetDevice(E->device));
+  int rc = E->xfer_setup();
+  if (rc != EDM_OK) return rc;
+  cudaStream_t s = (cudaStream_t)stream, u = E->up_stream;
+  const int64_t N = E->N;
+  const EdmEngine::Xfer& in = E->in;
+  E->cells_valid = false;
+  // the upload waits only for the previous one to leave the staging, not for `stream`
+  if (E->in_used) CUDA_TRY(cudaStreamWaitEvent(u, E->ev_in_free, 0));
+  CUDA_TRY(cudaMemcpyAsync(in.pos, st->positions, sizeof(double) * 2 * N, cudaMemcpyHostToDevice, u));
+  CUDA_TRY(cudaMemcpyAsync(in.sp, st->species_id, sizeof(int32_t) * N, cudaMemcpyHostToDevice, u));
+  CUDA_TRY(cudaMemcpyAsync(in.alive, st->is_alive, N, cudaMemcpyHostToDevice, u));
+  CUDA_TRY(cudaMemcpyAsync(in.bond, st->bond_partner, sizeof(int32_t) * N, cudaMemcpyHostToDevice, u));
+  CUDA_TRY(cudaMemcpyAsync(in.has_dye, st->has_dye, N, cudaMemcpyHostToDevice, u));
+  CUDA_TRY(cudaMemcpyAsync(in.dye, st->dye_type_id, sizeof(int32_t) * N, cudaMemcpyHostToDevice, u));
+  CUDA_TRY(cudaMemcpyAsync(in.ctmc, st->ctmc_state, N, cudaMemcpyHostToDevice, u));
+  CUDA_TRY(cudaMemcpyAsync(in.bleached, st->is_bleached, N, cudaMemcpyHostToDevice, u));
+  CUDA_TRY(cudaEventRecord(E->ev_staged, u));
+  // the installation, in order on `stream`: as edm_set_state from the staging
+  CUDA_TRY(cudaStreamWaitEvent(s, E->ev_staged, 0));
+  CUDA_TRY(cudaMemcpyAsync(E->bond, in.bond, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(E->has_dye, in.has_dye, N, cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(E->ctmc, in.ctmc, N, cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(E->bleached, in.bleached, N, cudaMemcpyDeviceToDevice, s));
+  if (N > 0) k_narrow_i8<<<148 * 8, 256, 0, s>>>(in.dye, E->dye, N);
+  CUDA_TRY(cudaMemsetAsync(E->cnt, 0, sizeof(int32_t) * (E->n_cells > 0 ? E->n_cells : 1), s));
+  if (E->npblk > 0) {
+    if (E->f64)
+      k_set_state<true><<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, in.pos, in.sp, in.alive, E->pos_post, E->lo_post,
+                                                    E->cell_post, E->flags[E->cur], E->ids[E->cur], E->slot_of_id,
+                                                    E->cnt);
+    else
+      k_set_state<false><<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, in.pos, in.sp, in.alive, E->pos_post, E->lo_post,
+                                                     E->cell_post, E->flags[E->cur], E->ids[E->cur], E->slot_of_id,
+                                                     E->cnt);
+    k_bond_to_global<<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, E->bond);
+  }
+  CUDA_TRY(cudaEventRecord(E->ev_in_free, s));
+  E->in_used = true;
+  CUDA_TRY(cudaGetLastError());
+  return EDM_OK;
+}
+
+int edm_get_state_async(EdmEngine* E, EdmHostState* st, void* stream) {
+  if (!E || !st || st->n != E->N) return fail(EDM_EINVAL, "edm_get_state_async: size mismatch");
+  CUDA_TRY(cudaSetDevice(E->device));
+  int rc = E->xfer_setup();
+  if (rc != EDM_OK) return rc;
+  cudaStream_t s = (cudaStream_t)stream, d = E->down_stream;
+  const int64_t N = E->N;
+  const EdmEngine::Xfer& out = E->out;
+  // the gathering, in order on `stream`, once the previous download has left the staging
+  if (E->out_used) CUDA_TRY(cudaStreamWaitEvent(s, E->ev_out_free, 0));
+  if (E->npblk > 0) {
+    if (E->f64)
+      k_get_state<true><<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, E->pos_post, E->lo_post, E->cell_post, E->flags[E->cur],
+                                                    E->slot_of_id, E->bond, out.pos, out.sp, out.alive, out.bond);
+    else
+      k_get_state<false><<<E->npblk, kBlock, 0, s>>>(E->dp, E->pblk, E->pos_post, E->lo_post, E->cell_post, E->flags[E->cur],
+                                                     E->slot_of_id, E->bond, out.pos, out.sp, out.alive, out.bond);
+  }
+  CUDA_TRY(cudaMemcpyAsync(out.ctmc, E->ctmc, N, cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(out.bleached, E->bleached, N, cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(out.has_dye, E->has_dye, N, cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(cudaEventRecord(E->ev_out_ready, s));
+  // the download, on the engine's stream, while `stream` goes on
+  CUDA_TRY(cudaStreamWaitEvent(d, E->ev_out_ready, 0));
+  if (st->positions) CUDA_TRY(cudaMemcpyAsync(st->positions, out.pos, sizeof(double) * 2 * N, cudaMemcpyDeviceToHost, d));
+  if (st->species_id) CUDA_TRY(cudaMemcpyAsync(st->species_id, out.sp, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, d));
+  if (st->is_alive) CUDA_TRY(cudaMemcpyAsync(st->is_alive, out.alive, N, cudaMemcpyDeviceToHost, d));
+  if (st->bond_partner) CUDA_TRY(cudaMemcpyAsync(st->bond_partner, out.bond, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, d));
+  if (st->ctmc_state) CUDA_TRY(cudaMemcpyAsync(st->ctmc_state, out.ctmc, N, cudaMemcpyDeviceToHost, d));
+  if (st->is_bleached) CUDA_TRY(cudaMemcpyAsync(st->is_bleached, out.bleached, N, cudaMemcpyDeviceToHost, d));
+  if (st->has_dye) CUDA_TRY(cudaMemcpyAsync(st->has_dye, out.has_dye, N, cudaMemcpyDeviceToHost, d));
+  CUDA_TRY(cudaEventRecord(E->ev_out_free, d));
+  E->out_used = true;
+  CUDA_TRY(cudaGetLastError());
+  return EDM_OK;
+}
+
+int edm_state_transfers_wait(EdmEngine* E) {
+  if (!E) return fail(EDM_EINVAL, "edm_state_transfers_wait: null engine");
+  CUDA_TRY(cudaSetDevice(E->device));
+  if (E->up_stream) CUDA_TRY(cudaStreamSynchronize(E->up_stream));
+  if (E->down_stream) CUDA_TRY(cudaStreamSynchronize(E->down_stream));
   return EDM_OK;
 }
 

@@ -75,6 +75,9 @@ def load_library():
     L.edm_autotune.argtypes = [vp, i32, i32, vp]
     L.edm_launch_shapes.argtypes = [vp, vp, vp]
     L.edm_contact_sides.argtypes = [vp, i32]
+    L.edm_set_state_async.argtypes = [vp, vp, vp]
+    L.edm_get_state_async.argtypes = [vp, vp, vp]
+    L.edm_state_transfers_wait.argtypes = [vp]
     L.edm_set_launch_shapes.argtypes = [vp, vp]
     L.edm_record_enable.argtypes = [vp, i32]
     L.edm_record_read.argtypes = [vp, i64, i32, vp, vp]
@@ -191,6 +194,45 @@ class Engine:
                              _ptr(out["has_dye"]), None, _ptr(out["ctmc"]), _ptr(out["bleached"]))
         _check(self.L.edm_get_state(self.handle, C.byref(hs), _stream_handle(stream)), "edm_get_state")
         return out
+
+    # ---- transfers overlapped with computation ------------------------------
+    SET_FIELDS = (("positions", np.float64, 2), ("species", np.int32, 1), ("alive", np.uint8, 1),
+                  ("bond", np.int32, 1), ("has_dye", np.uint8, 1), ("dye", np.int32, 1), ("ctmc", np.int8, 1),
+                  ("bleached", np.uint8, 1))
+
+    def _require(self, arrs: dict, fields, what: str):
+        N = self.N
+        for k, dt, w in fields:
+            a = arrs[k]
+            if a.dtype != dt or a.shape != ((N, w) if w > 1 else (N,)) or not a.flags.c_contiguous:
+                raise ValueError(f"{what}: '{k}' must be a contiguous {np.dtype(dt).name} array of N rows")
+
+    def set_state_async(self, arrs: dict, stream=None):
+        """edm_set_state_async: the host arrays (SET_FIELDS' dtypes, pinned)
+        go up on the engine's upload stream while `stream` computes; they
+        must stay unchanged until transfers_wait()."""
+        self._require(arrs, self.SET_FIELDS, "set_state_async")
+        hs = PR.EdmHostState(self.N, _ptr(arrs["positions"]), _ptr(arrs["species"]), _ptr(arrs["alive"]),
+                             _ptr(arrs["bond"]), _ptr(arrs["has_dye"]), _ptr(arrs["dye"]), _ptr(arrs["ctmc"]),
+                             _ptr(arrs["bleached"]))
+        self._xfer_refs = getattr(self, "_xfer_refs", []) + [arrs]
+        _check(self.L.edm_set_state_async(self.handle, C.byref(hs), _stream_handle(stream)), "edm_set_state_async")
+
+    def get_state_async(self, out: dict, stream=None) -> dict:
+        """edm_get_state_async: the state (STATE_FIELDS) comes down on the
+        engine's download stream while `stream` goes on; read `out` after
+        transfers_wait()."""
+        self._require(out, self.STATE_FIELDS, "get_state_async")
+        hs = PR.EdmHostState(self.N, _ptr(out["positions"]), _ptr(out["species"]), _ptr(out["alive"]),
+                             _ptr(out["bond"]), _ptr(out["has_dye"]), None, _ptr(out["ctmc"]), _ptr(out["bleached"]))
+        self._xfer_refs = getattr(self, "_xfer_refs", []) + [out]
+        _check(self.L.edm_get_state_async(self.handle, C.byref(hs), _stream_handle(stream)), "edm_get_state_async")
+        return out
+
+    def transfers_wait(self):
+        """Wait for the asynchronous state transfers (edm_state_transfers_wait)."""
+        _check(self.L.edm_state_transfers_wait(self.handle), "edm_state_transfers_wait")
+        self._xfer_refs = []
 
     def set_step(self, k: int):
         _check(self.L.edm_set_step(self.handle, int(k)), "edm_set_step")

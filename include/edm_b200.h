@@ -276,6 +276,22 @@ int edm_destroy(EdmEngine* eng);
  * memory. */
 int edm_set_state(EdmEngine* eng, const EdmHostState* st, void* stream);
 int edm_get_state(EdmEngine* eng, EdmHostState* st, void* stream);
+
+/* The same transfers overlapped with computation, for loops that feed a new
+ * state and read the result every frame.  No reference counterpart.
+ * edm_set_state_async copies the host arrays into a device staging area of
+ * its own on the engine's upload stream, without waiting for the work already
+ * queued on `stream`, and queues the state's installation on `stream` after
+ * that work.  edm_get_state_async queues the state's gathering into a second
+ * staging area on `stream` and copies it to the host arrays on the engine's
+ * download stream while `stream` goes on.  The host arrays should be pinned,
+ * and must stay valid (set) or unread (get) until edm_state_transfers_wait
+ * returns.  A set whose dye carriers differ from the last upload rebuilds the
+ * emitter list on the host: it falls back to edm_set_state.  The first call
+ * allocates both staging areas (2 * 28 bytes per particle). */
+int edm_set_state_async(EdmEngine* eng, const EdmHostState* st, void* stream);
+int edm_get_state_async(EdmEngine* eng, EdmHostState* st, void* stream);
+int edm_state_transfers_wait(EdmEngine* eng);
 int edm_set_step(EdmEngine* eng, int64_t step_index);
 int64_t edm_get_step(EdmEngine* eng);
 
