@@ -777,7 +777,7 @@ struct EdmEngine {
   } in, out;
   cudaStream_t up_stream = nullptr, down_stream = nullptr;
   cudaEvent_t ev_staged = nullptr, ev_in_free = nullptr, ev_out_ready = nullptr, ev_out_free = nullptr;
-  bool in_used = false, out_used = false;
+  bool in_used = false, out_used = false, staged = false;
 
   int xfer_setup() {
     if (up_stream) return EDM_OK;
@@ -1114,12 +1114,15 @@ namespace {
 // ---- sparse frame readout ----------------------------------------------------
 // A frame's TCSPC stacks are mostly zero (about one bin in a thousand holds a
 // photon at the bench's rates), so the readout can move only the nonzero
-// bins.  Block b owns the elements [b chunk, (b + 1) chunk) of the
-// concatenated stacks; a counting pass and a scan of the block counts give
-// each block its output offset, and the writing pass emits (element index,
-// count) in index order and clears the bins it emits.
+// bins.  Warp w owns the elements [w chunk, (w + 1) chunk) of the
+// concatenated stacks; a counting pass and a scan of the warp counts give
+// each warp its output offset, and the writing pass emits (element index,
+// count) in index order and clears the bins it emits.  Warps work alone (no
+// block barrier), and a 128-element stretch without a photon costs the
+// writing pass one ballot.
 constexpr int kSpBlocks = 148 * 8;
 constexpr int kSpThreads = 256;
+constexpr int kSpWarps = kSpBlocks * (kSpThreads / 32);
 
 __device__ __forceinline__ uint4 sp_load(const uint32_t* f, int64_t i, int64_t end) {
   if (i + 3 < end) return *reinterpret_cast<const uint4*>(f + i);
@@ -1130,26 +1133,25 @@ __device__ __forceinline__ uint4 sp_load(const uint32_t* f, int64_t i, int64_t e
   return v;
 }
 
-__global__ void __launch_bounds__(kSpThreads) k_sp_count(const uint32_t* __restrict__ flim, int64_t n, int64_t chunk,
-                                                         int32_t* __restrict__ bcount) {
-  __shared__ int ws[kSpThreads / 32];
-  const int64_t b0 = (int64_t)blockIdx.x * chunk, b1 = b0 + chunk < n ? b0 + chunk : n;
-  int c = 0;
-  for (int64_t i = b0 + 4 * (int64_t)threadIdx.x; i < b1; i += 4 * (int64_t)blockDim.x) {
-    const uint4 v = sp_load(flim, i, b1);
-    c += (v.x != 0u) + (v.y != 0u) + (v.z != 0u) + (v.w != 0u);
-  }
-  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
-  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int t = 0;
-    for (int w = 0; w < kSpThreads / 32; ++w) t += ws[w];
-    bcount[blockIdx.x] = t;
-  }
+__device__ __forceinline__ int sp_nonzero(const uint4& v) {
+  return (v.x != 0u) + (v.y != 0u) + (v.z != 0u) + (v.w != 0u);
 }
 
-// exclusive scan of the block counts (one block); off[nb] = total
+__global__ void __launch_bounds__(kSpThreads) k_sp_count(const uint32_t* __restrict__ flim, int64_t n, int64_t chunk,
+                                                         int32_t* __restrict__ wcount) {
+  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int64_t b0 = w * chunk, b1 = b0 + chunk < n ? b0 + chunk : n;
+  int c = 0;
+  for (int64_t i = b0 + 4 * lane; i < b1; i += 256) {  // two loads in flight per lane
+    c += sp_nonzero(sp_load(flim, i, b1));
+    if (i + 128 < b1) c += sp_nonzero(sp_load(flim, i + 128, b1));
+  }
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  if (lane == 0) wcount[w] = c;
+}
+
+// exclusive scan of the warp counts (one block); off[nb] = total
 __global__ void k_sp_scan(const int32_t* __restrict__ bcount, int nb, int64_t* __restrict__ off) {
   int64_t carry = 0;
   for (int base = 0; base < nb; base += blockDim.x) {
@@ -1170,15 +1172,23 @@ __global__ void __launch_bounds__(kSpThreads) k_sp_write(uint32_t* __restrict__ 
                                                          int64_t* __restrict__ idx_out, uint32_t* __restrict__ cnt_out,
                                                          int64_t cap) {
   if (off[nb] > cap) return;
-  const int64_t b0 = (int64_t)blockIdx.x * chunk, b1 = b0 + chunk < n ? b0 + chunk : n;
-  int64_t base = off[blockIdx.x];
-  for (int64_t t0 = b0; t0 < b1; t0 += 4 * (int64_t)blockDim.x) {  // same trip count in every thread
-    const int64_t i = t0 + 4 * (int64_t)threadIdx.x;
+  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int64_t b0 = w * chunk, b1 = b0 + chunk < n ? b0 + chunk : n;
+  int64_t base = off[w];
+  for (int64_t t0 = b0; t0 < b1; t0 += 128) {  // the same trip count in every lane of the warp
+    const int64_t i = t0 + 4 * lane;
     const uint4 v = sp_load(flim, i, b1);
+    const int c = sp_nonzero(v);
+    if (__ballot_sync(0xffffffffu, c != 0) == 0u) continue;
+    int q = c;  // inclusive scan over the lanes
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, q, o);
+      if (lane >= o) q += t;
+    }
+    const int total = __shfl_sync(0xffffffffu, q, 31);
+    q -= c;
     const uint32_t e[4] = {v.x, v.y, v.z, v.w};
-    const int c = (v.x != 0u) + (v.y != 0u) + (v.z != 0u) + (v.w != 0u);
-    int total;
-    int q = block_exclusive_scan(c, total);
     for (int k = 0; k < 4; ++k) {
       if (e[k] != 0u) {
         idx_out[base + q] = i + k;
@@ -1381,20 +1391,18 @@ int edm_get_state(EdmEngine* E, EdmHostState* st, void* stream) {
   return EDM_OK;
 }
 
-int edm_set_state_async(EdmEngine* E, const EdmHostState* st, void* stream) {
-  if (!E || !st || st->n != E->N) return fail(EDM_EINVAL, "edm_set_state_async: size mismatch");
-  // new dye carriers rebuild the emitter list on the host: the synchronous path
+int edm_stage_state_async(EdmEngine* E, const EdmHostState* st) {
+  if (!E || !st || st->n != E->N) return fail(EDM_EINVAL, "edm_stage_state_async: size mismatch");
   if (E->has_phot && !(E->has_dye_host.size() == (size_t)E->N &&
                        std::memcmp(E->has_dye_host.data(), st->has_dye, (size_t)E->N) == 0))
-    return edm_set_state(E, st, stream);
+    return fail(EDM_EINVAL, "edm_stage_state_async: the dye carriers differ from the last upload (edm_set_state)");
   CUDA_TRY(cudaSetDevice(E->device));
   int rc = E->xfer_setup();
   if (rc != EDM_OK) return rc;
-  cudaStream_t s = (cudaStream_t)stream, u = E->up_stream;
+  cudaStream_t u = E->up_stream;
   const int64_t N = E->N;
   const EdmEngine::Xfer& in = E->in;
-  E->cells_valid = false;
-  // the upload waits only for the previous one to leave the staging, not for `stream`
+  // waits only for the previous installation to leave the staging
   if (E->in_used) CUDA_TRY(cudaStreamWaitEvent(u, E->ev_in_free, 0));
   CUDA_TRY(cudaMemcpyAsync(in.pos, st->positions, sizeof(double) * 2 * N, cudaMemcpyHostToDevice, u));
   CUDA_TRY(cudaMemcpyAsync(in.sp, st->species_id, sizeof(int32_t) * N, cudaMemcpyHostToDevice, u));
@@ -1405,7 +1413,19 @@ int edm_set_state_async(EdmEngine* E, const EdmHostState* st, void* stream) {
   CUDA_TRY(cudaMemcpyAsync(in.ctmc, st->ctmc_state, N, cudaMemcpyHostToDevice, u));
   CUDA_TRY(cudaMemcpyAsync(in.bleached, st->is_bleached, N, cudaMemcpyHostToDevice, u));
   CUDA_TRY(cudaEventRecord(E->ev_staged, u));
-  // the installation, in order on `stream`: as edm_set_state from the staging
+  E->staged = true;
+  return EDM_OK;
+}
+
+int edm_install_state(EdmEngine* E, void* stream) {
+  if (!E) return fail(EDM_EINVAL, "edm_install_state: null engine");
+  if (!E->staged) return fail(EDM_EINVAL, "edm_install_state: no staged state");
+  CUDA_TRY(cudaSetDevice(E->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t N = E->N;
+  const EdmEngine::Xfer& in = E->in;
+  E->cells_valid = false;
+  // in order on `stream`: as edm_set_state, from the staging
   CUDA_TRY(cudaStreamWaitEvent(s, E->ev_staged, 0));
   CUDA_TRY(cudaMemcpyAsync(E->bond, in.bond, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, s));
   CUDA_TRY(cudaMemcpyAsync(E->has_dye, in.has_dye, N, cudaMemcpyDeviceToDevice, s));
@@ -1426,8 +1446,20 @@ int edm_set_state_async(EdmEngine* E, const EdmHostState* st, void* stream) {
   }
   CUDA_TRY(cudaEventRecord(E->ev_in_free, s));
   E->in_used = true;
+  E->staged = false;
   CUDA_TRY(cudaGetLastError());
   return EDM_OK;
+}
+
+int edm_set_state_async(EdmEngine* E, const EdmHostState* st, void* stream) {
+  if (!E || !st || st->n != E->N) return fail(EDM_EINVAL, "edm_set_state_async: size mismatch");
+  // new dye carriers rebuild the emitter list on the host: the synchronous path
+  if (E->has_phot && !(E->has_dye_host.size() == (size_t)E->N &&
+                       std::memcmp(E->has_dye_host.data(), st->has_dye, (size_t)E->N) == 0))
+    return edm_set_state(E, st, stream);
+  if (!E->contact_sides_counted && E->hdp[0].n_cat > 0) return edm_set_state(E, st, stream);
+  const int rc = edm_stage_state_async(E, st);
+  return rc != EDM_OK ? rc : edm_install_state(E, stream);
 }
 
 int edm_get_state_async(EdmEngine* E, EdmHostState* st, void* stream) {
@@ -1953,8 +1985,8 @@ int64_t edm_frame_out_sparse(EdmEngine* E, int64_t* idx_host, uint32_t* count_ho
   const int64_t dcap = cap < E->n_flim ? cap : E->n_flim;
   int rc;
   if (!E->sp_bcount) {
-    if ((rc = E->alloc(&E->sp_bcount, kSpBlocks)) != EDM_OK) return rc;
-    if ((rc = E->alloc(&E->sp_off, kSpBlocks + 1)) != EDM_OK) return rc;
+    if ((rc = E->alloc(&E->sp_bcount, kSpWarps)) != EDM_OK) return rc;
+    if ((rc = E->alloc(&E->sp_off, kSpWarps + 1)) != EDM_OK) return rc;
   }
   if (dcap > E->sp_cap) {  // (re)size the device output
     for (auto& a : E->allocs)
@@ -1970,15 +2002,15 @@ int64_t edm_frame_out_sparse(EdmEngine* E, int64_t* idx_host, uint32_t* count_ho
     E->sp_cap = dcap;
   }
   const int64_t n = E->n_flim;
-  const int64_t per = (n + kSpBlocks - 1) / kSpBlocks;
-  const int64_t quantum = 4 * kSpThreads;
+  const int64_t per = (n + kSpWarps - 1) / kSpWarps;
+  const int64_t quantum = 128;  // 4 elements per lane: uint4 loads stay 16-byte aligned
   const int64_t chunk = std::max<int64_t>(quantum, (per + quantum - 1) / quantum * quantum);
   k_sp_count<<<kSpBlocks, kSpThreads, 0, s>>>(E->flim, n, chunk, E->sp_bcount);
-  k_sp_scan<<<1, 1024, 0, s>>>(E->sp_bcount, kSpBlocks, E->sp_off);
-  k_sp_write<<<kSpBlocks, kSpThreads, 0, s>>>(E->flim, n, chunk, E->sp_off, kSpBlocks, E->sp_idx, E->sp_cnt, dcap);
+  k_sp_scan<<<1, 1024, 0, s>>>(E->sp_bcount, kSpWarps, E->sp_off);
+  k_sp_write<<<kSpBlocks, kSpThreads, 0, s>>>(E->flim, n, chunk, E->sp_off, kSpWarps, E->sp_idx, E->sp_cnt, dcap);
   CUDA_TRY(cudaGetLastError());
   int64_t total = 0;
-  CUDA_TRY(cudaMemcpyAsync(&total, E->sp_off + kSpBlocks, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(&total, E->sp_off + kSpWarps, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
   if (total > dcap)
     return fail(EDM_EINVAL, "edm_frame_out_sparse: " + std::to_string((long long)total) +

@@ -556,6 +556,30 @@ __global__ void __launch_bounds__(256, 4) k_hist(EdmFlimParams p, const float* _
   }
 }
 
+// uint32 counts -> T (uint8_t or uint16_t), four per thread per step with
+// 16-byte loads; *over is set when some count does not fit T.
+template <typename T>
+__global__ void k_narrow_counts(const uint32_t* __restrict__ in, int64_t n, T* __restrict__ out,
+                                uint32_t* __restrict__ over) {
+  const uint32_t lim = (uint32_t)(T)~(T)0;
+  bool bad = false;
+  const int64_t n4 = n / 4, stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += stride) {
+    const uint4 v = reinterpret_cast<const uint4*>(in)[q];
+    bad |= (v.x > lim) | (v.y > lim) | (v.z > lim) | (v.w > lim);
+    if constexpr (sizeof(T) == 1)
+      reinterpret_cast<uchar4*>(out)[q] = make_uchar4((uint8_t)v.x, (uint8_t)v.y, (uint8_t)v.z, (uint8_t)v.w);
+    else
+      reinterpret_cast<ushort4*>(out)[q] = make_ushort4((uint16_t)v.x, (uint16_t)v.y, (uint16_t)v.z, (uint16_t)v.w);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0)
+    for (int64_t i = 4 * n4; i < n; ++i) {
+      bad |= in[i] > lim;
+      out[i] = (T)in[i];
+    }
+  if (bad) atomicOr(over, 1u);
+}
+
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda)
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -595,6 +619,9 @@ struct EdmFlim {
   int2* alias = nullptr;
   uint32_t* hist = nullptr;
   uint32_t* err = nullptr;
+  uint8_t* narrow = nullptr;  // narrowed histogram copy (edm_flim_read_hist_narrow)
+  int64_t narrow_bytes = 0;
+  uint32_t* narrow_over = nullptr;
   CUtensorMap mA1, mB1, mA2, mB2;
   int hist_blocks = 148;  // resident k_hist blocks on this device (grid of the grid-stride loop)
   std::vector<void*> allocs;
@@ -783,6 +810,48 @@ int edm_flim_read(EdmFlim* F, int32_t what, int32_t replica, void* host_out, int
   FL_TRY(cudaMemcpyAsync(host_out, (const uint8_t*)base + off, (size_t)n, cudaMemcpyDeviceToHost,
                          (cudaStream_t)stream));
   FL_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  return EDM_OK;
+}
+
+int edm_flim_read_hist_narrow(EdmFlim* F, int32_t replica, int32_t bits, void* host_out, int64_t bytes,
+                              void* stream) {
+  if (!F || !host_out || (bits != 8 && bits != 16)) return fail(EDM_EINVAL, "edm_flim_read_hist_narrow: bad argument");
+  void* base = nullptr;
+  int64_t total = 0;
+  int rc = edm_flim_device_ptr(F, EDM_FLIM_HIST, &base, &total);
+  if (rc != EDM_OK) return rc;
+  int64_t n = total / 4, off = 0;  // elements
+  if (replica >= 0) {
+    if (replica >= F->p.n_replicas) return fail(EDM_EINVAL, "edm_flim_read_hist_narrow: replica out of range");
+    n /= F->p.n_replicas;
+    off = n * replica;
+  }
+  const int64_t nb = n * (bits / 8);
+  if (bytes < nb) return fail(EDM_EINVAL, "edm_flim_read_hist_narrow: host buffer too small");
+  FL_TRY(cudaSetDevice(F->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!F->narrow_over && (rc = falloc(F, &F->narrow_over, 1)) != EDM_OK) return rc;
+  if (F->narrow_bytes < nb) {
+    for (auto& a : F->allocs)
+      if (a == (void*)F->narrow) a = nullptr;
+    FL_TRY(cudaStreamSynchronize(s));
+    cudaFree(F->narrow);
+    F->narrow = nullptr;
+    F->narrow_bytes = 0;
+    if ((rc = falloc(F, &F->narrow, (size_t)nb)) != EDM_OK) return rc;
+    F->narrow_bytes = nb;
+  }
+  const uint32_t* in = (const uint32_t*)base + off;  // replica parts are whole multiples of 4 elements
+  FL_TRY(cudaMemsetAsync(F->narrow_over, 0, sizeof(uint32_t), s));
+  if (bits == 8) k_narrow_counts<uint8_t><<<148 * 8, 256, 0, s>>>(in, n, F->narrow, F->narrow_over);
+  else k_narrow_counts<uint16_t><<<148 * 8, 256, 0, s>>>(in, n, (uint16_t*)F->narrow, F->narrow_over);
+  FL_TRY(cudaGetLastError());
+  uint32_t over = 0;
+  FL_TRY(cudaMemcpyAsync(&over, F->narrow_over, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  FL_TRY(cudaStreamSynchronize(s));
+  if (over) return fail(EDM_ERANGE, "edm_flim_read_hist_narrow: a count exceeds " + std::to_string((1 << bits) - 1));
+  FL_TRY(cudaMemcpyAsync(host_out, F->narrow, (size_t)nb, cudaMemcpyDeviceToHost, s));
+  FL_TRY(cudaStreamSynchronize(s));
   return EDM_OK;
 }
 

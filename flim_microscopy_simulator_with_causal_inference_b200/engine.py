@@ -78,6 +78,8 @@ def load_library():
     L.edm_set_state_async.argtypes = [vp, vp, vp]
     L.edm_get_state_async.argtypes = [vp, vp, vp]
     L.edm_state_transfers_wait.argtypes = [vp]
+    L.edm_stage_state_async.argtypes = [vp, vp]
+    L.edm_install_state.argtypes = [vp, vp]
     L.edm_set_launch_shapes.argtypes = [vp, vp]
     L.edm_record_enable.argtypes = [vp, i32]
     L.edm_record_read.argtypes = [vp, i64, i32, vp, vp]
@@ -99,6 +101,7 @@ def load_library():
     L.edm_flim_acquire.argtypes = [vp, vp]
     L.edm_flim_device_ptr.argtypes = [vp, i32, C.POINTER(vp), C.POINTER(i64)]
     L.edm_flim_read.argtypes = [vp, i32, i32, vp, i64, vp]
+    L.edm_flim_read_hist_narrow.argtypes = [vp, i32, i32, vp, i64, vp]
     L.edm_flim_get_error.argtypes = [vp, C.POINTER(C.c_uint32)]
     L.edm_noise_normal_pairs.argtypes = [u64, i64, i32, vp, i64, vp, vp]
     L.edm_noise_uniforms.argtypes = [u64, i64, i32, vp, vp, i64, vp, vp]
@@ -217,6 +220,21 @@ class Engine:
                              _ptr(arrs["bleached"]))
         self._xfer_refs = getattr(self, "_xfer_refs", []) + [arrs]
         _check(self.L.edm_set_state_async(self.handle, C.byref(hs), _stream_handle(stream)), "edm_set_state_async")
+
+    def stage_state_async(self, arrs: dict):
+        """edm_stage_state_async: the upload half of set_state_async (the
+        arrays go up on the engine's upload stream); install_state() puts the
+        staged state in place on a stream."""
+        self._require(arrs, self.SET_FIELDS, "stage_state_async")
+        hs = PR.EdmHostState(self.N, _ptr(arrs["positions"]), _ptr(arrs["species"]), _ptr(arrs["alive"]),
+                             _ptr(arrs["bond"]), _ptr(arrs["has_dye"]), _ptr(arrs["dye"]), _ptr(arrs["ctmc"]),
+                             _ptr(arrs["bleached"]))
+        self._xfer_refs = getattr(self, "_xfer_refs", []) + [arrs]
+        _check(self.L.edm_stage_state_async(self.handle, C.byref(hs)), "edm_stage_state_async")
+
+    def install_state(self, stream=None):
+        """edm_install_state: the staged state, in order on `stream`."""
+        _check(self.L.edm_install_state(self.handle, _stream_handle(stream)), "edm_install_state")
 
     def get_state_async(self, out: dict, stream=None) -> dict:
         """edm_get_state_async: the state (STATE_FIELDS) comes down on the

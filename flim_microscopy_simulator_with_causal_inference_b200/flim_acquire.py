@@ -193,6 +193,23 @@ class FlimAcquisition:
                                            None))
         return out
 
+    def read_hist_narrow(self, bits: int = 8, replica: int = -1, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """The histograms as `bits`-bit counts (8 or 16), narrowed on the
+        device (edm_flim_read_hist_narrow): lossless, or OverflowError when a
+        count does not fit (read wider then)."""
+        dt = {8: np.uint8, 16: np.uint16}[bits]
+        shape = (NPIX, NPIX, self.n_bins) if replica >= 0 else (self.n_replicas, NPIX, NPIX, self.n_bins)
+        if out is None:
+            out = np.empty(shape, dtype=dt)
+        if out.dtype != dt or out.size != int(np.prod(shape)) or not out.flags.c_contiguous:
+            raise ValueError(f"read_hist_narrow: out must be a contiguous {np.dtype(dt).name} array of {shape}")
+        rc = self.lib.edm_flim_read_hist_narrow(self._h, int(replica), int(bits), out.ctypes.data_as(C.c_void_p),
+                                                out.nbytes, None)
+        if rc == -5:  # EDM_ERANGE
+            raise OverflowError(self.lib.edm_last_error().decode())
+        self._check(rc)
+        return out
+
     def error_word(self) -> int:
         w = C.c_uint32()
         self._check(self.lib.edm_flim_get_error(self._h, C.byref(w)))

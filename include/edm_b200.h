@@ -48,6 +48,7 @@ extern "C" {
 #define EDM_ECUDA -2    /* a CUDA runtime call failed                       */
 #define EDM_ENOMEM -3   /* device allocation failed                         */
 #define EDM_EUNSUP -4   /* feature not supported by this build              */
+#define EDM_ERANGE -5   /* a value does not fit the requested width          */
 
 /* ---- status bits (sticky, per engine) ------------------------------------ */
 #define EDM_STATUS_PHOTON_CAP 0x1u     /* photon stream reached max_photons (reference truncates too) */
@@ -292,6 +293,14 @@ int edm_get_state(EdmEngine* eng, EdmHostState* st, void* stream);
 int edm_set_state_async(EdmEngine* eng, const EdmHostState* st, void* stream);
 int edm_get_state_async(EdmEngine* eng, EdmHostState* st, void* stream);
 int edm_state_transfers_wait(EdmEngine* eng);
+/* edm_set_state_async in two halves, so that a frame loop can start the next
+ * upload before it queues this frame's reads: edm_stage_state_async queues
+ * the host-to-staging copy on the upload stream (after the previous
+ * installation has left the staging; the dye carriers must equal the last
+ * upload's), edm_install_state queues the installation of the staged state
+ * on `stream`. */
+int edm_stage_state_async(EdmEngine* eng, const EdmHostState* st);
+int edm_install_state(EdmEngine* eng, void* stream);
 int edm_set_step(EdmEngine* eng, int64_t step_index);
 int64_t edm_get_step(EdmEngine* eng);
 
@@ -579,6 +588,15 @@ int edm_flim_device_ptr(EdmFlim* flim, int32_t what, void** out, int64_t* bytes)
 int edm_flim_read(EdmFlim* flim, int32_t what, int32_t replica,
                   void* host_out, int64_t bytes, void* stream);
 int edm_flim_get_error(EdmFlim* flim, uint32_t* word);
+/* The histograms (EDM_FLIM_HIST: all replicas, or one when replica >= 0) read
+ * as `bits`-bit counts, bits = 8 or 16, narrowed on the device so 1/4 or 1/2
+ * of the uint32 bytes cross the link; host_out holds one uint8 / uint16 per
+ * bin, in the uint32 array's order.  Lossless or nothing: returns EDM_ERANGE
+ * (host_out then undefined) when some count exceeds 2^bits - 1, and the caller
+ * reads wider.  The first call allocates a device buffer for the narrow copy.
+ * Waits for `stream`. */
+int edm_flim_read_hist_narrow(EdmFlim* flim, int32_t replica, int32_t bits,
+                              void* host_out, int64_t bytes, void* stream);
 
 /* ---- lifetime readouts of TCSPC stacks (analysis.py:87-150, 497-566) ----
  * For a device stack [n_px][n_bins] of uint32 counts (an engine stack from

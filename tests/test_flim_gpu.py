@@ -141,3 +141,29 @@ def test_pixel_totals_are_poisson(acq, ref):
         assert abs(d.sum()) / math.sqrt(lam[m].sum()) < 6.0
         disp = float(((d ** 2) / lam[m]).mean())
         assert abs(disp - 1.0) < 6.0 * math.sqrt(3.0 / m.sum()), (r, disp)
+
+
+def test_narrow_histogram_reads_are_lossless(acq):
+    """edm_flim_read_hist_narrow: 8- and 16-bit reads equal the uint32 counts
+    (all replicas and one replica); a count above 255 makes the 8-bit read
+    refuse, not wrap."""
+    a, hist = acq["acq"], acq["hist"]
+    assert int(hist.max()) <= 255, "this workload's counts fit 8 bits"
+    for bits in (8, 16):
+        np.testing.assert_array_equal(a.read_hist_narrow(bits).astype(np.uint32), hist)
+        np.testing.assert_array_equal(a.read_hist_narrow(bits, replica=2).astype(np.uint32), hist[2])
+
+
+def test_narrow_histogram_read_refuses_overflow():
+    b = FA.FlimAcquisition(FA.flim_config(), 1, n_emitters=50_000, photon_budget=200_000.0, seed=SEED,
+                           bound_fraction=np.array([0.5]))
+    try:
+        b.acquire()
+        h = b.read(FA.HIST)
+        assert int(h.max()) > 255
+        with pytest.raises(OverflowError):
+            b.read_hist_narrow(8)
+        if int(h.max()) <= 65535:
+            np.testing.assert_array_equal(b.read_hist_narrow(16).astype(np.uint32), h)
+    finally:
+        b.close()

@@ -1,7 +1,8 @@
-"""State transfers overlapped with computation (edm_set_state_async,
-edm_get_state_async): a pipelined frame loop (the next frame's state goes up
-while this frame's result comes down) gives, frame by frame, the states the
-synchronous edm_set_state / edm_get_state loop gives."""
+"""State transfers overlapped with computation (edm_set_state_async, or its
+halves edm_stage_state_async + edm_install_state, and edm_get_state_async): a
+pipelined frame loop (the next frame's state goes up while this frame's result
+comes down) gives, frame by frame, the states the synchronous edm_set_state /
+edm_get_state loop gives."""
 import numpy as np
 import pytest
 
@@ -17,7 +18,8 @@ def _pinned(a):
 
 
 @pytest.mark.parametrize("precision", [64, 32])
-def test_pipelined_async_frames_equal_synchronous_frames(precision):
+@pytest.mark.parametrize("split", [False, True])
+def test_pipelined_async_frames_equal_synchronous_frames(precision, split):
     import torch
     raw = cases.get("rich_small")
     A = Pair(raw, precision=precision, photons=True)
@@ -40,12 +42,18 @@ def test_pipelined_async_frames_equal_synchronous_frames(precision):
         A.eng.pipeline_steps(10, True, 10, stream=s)
         want.append(A.eng.get_state(stream=s))
     # pipelined loop: upload frame k + 1 before frame k's result has come down
+    # (split: the upload is queued before this frame's read, the installation after)
     B.eng.set_state_async(pinned, stream=s)
     for k in range(frames):
         B.eng.pipeline_steps(10, True, 10, stream=s)
+        if split and k + 1 < frames:
+            B.eng.stage_state_async(pinned)
         B.eng.get_state_async(outs[k], stream=s)
         if k + 1 < frames:
-            B.eng.set_state_async(pinned, stream=s)
+            if split:
+                B.eng.install_state(stream=s)
+            else:
+                B.eng.set_state_async(pinned, stream=s)
     B.eng.transfers_wait()
     s.synchronize()
     for k in range(frames):
