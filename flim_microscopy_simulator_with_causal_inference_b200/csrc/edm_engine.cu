@@ -1396,6 +1396,7 @@ int edm_stage_state_async(EdmEngine* E, const EdmHostState* st) {
   if (E->has_phot && !(E->has_dye_host.size() == (size_t)E->N &&
                        std::memcmp(E->has_dye_host.data(), st->has_dye, (size_t)E->N) == 0))
     return fail(EDM_EINVAL, "edm_stage_state_async: the dye carriers differ from the last upload (edm_set_state)");
+  if (E->staged) return fail(EDM_EINVAL, "edm_stage_state_async: a staged state waits for edm_install_state");
   CUDA_TRY(cudaSetDevice(E->device));
   int rc = E->xfer_setup();
   if (rc != EDM_OK) return rc;

@@ -297,8 +297,8 @@ int edm_state_transfers_wait(EdmEngine* eng);
  * upload before it queues this frame's reads: edm_stage_state_async queues
  * the host-to-staging copy on the upload stream (after the previous
  * installation has left the staging; the dye carriers must equal the last
- * upload's), edm_install_state queues the installation of the staged state
- * on `stream`. */
+ * upload's; one staged state at a time), edm_install_state queues the
+ * installation of the staged state on `stream`. */
 int edm_stage_state_async(EdmEngine* eng, const EdmHostState* st);
 int edm_install_state(EdmEngine* eng, void* stream);
 int edm_set_step(EdmEngine* eng, int64_t step_index);
