@@ -622,10 +622,16 @@ struct EdmFlim {
   uint8_t* narrow = nullptr;  // narrowed histogram copy (edm_flim_read_hist_narrow)
   int64_t narrow_bytes = 0;
   uint32_t* narrow_over = nullptr;
+  cudaStream_t read_stream = nullptr;  // the overlapped read's copy stream
+  cudaEvent_t ev_narrow = nullptr, ev_read = nullptr;
+  bool read_pending = false;
   CUtensorMap mA1, mB1, mA2, mB2;
   int hist_blocks = 148;  // resident k_hist blocks on this device (grid of the grid-stride loop)
   std::vector<void*> allocs;
   ~EdmFlim() {
+    if (read_stream) cudaStreamDestroy(read_stream);
+    if (ev_narrow) cudaEventDestroy(ev_narrow);
+    if (ev_read) cudaEventDestroy(ev_read);
     for (void* a : allocs) cudaFree(a);
   }
 };
@@ -813,6 +819,74 @@ int edm_flim_read(EdmFlim* F, int32_t what, int32_t replica, void* host_out, int
   return EDM_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// Narrows the histograms [off, off + n) (elements) into F->narrow on `s`,
+// after a pending overlapped read has left it, and waits for the overflow
+// flag: EDM_ERANGE when some count does not fit.
+int narrow_hist(EdmFlim* F, int64_t off, int64_t n, int32_t bits, cudaStream_t s) {
+  const int64_t nb = n * (bits / 8);
+  int rc;
+  if (!F->narrow_over && (rc = falloc(F, &F->narrow_over, 1)) != EDM_OK) return rc;
+  if (F->read_pending) FL_TRY(cudaStreamWaitEvent(s, F->ev_read, 0));
+  if (F->narrow_bytes < nb) {
+    for (auto& a : F->allocs)
+      if (a == (void*)F->narrow) a = nullptr;
+    FL_TRY(cudaStreamSynchronize(s));
+    cudaFree(F->narrow);
+    F->narrow = nullptr;
+    F->narrow_bytes = 0;
+    if ((rc = falloc(F, &F->narrow, (size_t)nb)) != EDM_OK) return rc;
+    F->narrow_bytes = nb;
+  }
+  const uint32_t* in = F->hist + off;  // replica parts are whole multiples of 4 elements
+  FL_TRY(cudaMemsetAsync(F->narrow_over, 0, sizeof(uint32_t), s));
+  if (bits == 8) k_narrow_counts<uint8_t><<<148 * 8, 256, 0, s>>>(in, n, F->narrow, F->narrow_over);
+  else k_narrow_counts<uint16_t><<<148 * 8, 256, 0, s>>>(in, n, (uint16_t*)F->narrow, F->narrow_over);
+  FL_TRY(cudaGetLastError());
+  uint32_t over = 0;
+  FL_TRY(cudaMemcpyAsync(&over, F->narrow_over, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  FL_TRY(cudaStreamSynchronize(s));
+  if (over) return fail(EDM_ERANGE, "edm_flim_read_hist_narrow: a count exceeds " + std::to_string((1 << bits) - 1));
+  return EDM_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int edm_flim_read_hist_narrow_async(EdmFlim* F, int32_t bits, void* host_out, int64_t bytes, void* stream) {
+  if (!F || !host_out || (bits != 8 && bits != 16))
+    return fail(EDM_EINVAL, "edm_flim_read_hist_narrow_async: bad argument");
+  const int64_t n = (int64_t)F->p.n_replicas * kDim * kDim * F->p.n_bins;
+  const int64_t nb = n * (bits / 8);
+  if (bytes < nb) return fail(EDM_EINVAL, "edm_flim_read_hist_narrow_async: host buffer too small");
+  FL_TRY(cudaSetDevice(F->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!F->read_stream) {
+    FL_TRY(cudaStreamCreateWithFlags(&F->read_stream, cudaStreamNonBlocking));
+    FL_TRY(cudaEventCreateWithFlags(&F->ev_narrow, cudaEventDisableTiming));
+    FL_TRY(cudaEventCreateWithFlags(&F->ev_read, cudaEventDisableTiming));
+  }
+  const int rc = narrow_hist(F, 0, n, bits, s);
+  if (rc != EDM_OK) return rc;
+  FL_TRY(cudaEventRecord(F->ev_narrow, s));
+  FL_TRY(cudaStreamWaitEvent(F->read_stream, F->ev_narrow, 0));
+  FL_TRY(cudaMemcpyAsync(host_out, F->narrow, (size_t)nb, cudaMemcpyDeviceToHost, F->read_stream));
+  FL_TRY(cudaEventRecord(F->ev_read, F->read_stream));
+  F->read_pending = true;
+  return EDM_OK;
+}
+
+int edm_flim_read_wait(EdmFlim* F) {
+  if (!F) return fail(EDM_EINVAL, "edm_flim_read_wait: null handle");
+  if (!F->read_pending) return EDM_OK;
+  FL_TRY(cudaSetDevice(F->device));
+  FL_TRY(cudaEventSynchronize(F->ev_read));
+  F->read_pending = false;
+  return EDM_OK;
+}
+
 int edm_flim_read_hist_narrow(EdmFlim* F, int32_t replica, int32_t bits, void* host_out, int64_t bytes,
                               void* stream) {
   if (!F || !host_out || (bits != 8 && bits != 16)) return fail(EDM_EINVAL, "edm_flim_read_hist_narrow: bad argument");
@@ -830,26 +904,8 @@ int edm_flim_read_hist_narrow(EdmFlim* F, int32_t replica, int32_t bits, void* h
   if (bytes < nb) return fail(EDM_EINVAL, "edm_flim_read_hist_narrow: host buffer too small");
   FL_TRY(cudaSetDevice(F->device));
   cudaStream_t s = (cudaStream_t)stream;
-  if (!F->narrow_over && (rc = falloc(F, &F->narrow_over, 1)) != EDM_OK) return rc;
-  if (F->narrow_bytes < nb) {
-    for (auto& a : F->allocs)
-      if (a == (void*)F->narrow) a = nullptr;
-    FL_TRY(cudaStreamSynchronize(s));
-    cudaFree(F->narrow);
-    F->narrow = nullptr;
-    F->narrow_bytes = 0;
-    if ((rc = falloc(F, &F->narrow, (size_t)nb)) != EDM_OK) return rc;
-    F->narrow_bytes = nb;
-  }
-  const uint32_t* in = (const uint32_t*)base + off;  // replica parts are whole multiples of 4 elements
-  FL_TRY(cudaMemsetAsync(F->narrow_over, 0, sizeof(uint32_t), s));
-  if (bits == 8) k_narrow_counts<uint8_t><<<148 * 8, 256, 0, s>>>(in, n, F->narrow, F->narrow_over);
-  else k_narrow_counts<uint16_t><<<148 * 8, 256, 0, s>>>(in, n, (uint16_t*)F->narrow, F->narrow_over);
-  FL_TRY(cudaGetLastError());
-  uint32_t over = 0;
-  FL_TRY(cudaMemcpyAsync(&over, F->narrow_over, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  FL_TRY(cudaStreamSynchronize(s));
-  if (over) return fail(EDM_ERANGE, "edm_flim_read_hist_narrow: a count exceeds " + std::to_string((1 << bits) - 1));
+  rc = narrow_hist(F, off, n, bits, s);
+  if (rc != EDM_OK) return rc;
   FL_TRY(cudaMemcpyAsync(host_out, F->narrow, (size_t)nb, cudaMemcpyDeviceToHost, s));
   FL_TRY(cudaStreamSynchronize(s));
   return EDM_OK;

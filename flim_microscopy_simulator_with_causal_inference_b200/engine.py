@@ -102,6 +102,8 @@ def load_library():
     L.edm_flim_device_ptr.argtypes = [vp, i32, C.POINTER(vp), C.POINTER(i64)]
     L.edm_flim_read.argtypes = [vp, i32, i32, vp, i64, vp]
     L.edm_flim_read_hist_narrow.argtypes = [vp, i32, i32, vp, i64, vp]
+    L.edm_flim_read_hist_narrow_async.argtypes = [vp, i32, vp, i64, vp]
+    L.edm_flim_read_wait.argtypes = [vp]
     L.edm_flim_get_error.argtypes = [vp, C.POINTER(C.c_uint32)]
     L.edm_noise_normal_pairs.argtypes = [u64, i64, i32, vp, i64, vp, vp]
     L.edm_noise_uniforms.argtypes = [u64, i64, i32, vp, vp, i64, vp, vp]

@@ -210,6 +210,27 @@ class FlimAcquisition:
         self._check(rc)
         return out
 
+    def read_hist_narrow_async(self, out: np.ndarray, bits: int = 8, stream: Optional[int] = None) -> None:
+        """edm_flim_read_hist_narrow_async: every replica's histograms as
+        `bits`-bit counts into `out` (pinned, (R, 256, 256, n_bins) of
+        uint8 / uint16), the copy overlapping what `stream` does next; read
+        `out` after read_wait().  OverflowError (before any copy) when a count
+        does not fit."""
+        dt = {8: np.uint8, 16: np.uint16}[bits]
+        if out.dtype != dt or out.size != self.n_replicas * NPIX * NPIX * self.n_bins or not out.flags.c_contiguous:
+            raise ValueError("read_hist_narrow_async: out must be a contiguous array of every bin")
+        self._pending_out = out
+        rc = self.lib.edm_flim_read_hist_narrow_async(self._h, int(bits), out.ctypes.data_as(C.c_void_p),
+                                                      out.nbytes, stream)
+        if rc == -5:  # EDM_ERANGE
+            raise OverflowError(self.lib.edm_last_error().decode())
+        self._check(rc)
+
+    def read_wait(self) -> None:
+        """Wait for the last overlapped histogram read (edm_flim_read_wait)."""
+        self._check(self.lib.edm_flim_read_wait(self._h))
+        self._pending_out = None
+
     def error_word(self) -> int:
         w = C.c_uint32()
         self._check(self.lib.edm_flim_get_error(self._h, C.byref(w)))

@@ -597,6 +597,16 @@ int edm_flim_get_error(EdmFlim* flim, uint32_t* word);
  * Waits for `stream`. */
 int edm_flim_read_hist_narrow(EdmFlim* flim, int32_t replica, int32_t bits,
                               void* host_out, int64_t bytes, void* stream);
+/* The same read of every replica's histograms, overlapped with what `stream`
+ * does next: narrows on `stream` and waits for the overflow check (EDM_ERANGE
+ * as above, before any copy), then copies the narrow array to host_out (one
+ * byte or two per bin, pinned memory) on a copy stream of the handle's own
+ * and returns; the next acquisition may start at once.  A new read (or a
+ * narrow read) waits, on `stream`, for the previous copy to leave the device
+ * buffer; edm_flim_read_wait blocks until the last copy has landed. */
+int edm_flim_read_hist_narrow_async(EdmFlim* flim, int32_t bits, void* host_out,
+                                    int64_t bytes, void* stream);
+int edm_flim_read_wait(EdmFlim* flim);
 
 /* ---- lifetime readouts of TCSPC stacks (analysis.py:87-150, 497-566) ----
  * For a device stack [n_px][n_bins] of uint32 counts (an engine stack from

@@ -168,3 +168,23 @@ def test_narrow_histogram_read_refuses_overflow():
             np.testing.assert_array_equal(b.read_hist_narrow(16).astype(np.uint32), h)
     finally:
         b.close()
+
+
+def test_overlapped_narrow_read_survives_the_next_acquisition(acq):
+    """edm_flim_read_hist_narrow_async: the copy lands the histograms of the
+    acquisition it was issued after, though the next acquisition (another
+    seed) starts at once on the same stream."""
+    import torch
+    a = acq["acq"]
+    s = torch.cuda.Stream()
+    a.acquire(stream=s.cuda_stream)
+    s.synchronize()
+    first = a.read(FA.HIST)
+    out = torch.empty(first.size, dtype=torch.uint8).pin_memory().numpy().reshape(first.shape)
+    a.read_hist_narrow_async(out, 8, stream=s.cuda_stream)
+    a.set_inputs(BOUND, SEED + 99, stream=s.cuda_stream)
+    a.acquire(stream=s.cuda_stream)
+    a.read_wait()
+    s.synchronize()
+    np.testing.assert_array_equal(out.astype(np.uint32), first)
+    assert not np.array_equal(a.read(FA.HIST), first), "the second acquisition should differ"
