@@ -624,10 +624,10 @@ def main():
     # the reactions group's in-graph time.
     cand = {
         "k_scan (3 launches)": (groups["cell_scan"], 20 * n_buckets, "20 B per sort bucket"),
-        "k_scatter": (groups["scatter"], 54 * N, "54 B per slot: 25 B slot record (offset hi + lo, cell, flags, id) "
-                                                 "read + written, 4 B inverse map"),
-        "k_move": (groups["move"], 45 * N, "45 B per slot: 25 B pre-move slot read (offset hi + lo, cell, flags, "
-                                           "id), 20 B offset hi + lo and cell written"),
+        "k_scatter": (groups["scatter"], 46 * N, "46 B per slot: 21 B slot record (offset hi 8 + lo 4, cell, flags, "
+                                                 "id) read + written, 4 B inverse map"),
+        "k_move": (groups["move"], 37 * N, "37 B per slot: 21 B pre-move slot read (offset hi 8 + lo 4, cell, "
+                                           "flags, id), 16 B offset hi + lo and cell written"),
     }
     eager_rx = sum(pm for _, _, pm in passes)
     scale_rx = groups["reactions"] / eager_rx if eager_rx > 0 else 1.0
@@ -742,7 +742,7 @@ def main():
                                    "frame of 100 BD steps",
                        "replicas": args.replicas, "particles": N, "membrane_particles": n_mem,
                        "bd_steps_per_step": STEPS_PER_FRAME, "precision": "f32 cell-relative positions",
-                       "l2": "working set > 126 MB L2 (resident state ~45 B/particle)"},
+                       "l2": "working set > 126 MB L2 (resident state ~37 B/particle)"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "note": "per frame: state H2D from pinned host (edm_set_state_async: uploaded while the "
                             "previous frame computes), 100 BD steps, finalize, state D2H (edm_get_state_async: "

@@ -42,8 +42,8 @@ struct DevState {
   void* pos_post;     // same, after the move
   // f32 path: the float32 remainder of each offset (offset = hi + lo, hi in
   // pos_*); range tests read hi alone, exact arithmetic reads both
-  float2* lo_pre;
-  float2* lo_post;
+  short2* lo_pre;
+  short2* lo_post;
   int32_t* cell_pre;  // reference cell of each slot, before the move
   int32_t* cell_post;
   const uint8_t* flags_old;
@@ -209,19 +209,29 @@ __device__ __forceinline__ void split_cell(int c, const Geo& g, int& cx, int& cy
 }
 
 // float32 path: a cell offset o (float64) is stored as hi = its float32
-// rounding, clamped into [0, cell side), and lo = the float32 rounding of
-// o - hi, so hi + lo keeps about 48 bits of o.
-__device__ __forceinline__ void split_offset(double o, float side_f, float& hi, float& lo) {
+// rounding, clamped into [0, cell side), and lo = o - hi as an int16 count of
+// the quantum q = 2^(e - 37), 2^e <= side < 2^(e + 1).  |o - hi| stays within
+// 1.5 float32 ulps of the side, 3 * 2^13 q, so lo fits, and hi + lo q is
+// within q / 2 of o (3e-13 µm for a 0.165 µm cell).  The scalings by q are
+// exact.
+__device__ __forceinline__ int lo_exponent(float side_f) {
+  return (int)((__float_as_uint(side_f) >> 23) & 0xFFu) - 127 - 37;
+}
+__device__ __forceinline__ double pow2(int e) { return __longlong_as_double((long long)(1023 + e) << 52); }
+__device__ __forceinline__ double lo_value(short l, float side_f) { return (double)l * pow2(lo_exponent(side_f)); }
+__device__ __forceinline__ void split_offset(double o, float side_f, float& hi, short& lo) {
   float h = (float)o;
   if (!(h >= 0.0f)) h = 0.0f;
   else if (h >= side_f) h = __int_as_float(__float_as_int(side_f) - 1);  // largest float below the side
   hi = h;
-  lo = (float)(o - (double)h);
+  int q = __double2int_rn((o - (double)h) * pow2(-lo_exponent(side_f)));
+  q = q > 32767 ? 32767 : (q < -32767 ? -32767 : q);
+  lo = (short)q;
 }
 
 // Absolute position of a slot (float64); lo is the f32 path's remainder array.
 template <bool F64>
-__device__ __forceinline__ void abs_pos(const void* pos, const float2* lo, const int32_t* cell, int64_t s,
+__device__ __forceinline__ void abs_pos(const void* pos, const short2* lo, const int32_t* cell, int64_t s,
                                         const Geo& g, double& x, double& y) {
   if constexpr (F64) {
     const double2 v = ((const double2*)pos)[s];
@@ -229,11 +239,11 @@ __device__ __forceinline__ void abs_pos(const void* pos, const float2* lo, const
     y = v.y;
   } else {
     const float2 v = ((const float2*)pos)[s];
-    const float2 l = lo[s];
+    const short2 l = lo[s];
     int cx, cy;
     split_cell(cell[s], g, cx, cy);
-    x = __dadd_rn(__dmul_rn((double)cx, g.sx), __dadd_rn((double)v.x, (double)l.x));
-    y = __dadd_rn(__dmul_rn((double)cy, g.sy), __dadd_rn((double)v.y, (double)l.y));
+    x = __dadd_rn(__dmul_rn((double)cx, g.sx), __dadd_rn((double)v.x, lo_value(l.x, g.sxf)));
+    y = __dadd_rn(__dmul_rn((double)cy, g.sy), __dadd_rn((double)v.y, lo_value(l.y, g.syf)));
   }
 }
 
@@ -615,9 +625,11 @@ __device__ __forceinline__ void for_each_force_term(const EdmDynParams& p, const
         const float fdy = __fmaf_rn(-(float)dcy, g.syf, oi.y - oj.y);
         const float fdsq = __fmaf_rn(fdx, fdx, fdy * fdy);
         if (!(fdsq < range_sqf)) return;
-        const float2 li = st.lo_pre[s], lj = st.lo_pre[j];
-        dx = (double)(-dcx) * g.sx + (((double)oi.x - (double)oj.x) + ((double)li.x - (double)lj.x));
-        dy = (double)(-dcy) * g.sy + (((double)oi.y - (double)oj.y) + ((double)li.y - (double)lj.y));
+        const short2 li = st.lo_pre[s], lj = st.lo_pre[j];
+        dx = (double)(-dcx) * g.sx +
+             (((double)oi.x - (double)oj.x) + (double)((int)li.x - (int)lj.x) * pow2(lo_exponent(g.sxf)));
+        dy = (double)(-dcy) * g.sy +
+             (((double)oi.y - (double)oj.y) + (double)((int)li.y - (int)lj.y) * pow2(lo_exponent(g.syf)));
         dsq = dx * dx + dy * dy;
         if (!(dsq < range_sq)) return;
       }
@@ -847,11 +859,12 @@ __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restric
     }
     // the new offset in float64 from hi + lo, carried into the next cell
     // against the float64 cell side, then stored as hi + lo again
-    const float2 oh = ((const float2*)st.pos_pre)[s], ol = st.lo_pre[s];
+    const float2 oh = ((const float2*)st.pos_pre)[s];
+    const short2 ol = st.lo_pre[s];
     int cx, cy;
     split_cell(c, g, cx, cy);
-    double ax = ((double)oh.x + (double)ol.x) + ddx;
-    double ay = ((double)oh.y + (double)ol.y) + ddy;
+    double ax = ((double)oh.x + lo_value(ol.x, g.sxf)) + ddx;
+    double ay = ((double)oh.y + lo_value(ol.y, g.syf)) + ddy;
     if (!(ax >= 0.0 && ax < g.sx)) {
       const int k = (int)floor(ax / g.sx);
       cx += k;
@@ -883,7 +896,8 @@ __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restric
       ay = by - (double)cy * g.sy;
     }
     if (!isfinite(ax) || !isfinite(ay)) set_status(st.status, EDM_STATUS_NONFINITE);
-    float2 o, l;
+    float2 o;
+    short2 l;
     split_offset(ax, g.sxf, o.x, l.x);
     split_offset(ay, g.syf, o.y, l.y);
     ((float2*)st.pos_post)[s] = o;
@@ -1387,7 +1401,8 @@ __global__ void k_recruit_apply(const EdmDynParams* __restrict__ P, int n_rep, D
     if constexpr (F64) {
       ((double2*)st.pos_post)[slot] = make_double2(x, y);
     } else {
-      float2 o, l;
+      float2 o;
+      short2 l;
       split_offset(x - (double)cxn * g.sx, g.sxf, o.x, l.x);
       split_offset(y - (double)cyn * g.sy, g.syf, o.y, l.y);
       ((float2*)st.pos_post)[slot] = o;

@@ -122,7 +122,7 @@ struct EdmEngine {
   cudaEvent_t tune_ev[2] = {nullptr, nullptr};
   void* pos_pre = nullptr;
   void* pos_post = nullptr;
-  float2 *lo_pre = nullptr, *lo_post = nullptr;
+  short2 *lo_pre = nullptr, *lo_post = nullptr;
   int32_t *cell_pre = nullptr, *cell_post = nullptr;
   uint8_t* flags[2] = {nullptr, nullptr};
   int32_t* ids[2] = {nullptr, nullptr};
@@ -1203,7 +1203,7 @@ __global__ void __launch_bounds__(kSpThreads) k_sp_write(uint32_t* __restrict__ 
 
 template <bool F64>
 __global__ void k_set_state(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk, const double* pos,
-                            const int32_t* species, const uint8_t* alive, void* pos_post, float2* lo_post,
+                            const int32_t* species, const uint8_t* alive, void* pos_post, short2* lo_post,
                             int32_t* cell_post, uint8_t* flags, int32_t* ids, int32_t* slot_of_id, int32_t* cnt) {
   const Tile t = tile_of(blk);
   const EdmDynParams& p = P[t.r];
@@ -1215,7 +1215,8 @@ __global__ void k_set_state(const EdmDynParams* __restrict__ P, const int2* __re
   if constexpr (F64) {
     ((double2*)pos_post)[s] = make_double2(x, y);
   } else {
-    float2 o, l;
+    float2 o;
+    short2 l;
     split_offset(x - (double)cx * g.sx, g.sxf, o.x, l.x);
     split_offset(y - (double)cy * g.sy, g.syf, o.y, l.y);
     ((float2*)pos_post)[s] = o;
@@ -1231,7 +1232,7 @@ __global__ void k_set_state(const EdmDynParams* __restrict__ P, const int2* __re
 
 template <bool F64>
 __global__ void k_get_state(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk, const void* pos_post,
-                            const float2* lo_post, const int32_t* cell_post, const uint8_t* flags, const int32_t* slot_of_id,
+                            const short2* lo_post, const int32_t* cell_post, const uint8_t* flags, const int32_t* slot_of_id,
                             const int32_t* bond, double* pos, int32_t* species, uint8_t* alive, int32_t* bond_local) {
   const Tile t = tile_of(blk);
   const EdmDynParams& p = P[t.r];
