@@ -381,11 +381,12 @@ __device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
   return z ^ (z >> 31);
 }
 
-// Per-lane uniform stream: xoshiro128** (D. Blackman, S. Vigna, "Scrambled
-// linear pseudorandom number generators", ACM TOMS 47 (2021)) seeded, as its
-// authors recommend, with SplitMix64 outputs of a key unique to (acquisition
-// seed, replica, pixel, lane), so every lane of every pixel has its own
-// reproducible stream.
+// Per-lane uniform stream: xoshiro128++ (D. Blackman, S. Vigna, "Scrambled
+// linear pseudorandom number generators", ACM TOMS 47 (2021); the ++
+// scrambler, rotl(s0 + s3, 7) + s0, needs no multiply, and its 32 output bits
+// are all full-quality) seeded, as its authors recommend, with SplitMix64
+// outputs of a key unique to (acquisition seed, replica, pixel, lane), so
+// every lane of every pixel has its own reproducible stream.
 struct LaneRng {
   uint32_t s0, s1, s2, s3;
   __device__ __forceinline__ LaneRng(uint64_t seed, uint32_t r, uint32_t px, uint32_t lane) {
@@ -400,7 +401,8 @@ struct LaneRng {
     s3 = (uint32_t)(b >> 32) | ((a | b) == 0ull ? 1u : 0u);  // the all-zero state is the one fixed point
   }
   __device__ __forceinline__ uint32_t next() {
-    const uint32_t out = __funnelshift_l(s1 * 5u, s1 * 5u, 7) * 9u;
+    const uint32_t sum = s0 + s3;
+    const uint32_t out = __funnelshift_l(sum, sum, 7) + s0;
     const uint32_t t = s1 << 9;
     s2 ^= s0;
     s3 ^= s1;
