@@ -256,6 +256,7 @@ struct EdmEngine {
     p.ph_fret = ph_fret;
     p.ph_count = ph_count;
     p.flim = flim;
+    p.touch = touch;
     p.d_pstep = d_pstep;
     p.d_batch_key = d_batch_key;
     return p;
@@ -756,6 +757,10 @@ struct EdmEngine {
 
   // overlapped frame readout (edm_frame_out_begin / _wait)
   uint32_t* flim_snap = nullptr;
+  // one bit per 128-bin stretch of the stacks that a count has landed in
+  // since the last clear: the sparse readout visits only these
+  uint32_t* touch = nullptr;
+  int64_t n_touch = 0;  // words
   // sparse frame readout: block counts and offsets, device output of sp_cap entries
   int32_t* sp_bcount = nullptr;
   int64_t* sp_off = nullptr;
@@ -1081,6 +1086,8 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
     ALLOC(E->sp, (size_t)n_replicas);
     CUDA_TRY(cudaMemcpy(E->sp, E->hsp.data(), sizeof(EdmScopeParams) * n_replicas, cudaMemcpyHostToDevice));
     ALLOC(E->flim, (size_t)nfl);
+    E->n_touch = (nfl + 4095) / 4096;
+    ALLOC(E->touch, (size_t)std::max<int64_t>(E->n_touch, 1));  // zeroed, as every allocation
     std::vector<int2> px = tiles(pxfirst, pxcount);
     E->npxblk = (int)px.size();
     ALLOC(E->pxblk, px.size());
@@ -1137,16 +1144,21 @@ __device__ __forceinline__ int sp_nonzero(const uint4& v) {
   return (v.x != 0u) + (v.y != 0u) + (v.z != 0u) + (v.w != 0u);
 }
 
+// Whether the 128-element stretch starting at t0 (a multiple of 128) has been
+// touched since the last clear.
+__device__ __forceinline__ bool sp_touched(const uint32_t* __restrict__ touch, int64_t t0) {
+  return (touch[t0 >> 12] >> ((t0 >> 7) & 31)) & 1u;
+}
+
 __global__ void __launch_bounds__(kSpThreads) k_sp_count(const uint32_t* __restrict__ flim, int64_t n, int64_t chunk,
+                                                         const uint32_t* __restrict__ touch,
                                                          int32_t* __restrict__ wcount) {
   const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const int64_t b0 = w * chunk, b1 = b0 + chunk < n ? b0 + chunk : n;
   int c = 0;
-  for (int64_t i = b0 + 4 * lane; i < b1; i += 256) {  // two loads in flight per lane
-    c += sp_nonzero(sp_load(flim, i, b1));
-    if (i + 128 < b1) c += sp_nonzero(sp_load(flim, i + 128, b1));
-  }
+  for (int64_t t0 = b0; t0 < b1; t0 += 128)  // only the touched stretches (the same test in every lane)
+    if (sp_touched(touch, t0)) c += sp_nonzero(sp_load(flim, t0 + 4 * lane, b1));
   for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
   if (lane == 0) wcount[w] = c;
 }
@@ -1168,6 +1180,7 @@ __global__ void k_sp_scan(const int32_t* __restrict__ bcount, int nb, int64_t* _
 // Emit and clear the nonzero bins; writes nothing (and clears nothing) when
 // the frame holds more nonzero bins than the output's capacity.
 __global__ void __launch_bounds__(kSpThreads) k_sp_write(uint32_t* __restrict__ flim, int64_t n, int64_t chunk,
+                                                         const uint32_t* __restrict__ touch,
                                                          const int64_t* __restrict__ off, int nb,
                                                          int64_t* __restrict__ idx_out, uint32_t* __restrict__ cnt_out,
                                                          int64_t cap) {
@@ -1177,6 +1190,7 @@ __global__ void __launch_bounds__(kSpThreads) k_sp_write(uint32_t* __restrict__ 
   const int64_t b0 = w * chunk, b1 = b0 + chunk < n ? b0 + chunk : n;
   int64_t base = off[w];
   for (int64_t t0 = b0; t0 < b1; t0 += 128) {  // the same trip count in every lane of the warp
+    if (!sp_touched(touch, t0)) continue;
     const int64_t i = t0 + 4 * lane;
     const uint4 v = sp_load(flim, i, b1);
     const int c = sp_nonzero(v);
@@ -1919,8 +1933,9 @@ int edm_scope_finalize(EdmEngine* E, int64_t frame_index, void* stream) {
   CUDA_TRY(cudaSetDevice(E->device));
   cudaStream_t s = (cudaStream_t)stream;
   if (E->npxblk > 0) {
-    k_dark<<<E->npxblk, kBlock, 0, s>>>(E->dp, E->sp, E->pxblk, E->flim, frame_index, E->counters);
-    k_afterpulse<<<E->npxblk, kBlock, 0, s>>>(E->dp, E->sp, E->pxblk, E->flim, frame_index, E->counters);
+    k_dark<<<E->npxblk, kBlock, 0, s>>>(E->dp, E->sp, E->pxblk, E->flim, E->touch, frame_index, E->counters);
+    k_afterpulse<<<E->npxblk, kBlock, 0, s>>>(E->dp, E->sp, E->pxblk, E->flim, E->touch, frame_index,
+                                              E->counters);
   }
   CUDA_TRY(cudaGetLastError());
   return EDM_OK;
@@ -1940,6 +1955,7 @@ int edm_get_flim(EdmEngine* E, int32_t replica, uint32_t* host_out, int64_t n_el
 int edm_reset_flim(EdmEngine* E, void* stream) {
   if (!E || !E->has_scope) return fail(EDM_EINVAL, "edm_reset_flim: engine has no microscope");
   CUDA_TRY(cudaMemsetAsync(E->flim, 0, sizeof(uint32_t) * E->n_flim, (cudaStream_t)stream));
+  CUDA_TRY(cudaMemsetAsync(E->touch, 0, sizeof(uint32_t) * E->n_touch, (cudaStream_t)stream));
   return EDM_OK;
 }
 
@@ -1971,6 +1987,7 @@ int edm_frame_out_begin(EdmEngine* E, uint32_t* host_out, int64_t n_elems, void*
   if (E->read_pending) CUDA_TRY(cudaStreamWaitEvent(s, E->ev_read, 0));  // snapshot free again
   CUDA_TRY(cudaMemcpyAsync(E->flim_snap, E->flim, bytes, cudaMemcpyDeviceToDevice, s));
   CUDA_TRY(cudaMemsetAsync(E->flim, 0, bytes, s));
+  CUDA_TRY(cudaMemsetAsync(E->touch, 0, sizeof(uint32_t) * E->n_touch, s));
   CUDA_TRY(cudaEventRecord(E->ev_snap, s));
   CUDA_TRY(cudaStreamWaitEvent(E->copy_stream, E->ev_snap, 0));
   CUDA_TRY(cudaMemcpyAsync(host_out, E->flim_snap, bytes, cudaMemcpyDeviceToHost, E->copy_stream));
@@ -2007,9 +2024,10 @@ int64_t edm_frame_out_sparse(EdmEngine* E, int64_t* idx_host, uint32_t* count_ho
   const int64_t per = (n + kSpWarps - 1) / kSpWarps;
   const int64_t quantum = 128;  // 4 elements per lane: uint4 loads stay 16-byte aligned
   const int64_t chunk = std::max<int64_t>(quantum, (per + quantum - 1) / quantum * quantum);
-  k_sp_count<<<kSpBlocks, kSpThreads, 0, s>>>(E->flim, n, chunk, E->sp_bcount);
+  k_sp_count<<<kSpBlocks, kSpThreads, 0, s>>>(E->flim, n, chunk, E->touch, E->sp_bcount);
   k_sp_scan<<<1, 1024, 0, s>>>(E->sp_bcount, kSpWarps, E->sp_off);
-  k_sp_write<<<kSpBlocks, kSpThreads, 0, s>>>(E->flim, n, chunk, E->sp_off, kSpWarps, E->sp_idx, E->sp_cnt, dcap);
+  k_sp_write<<<kSpBlocks, kSpThreads, 0, s>>>(E->flim, n, chunk, E->touch, E->sp_off, kSpWarps, E->sp_idx, E->sp_cnt,
+                                              dcap);
   CUDA_TRY(cudaGetLastError());
   int64_t total = 0;
   CUDA_TRY(cudaMemcpyAsync(&total, E->sp_off + kSpWarps, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
@@ -2017,6 +2035,7 @@ int64_t edm_frame_out_sparse(EdmEngine* E, int64_t* idx_host, uint32_t* count_ho
   if (total > dcap)
     return fail(EDM_EINVAL, "edm_frame_out_sparse: " + std::to_string((long long)total) +
                                 " nonzero bins exceed the capacity; the stacks are left in place");
+  CUDA_TRY(cudaMemsetAsync(E->touch, 0, sizeof(uint32_t) * E->n_touch, s));  // every touched bin is cleared
   if (total > 0) {
     CUDA_TRY(cudaMemcpyAsync(idx_host, E->sp_idx, sizeof(int64_t) * total, cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaMemcpyAsync(count_host, E->sp_cnt, sizeof(uint32_t) * total, cudaMemcpyDeviceToHost, s));

@@ -19,6 +19,12 @@ namespace edm {
 
 constexpr int kPsfMaxR = 16;  // largest PSF window half-width in pixels (4 sigma / pixel, rounded up)
 
+// Mark the 128-element stretch of the stacks holding element e as touched
+// (the sparse readout visits only touched stretches).
+__device__ __forceinline__ void touch_stretch(uint32_t* touch, int64_t e) {
+  if (touch) atomicOr(&touch[e >> 12], 1u << ((e >> 7) & 31));
+}
+
 struct PhotState {
   const int32_t* emit_id;   // global particle id of each emitter (particle order per replica)
   int32_t* emit_n;          // photons (donor + acceptor) of the current batch
@@ -36,6 +42,7 @@ struct PhotState {
   uint8_t* ph_fret;
   int64_t* ph_count;        // [R] photons of the batch (after the max_photons cap)
   uint32_t* flim;
+  uint32_t* touch;          // one bit per 128-bin stretch of flim that a count has landed in
   int64_t* d_pstep;         // photophysics call counter
   int64_t* d_batch_key;     // key of the last batch
 };
@@ -414,7 +421,9 @@ __global__ void __launch_bounds__(kBlock) k_scope(const EdmDynParams* __restrict
   if (tt < 0.0) tt = 0.0;
   const int64_t b = (int64_t)__ddiv_rn(tt, sp.bin_width);
   if (b >= sp.n_bins) return;
-  atomicAdd(&ph.flim[sp.flim_offset + (((int64_t)ch * sp.nx + si) * sp.ny + sj) * sp.n_bins + b], 1u);
+  const int64_t e = sp.flim_offset + (((int64_t)ch * sp.nx + si) * sp.ny + sj) * sp.n_bins + b;
+  atomicAdd(&ph.flim[e], 1u);
+  touch_stretch(ph.touch, e);
 }
 
 // Photons received per replica (microscope.py:1093).
@@ -426,7 +435,8 @@ __global__ void k_scope_received(const EdmPhotParams* __restrict__ PP, int n_rep
 // Dark counts (microscope.py:850-887) — one thread per (channel, pixel).
 __global__ void __launch_bounds__(kBlock) k_dark(const EdmDynParams* __restrict__ DP,
                                                  const EdmScopeParams* __restrict__ SP, const int2* __restrict__ pxblk,
-                                                 uint32_t* flim, int64_t frame, int64_t* counters) {
+                                                 uint32_t* flim, uint32_t* touch, int64_t frame,
+                                                 int64_t* counters) {
   const Tile t = tile_of(pxblk);
   const EdmScopeParams& sp = SP[t.r];
   const int64_t q = t.s;
@@ -440,10 +450,12 @@ __global__ void __launch_bounds__(kBlock) k_dark(const EdmDynParams* __restrict_
     if (pr <= sp.dark_exp_neg) break;
     ++n;
   }
-  uint32_t* px = flim + sp.flim_offset + q * sp.n_bins;
+  const int64_t e0 = sp.flim_offset + q * sp.n_bins;
   for (int64_t m = 0; m < n; ++m) {
     const double u = uniform1(seed, frame, EDM_S_SC_DARK_BIN, (uint64_t)q, (uint64_t)m);
-    px[(int64_t)(u * (double)sp.n_bins)] += 1u;
+    const int64_t e = e0 + (int64_t)(u * (double)sp.n_bins);
+    flim[e] += 1u;
+    touch_stretch(touch, e);
   }
   if (n) atomic_add_i64(counters + (int64_t)t.r * EDM_NCOUNTERS + EDM_C_DARK, n);
 }
@@ -451,8 +463,8 @@ __global__ void __launch_bounds__(kBlock) k_dark(const EdmDynParams* __restrict_
 // Afterpulsing (microscope.py:889-922): Binomial(total, p) as keyed Bernoullis.
 __global__ void __launch_bounds__(kBlock) k_afterpulse(const EdmDynParams* __restrict__ DP,
                                                        const EdmScopeParams* __restrict__ SP,
-                                                       const int2* __restrict__ pxblk, uint32_t* flim, int64_t frame,
-                                                       int64_t* counters) {
+                                                       const int2* __restrict__ pxblk, uint32_t* flim,
+                                                       uint32_t* touch, int64_t frame, int64_t* counters) {
   const Tile t = tile_of(pxblk);
   const EdmScopeParams& sp = SP[t.r];
   const int64_t q = t.s;
@@ -468,7 +480,9 @@ __global__ void __launch_bounds__(kBlock) k_afterpulse(const EdmDynParams* __res
     if (uniform1(seed, frame, EDM_S_SC_AP, (uint64_t)q, (uint64_t)m) < sp.ap_prob) ++n;
   for (int64_t m = 0; m < n; ++m) {
     const double u = uniform1(seed, frame, EDM_S_SC_AP_BIN, (uint64_t)q, (uint64_t)m);
-    px[(int64_t)(u * (double)sp.n_bins)] += 1u;
+    const int64_t b = (int64_t)(u * (double)sp.n_bins);
+    px[b] += 1u;
+    touch_stretch(touch, sp.flim_offset + q * sp.n_bins + b);
   }
   if (n) atomic_add_i64(counters + (int64_t)t.r * EDM_NCOUNTERS + EDM_C_AFTERPULSE, n);
 }

@@ -79,3 +79,27 @@ def test_sparse_frame_out_beyond_capacity_leaves_the_stacks():
         eng.frame_out_sparse(idx, cnt, stream=s)
     after = np.concatenate([eng.flim(r).ravel() for r in range(ens.R)])
     np.testing.assert_array_equal(after, before)
+
+
+def test_sparse_frame_out_sees_dark_counts_and_afterpulses():
+    """Every writer of the stacks marks the stretches it touches: the
+    detection pass, dark counts and afterpulsing (rich_small has both, at high
+    rates), so the sparse read equals the dense stacks."""
+    from tests import cases
+    from tests.harness import Pair
+    P = Pair(cases.get("rich_small"), precision=32, photons=True)
+    eng = P.eng
+    n = eng.flim_elems()
+    idx = np.zeros(n, dtype=np.int64)
+    cnt = np.zeros(n, dtype=np.uint32)
+    s = torch.cuda.Stream()
+    for frame in range(2):
+        eng.pipeline_steps(30, True, 30, stream=s)
+        eng.finalize(frame, stream=s)
+        s.synchronize()
+        expect = eng.flim(0).ravel().copy()
+        c = eng.counters()[0]
+        assert c[11] > 0 and c[12] > 0, "the system should produce dark counts and afterpulses"
+        nnz = eng.frame_out_sparse(idx, cnt, stream=s)
+        assert nnz == int(np.count_nonzero(expect)) > 0
+        np.testing.assert_array_equal(eng.sparse_to_dense(idx, cnt, nnz, n), expect)
