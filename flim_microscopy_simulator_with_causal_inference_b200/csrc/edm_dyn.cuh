@@ -88,6 +88,8 @@ struct DevState {
   int4* pl;
   int32_t* pl_count;
   int32_t* pl_index;
+  // per species: the density grids (bit g) that sense it in some replica
+  uint32_t sensor_grids[EDM_MAX_SPECIES];
   // the contact search's sweepers of this step (k_sweep_list), block by block
   int32_t* sw_list;
   int32_t* sw_count;
@@ -908,7 +910,11 @@ __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restric
   }
   st.cell_post[s] = newc;
   atomicAdd(&st.cnt_next[g.cbase + newc], 1);  // result unused: a fire-and-forget reduction
-  grid_add(p, st.grid_cnt, sp, x, y, 1);
+  // grid_add over only the grids that can sense this species (most species have none)
+  for (uint32_t gm = st.sensor_grids[sp]; gm; gm &= gm - 1) {
+    const int gi = __ffs(gm) - 1;
+    if (p.grid[gi].sensor == sp) atomicAdd(&st.grid_cnt[grid_cell_of(p.grid[gi], x, y)], 1);
+  }
 }
 
 // =============================================================================

@@ -175,6 +175,7 @@ struct EdmEngine {
   int4* pl = nullptr;  // listed particles of the per-particle passes: (slot, pass bits, replica, id)
   int32_t *pl_count = nullptr, *pl_index = nullptr;
   int32_t *sw_list = nullptr, *sw_count = nullptr;  // the contact search's sweeper list
+  uint32_t sensor_grids[EDM_MAX_SPECIES] = {};  // per species: the grids that sense it in some replica
   double *adapt_w = nullptr, *local_cdf = nullptr;  // per global grid cell
   std::vector<int32_t> emit_host;  // emitter list last uploaded
   std::vector<uint8_t> has_dye_host;  // has_dye of the last edm_set_state
@@ -229,6 +230,7 @@ struct EdmEngine {
     s.pl = pl;
     s.pl_count = pl_count;
     s.pl_index = pl_index;
+    for (int sp = 0; sp < EDM_MAX_SPECIES; ++sp) s.sensor_grids[sp] = sensor_grids[sp];
     s.sw_list = sw_list;
     s.sw_count = sw_count;
     s.adapt_w = adapt_w;
@@ -1009,6 +1011,9 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
   ALLOC(E->bind_count, n_replicas);
   ALLOC(E->bind_key, (size_t)n_replicas * kBindCap);
   ALLOC(E->bind_ab, (size_t)n_replicas * kBindCap * 2);
+  for (const EdmDynParams& q : E->hdp)
+    for (int g = 0; g < q.n_grids && g < EDM_MAX_GRIDS; ++g)
+      if (q.grid[g].sensor >= 0 && q.grid[g].sensor < EDM_MAX_SPECIES) E->sensor_grids[q.grid[g].sensor] |= 1u << g;
   if ((rc = E->build_schedule()) != EDM_OK || (rc = E->upload_thresholds()) != EDM_OK) {
     delete E;
     return rc;
