@@ -146,6 +146,7 @@ struct EdmEngine {
   double* ph_t = nullptr;
   int8_t* ph_ch = nullptr;
   uint8_t* ph_fret = nullptr;
+  double2* ph_xy = nullptr;
   int64_t* ph_count = nullptr;
   uint32_t* flim = nullptr;
   // host staging for get_state
@@ -256,6 +257,7 @@ struct EdmEngine {
     p.ph_t = ph_t;
     p.ph_ch = ph_ch;
     p.ph_fret = ph_fret;
+    p.ph_xy = ph_xy;
     p.ph_count = ph_count;
     p.flim = flim;
     p.touch = touch;
@@ -710,7 +712,7 @@ struct EdmEngine {
     PhotState ph = phot_state();
     if (neblk > 0) k_phot_count<F64><<<neblk, kBlock, 0, s>>>(dp, pp, eblk, st, ph, cells_valid ? 1 : 0);
     k_phot_scan<<<R, 256, 0, s>>>(pp, ph, counters, status);
-    if (neblk > 0) k_phot_write<<<neblk, kBlock, 0, s>>>(dp, pp, eblk, ph, counters);
+    if (neblk > 0) k_phot_write<F64><<<neblk, kBlock, 0, s>>>(dp, pp, eblk, st, ph, counters);
     k_phot_advance<<<1, 1, 0, s>>>(d_pstep, d_batch_key);
   }
 
@@ -730,6 +732,35 @@ struct EdmEngine {
   void enqueue_scope(cudaStream_t s) {
     if (f64) enqueue_scope_t<true>(s);
     else enqueue_scope_t<false>(s);
+  }
+
+  // The positions of the current photon batch from the current state (a batch
+  // the host set, before a standalone detection pass).
+  void enqueue_photon_positions(cudaStream_t s) {
+    if (nphblk == 0) return;
+    DevState st = dev_state();
+    PhotState ph = phot_state();
+    if (f64) k_photon_positions<true><<<nphblk, kBlock, 0, s>>>(dp, pp, phblk, st, ph);
+    else k_photon_positions<false><<<nphblk, kBlock, 0, s>>>(dp, pp, phblk, st, ph);
+  }
+
+  // A step's detection pass beside the next step on a stream of its own (it
+  // reads only the photon records, which carry their positions); the next
+  // photon pass, a census, and the end of the call wait for it.
+  cudaStream_t scope_stream = nullptr;
+  cudaEvent_t ev_scope_fork = nullptr, ev_scope_join = nullptr;
+  bool scope_pending = false;
+  void enqueue_scope_beside(cudaStream_t s) {  // errors surface at the call's cudaGetLastError / capture end
+    cudaEventRecord(ev_scope_fork, s);
+    cudaStreamWaitEvent(scope_stream, ev_scope_fork, 0);
+    enqueue_scope(scope_stream);
+    cudaEventRecord(ev_scope_join, scope_stream);
+    scope_pending = true;
+  }
+  void join_scope(cudaStream_t s) {
+    if (!scope_pending) return;
+    cudaStreamWaitEvent(s, ev_scope_join, 0);
+    scope_pending = false;
   }
 
   // Census of the state into `base` (ring of `cap` steps, or one block when
@@ -814,6 +845,9 @@ struct EdmEngine {
     if (ev_read) cudaEventDestroy(ev_read);
     if (copy_stream) cudaStreamDestroy(copy_stream);
     if (up_stream) cudaStreamDestroy(up_stream);
+    if (scope_stream) cudaStreamDestroy(scope_stream);
+    if (ev_scope_fork) cudaEventDestroy(ev_scope_fork);
+    if (ev_scope_join) cudaEventDestroy(ev_scope_join);
     if (down_stream) cudaStreamDestroy(down_stream);
     for (cudaEvent_t ev : {ev_staged, ev_in_free, ev_out_ready, ev_out_free})
       if (ev) cudaEventDestroy(ev);
@@ -1018,6 +1052,11 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
     delete E;
     return rc;
   }
+  if (E->has_scope) {
+    CUDA_TRY(cudaStreamCreateWithFlags(&E->scope_stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&E->ev_scope_fork, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&E->ev_scope_join, cudaEventDisableTiming));
+  }
   if (E->draws_early) {
     CUDA_TRY(cudaStreamCreateWithFlags(&E->side_stream, cudaStreamNonBlocking));
     CUDA_TRY(cudaEventCreateWithFlags(&E->ev_fork, cudaEventDisableTiming));
@@ -1080,6 +1119,7 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
     ALLOC(E->ph_t, nph);
     ALLOC(E->ph_ch, nph);
     ALLOC(E->ph_fret, nph);
+    ALLOC(E->ph_xy, nph);
     ALLOC(E->ph_count, n_replicas);
     std::vector<int2> ph = tiles(phfirst, phcount);
     E->nphblk = (int)ph.size();
@@ -1591,6 +1631,7 @@ int edm_get_photons(EdmEngine* E, int32_t replica, int32_t* particle_idx, double
 int edm_scope_process(EdmEngine* E, void* stream) {
   if (!E || !E->has_scope) return fail(EDM_EINVAL, "edm_scope_process: engine has no microscope");
   CUDA_TRY(cudaSetDevice(E->device));
+  E->enqueue_photon_positions((cudaStream_t)stream);  // the batch may come from the host
   E->enqueue_scope((cudaStream_t)stream);
   CUDA_TRY(cudaGetLastError());
   return EDM_OK;
@@ -1623,12 +1664,16 @@ int edm_pipeline_steps(EdmEngine* E, int32_t n_steps, int32_t with_photons, int3
   CUDA_TRY(cudaSetDevice(E->device));
   cudaStream_t s = (cudaStream_t)stream;
   auto body = [&](cudaStream_t st) {
-    E->enqueue_dynamics(st);
+    E->enqueue_dynamics(st);  // beside the previous step's detection pass
     if (with_photons) {
+      E->join_scope(st);  // that pass leaves the photon records to this step's photon pass
       E->enqueue_photons(st);
-      E->enqueue_scope(st);
+      E->enqueue_scope_beside(st);
     }
-    if (E->rec_cap > 0) E->enqueue_census(st, E->rec_ring, E->rec_cap, with_photons != 0);
+    if (E->rec_cap > 0) {
+      E->join_scope(st);  // the census reads the detection counters
+      E->enqueue_census(st, E->rec_ring, E->rec_cap, with_photons != 0);
+    }
   };
   int done = 0;
   if (graph_chunk > 0 && s != nullptr) {
@@ -1640,6 +1685,7 @@ int edm_pipeline_steps(EdmEngine* E, int32_t n_steps, int32_t with_photons, int3
         cudaGraph_t g;
         CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         for (int i = 0; i < graph_chunk; ++i) body(s);
+        E->join_scope(s);  // the capture ends on the origin stream
         CUDA_TRY(cudaStreamEndCapture(s, &g));
         cudaGraphExec_t ge;
         CUDA_TRY(cudaGraphInstantiate(&ge, g, 0));
@@ -1653,6 +1699,7 @@ int edm_pipeline_steps(EdmEngine* E, int32_t n_steps, int32_t with_photons, int3
     }
   }
   for (; done < n_steps; ++done) body(s);
+  E->join_scope(s);  // whatever the caller queues next sees the detection pass done
   CUDA_TRY(cudaGetLastError());
   return EDM_OK;
 }

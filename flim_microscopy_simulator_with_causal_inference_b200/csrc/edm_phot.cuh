@@ -40,6 +40,7 @@ struct PhotState {
   double* ph_t;
   int8_t* ph_ch;
   uint8_t* ph_fret;
+  double2* ph_xy;           // the emitting particle's position when the photon was written
   int64_t* ph_count;        // [R] photons of the batch (after the max_photons cap)
   uint32_t* flim;
   uint32_t* touch;          // one bit per 128-bin stretch of flim that a count has landed in
@@ -268,9 +269,22 @@ __global__ void k_phot_scan(const EdmPhotParams* __restrict__ PP, PhotState ph, 
 }
 
 // Write the photons of each emitter (photophysics.py:433-472).
+// Absolute position of the particle with replica-local index pid.
+template <bool F64>
+__device__ __forceinline__ double2 particle_pos(const DevState& st, const Geo& g, int pid) {
+  double x, y;
+  abs_pos<F64>(st.pos_post, st.lo_post, st.cell_post, st.slot_of_id[g.poff + pid], g, x, y);
+  return make_double2(x, y);
+}
+
+// The photon records, each with the position of the particle it leaves
+// (the donor, or the acceptor of a FRET photon), so the detection pass reads
+// no particle state and can run beside the next step.
+template <bool F64>
 __global__ void __launch_bounds__(kBlock) k_phot_write(const EdmDynParams* __restrict__ DP,
                                                        const EdmPhotParams* __restrict__ PP,
-                                                       const int2* __restrict__ eblk, PhotState ph, int64_t* counters) {
+                                                       const int2* __restrict__ eblk, DevState st, PhotState ph,
+                                                       int64_t* counters) {
   const Tile t = tile_of(eblk);
   const EdmPhotParams& pp = PP[t.r];
   const int64_t e = t.s;
@@ -286,6 +300,10 @@ __global__ void __launch_bounds__(kBlock) k_phot_write(const EdmDynParams* __res
   const double tau = pp.tau[dt][cls];
   const int64_t off = ph.emit_off[e];
   const int64_t key = *ph.d_pstep;
+  const Geo g(p);
+  const double2 xy_donor = particle_pos<F64>(st, g, lid);
+  double2 xy_acc = xy_donor;
+  bool have_acc = false;
   int n_donor_ch = 0, n_acc_ch = 0, n_fret = 0;
   for (int j = 0; j < ntot; ++j) {
     const int64_t k = off + j;
@@ -309,6 +327,11 @@ __global__ void __launch_bounds__(kBlock) k_phot_write(const EdmDynParams* __res
       tt = ta;
     }
     const int64_t o = pp.photon_offset + k;
+    if (fret && !have_acc && pid >= 0 && pid < p.n_particles) {
+      xy_acc = particle_pos<F64>(st, g, pid);
+      have_acc = true;
+    }
+    ph.ph_xy[o] = fret ? xy_acc : xy_donor;
     ph.ph_pid[o] = pid;
     ph.ph_t[o] = tt;
     ph.ph_ch[o] = (int8_t)ch;
@@ -345,10 +368,8 @@ __global__ void __launch_bounds__(kBlock) k_scope(const EdmDynParams* __restrict
   if (!(uniform1(p.seed, key, EDM_S_SC_QE, (uint64_t)k, 0) < sp.qe)) return;
   const int pid = ph.ph_pid[o];
   if (pid < 0 || pid >= p.n_particles) return;
-  const Geo g(p);
-  const int64_t slot = st.slot_of_id[g.poff + pid];
-  double x, y;
-  abs_pos<F64>(st.pos_post, st.lo_post, st.cell_post, slot, g, x, y);
+  const double2 xy = ph.ph_xy[o];
+  const double x = xy.x, y = xy.y;
   int ch = ph.ph_ch[o];
   int chs = ch;
   if (chs < 0) chs = 0;
@@ -424,6 +445,24 @@ __global__ void __launch_bounds__(kBlock) k_scope(const EdmDynParams* __restrict
   const int64_t e = sp.flim_offset + (((int64_t)ch * sp.nx + si) * sp.ny + sj) * sp.n_bins + b;
   atomicAdd(&ph.flim[e], 1u);
   touch_stretch(ph.touch, e);
+}
+
+// The positions of a photon batch set from the host (edm_set_photons) or left
+// by an earlier pass: each photon's particle, from the current state.
+template <bool F64>
+__global__ void __launch_bounds__(kBlock) k_photon_positions(const EdmDynParams* __restrict__ DP,
+                                                             const EdmPhotParams* __restrict__ PP,
+                                                             const int2* __restrict__ phblk, DevState st,
+                                                             PhotState ph) {
+  const Tile t = tile_of(phblk);
+  const EdmPhotParams& pp = PP[t.r];
+  const int64_t k = t.s - pp.photon_offset;
+  if (k >= ph.ph_count[t.r]) return;
+  const EdmDynParams& p = DP[t.r];
+  const int pid = ph.ph_pid[t.s];
+  if (pid < 0 || pid >= p.n_particles) return;
+  const Geo g(p);
+  ph.ph_xy[t.s] = particle_pos<F64>(st, g, pid);
 }
 
 // Photons received per replica (microscope.py:1093).
