@@ -622,6 +622,7 @@ struct EdmEngine {
     z.p[5] = sw_count, z.n[5] = sw_count ? 1 : 0;
     k_scan_reduce<<<nbs, kScanThreads, 0, s>>>(cnt, n_cells, bsum, z);
     k_scan_bsum<<<1, 1024, 0, s>>>(bsum, nbs);
+    join_photons(s);  // the previous step's photon pass reads the cell list and slots about to change
     k_scan_down<<<nbs, kScanThreads, 0, s>>>(cnt, n_cells, bsum, cell_start, cursor);
     mark(1, s);
     cur ^= 1;
@@ -744,20 +745,35 @@ struct EdmEngine {
     else k_photon_positions<false><<<nphblk, kBlock, 0, s>>>(dp, pp, phblk, st, ph);
   }
 
-  // A step's detection pass beside the next step on a stream of its own (it
-  // reads only the photon records, which carry their positions); the next
-  // photon pass, a census, and the end of the call wait for it.
-  cudaStream_t scope_stream = nullptr;
-  cudaEvent_t ev_scope_fork = nullptr, ev_scope_join = nullptr;
-  bool scope_pending = false;
-  void enqueue_scope_beside(cudaStream_t s) {  // errors surface at the call's cudaGetLastError / capture end
-    cudaEventRecord(ev_scope_fork, s);
-    cudaStreamWaitEvent(scope_stream, ev_scope_fork, 0);
+  // A step's photon pass and detection pass beside the next step, each on a
+  // stream of its own.  The photon pass reads the step's final state: the next
+  // step's bucket scan may run beside it, its bucket starts and sort may not
+  // (enqueue_dynamics joins it before them).  The detection pass reads only the
+  // photon records, which carry their positions: the next step's dynamics run
+  // beside it, the next photon pass waits for it.  A census and the end of the
+  // call wait for both.  Errors surface at the call's cudaGetLastError or at
+  // the capture's end.
+  cudaStream_t phot_stream = nullptr, scope_stream = nullptr;
+  cudaEvent_t ev_phot_fork = nullptr, ev_phot_join = nullptr, ev_scope_join = nullptr;
+  bool phot_pending = false, scope_pending = false;
+  void enqueue_photons_beside(cudaStream_t s) {
+    cudaEventRecord(ev_phot_fork, s);
+    cudaStreamWaitEvent(phot_stream, ev_phot_fork, 0);
+    if (scope_pending) cudaStreamWaitEvent(phot_stream, ev_scope_join, 0);  // the records are free again
+    enqueue_photons(phot_stream);
+    cudaEventRecord(ev_phot_join, phot_stream);
+    cudaStreamWaitEvent(scope_stream, ev_phot_join, 0);
     enqueue_scope(scope_stream);
     cudaEventRecord(ev_scope_join, scope_stream);
-    scope_pending = true;
+    phot_pending = scope_pending = true;
   }
-  void join_scope(cudaStream_t s) {
+  void join_photons(cudaStream_t s) {
+    if (!phot_pending) return;
+    cudaStreamWaitEvent(s, ev_phot_join, 0);
+    phot_pending = false;
+  }
+  void join_beside(cudaStream_t s) {
+    join_photons(s);
     if (!scope_pending) return;
     cudaStreamWaitEvent(s, ev_scope_join, 0);
     scope_pending = false;
@@ -845,9 +861,10 @@ struct EdmEngine {
     if (ev_read) cudaEventDestroy(ev_read);
     if (copy_stream) cudaStreamDestroy(copy_stream);
     if (up_stream) cudaStreamDestroy(up_stream);
+    if (phot_stream) cudaStreamDestroy(phot_stream);
     if (scope_stream) cudaStreamDestroy(scope_stream);
-    if (ev_scope_fork) cudaEventDestroy(ev_scope_fork);
-    if (ev_scope_join) cudaEventDestroy(ev_scope_join);
+    for (cudaEvent_t ev : {ev_phot_fork, ev_phot_join, ev_scope_join})
+      if (ev) cudaEventDestroy(ev);
     if (down_stream) cudaStreamDestroy(down_stream);
     for (cudaEvent_t ev : {ev_staged, ev_in_free, ev_out_ready, ev_out_free})
       if (ev) cudaEventDestroy(ev);
@@ -1053,8 +1070,10 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
     return rc;
   }
   if (E->has_scope) {
+    CUDA_TRY(cudaStreamCreateWithFlags(&E->phot_stream, cudaStreamNonBlocking));
     CUDA_TRY(cudaStreamCreateWithFlags(&E->scope_stream, cudaStreamNonBlocking));
-    CUDA_TRY(cudaEventCreateWithFlags(&E->ev_scope_fork, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&E->ev_phot_fork, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&E->ev_phot_join, cudaEventDisableTiming));
     CUDA_TRY(cudaEventCreateWithFlags(&E->ev_scope_join, cudaEventDisableTiming));
   }
   if (E->draws_early) {
@@ -1664,14 +1683,10 @@ int edm_pipeline_steps(EdmEngine* E, int32_t n_steps, int32_t with_photons, int3
   CUDA_TRY(cudaSetDevice(E->device));
   cudaStream_t s = (cudaStream_t)stream;
   auto body = [&](cudaStream_t st) {
-    E->enqueue_dynamics(st);  // beside the previous step's detection pass
-    if (with_photons) {
-      E->join_scope(st);  // that pass leaves the photon records to this step's photon pass
-      E->enqueue_photons(st);
-      E->enqueue_scope_beside(st);
-    }
+    E->enqueue_dynamics(st);  // beside the previous step's photon and detection passes
+    if (with_photons) E->enqueue_photons_beside(st);
     if (E->rec_cap > 0) {
-      E->join_scope(st);  // the census reads the detection counters
+      E->join_beside(st);  // the census reads the photon state and the detection counters
       E->enqueue_census(st, E->rec_ring, E->rec_cap, with_photons != 0);
     }
   };
@@ -1685,7 +1700,7 @@ int edm_pipeline_steps(EdmEngine* E, int32_t n_steps, int32_t with_photons, int3
         cudaGraph_t g;
         CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         for (int i = 0; i < graph_chunk; ++i) body(s);
-        E->join_scope(s);  // the capture ends on the origin stream
+        E->join_beside(s);  // the capture ends on the origin stream
         CUDA_TRY(cudaStreamEndCapture(s, &g));
         cudaGraphExec_t ge;
         CUDA_TRY(cudaGraphInstantiate(&ge, g, 0));
@@ -1699,7 +1714,7 @@ int edm_pipeline_steps(EdmEngine* E, int32_t n_steps, int32_t with_photons, int3
     }
   }
   for (; done < n_steps; ++done) body(s);
-  E->join_scope(s);  // whatever the caller queues next sees the detection pass done
+  E->join_beside(s);  // whatever the caller queues next sees the photon and detection passes done
   CUDA_TRY(cudaGetLastError());
   return EDM_OK;
 }
