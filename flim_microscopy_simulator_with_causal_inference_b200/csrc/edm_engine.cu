@@ -622,8 +622,11 @@ struct EdmEngine {
     z.p[5] = sw_count, z.n[5] = sw_count ? 1 : 0;
     k_scan_reduce<<<nbs, kScanThreads, 0, s>>>(cnt, n_cells, bsum, z);
     k_scan_bsum<<<1, 1024, 0, s>>>(bsum, nbs);
-    join_photons(s);  // the previous step's photon pass reads the cell list and slots about to change
+    // the previous step's photon pass reads the slots and positions the sort
+    // rewrites, and with proximity FRET the bucket starts
+    if (phot_uses_cells) join_photons(s);
     k_scan_down<<<nbs, kScanThreads, 0, s>>>(cnt, n_cells, bsum, cell_start, cursor);
+    join_photons(s);
     mark(1, s);
     cur ^= 1;
     DevState st = dev_state();
@@ -754,6 +757,7 @@ struct EdmEngine {
   // call wait for both.  Errors surface at the call's cudaGetLastError or at
   // the capture's end.
   cudaStream_t phot_stream = nullptr, scope_stream = nullptr;
+  bool phot_uses_cells = true;  // some replica's FRET is by proximity (a cell-list search)
   cudaEvent_t ev_phot_fork = nullptr, ev_phot_join = nullptr, ev_scope_join = nullptr;
   bool phot_pending = false, scope_pending = false;
   void enqueue_photons_beside(cudaStream_t s) {
@@ -1068,6 +1072,12 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
   if ((rc = E->build_schedule()) != EDM_OK || (rc = E->upload_thresholds()) != EDM_OK) {
     delete E;
     return rc;
+  }
+  if (E->has_phot) {
+    E->phot_uses_cells = false;
+    for (const EdmPhotParams& q : E->hpp)
+      for (int f = 0; f < q.n_fret && f < EDM_MAX_FRET; ++f)
+        if (q.fret[f].mode != 0) E->phot_uses_cells = true;
   }
   if (E->has_scope) {
     CUDA_TRY(cudaStreamCreateWithFlags(&E->phot_stream, cudaStreamNonBlocking));
