@@ -318,7 +318,8 @@ int edm_get_photons(EdmEngine* eng, int32_t replica, int32_t* particle_idx,
                     int64_t capacity, void* stream);
 
 /* VirtualMicroscope.process_photons(batch) (microscope.py:1069-1157) on the
- * last device batch. */
+ * last device batch, each photon at its particle's position in the current
+ * state (as the reference reads it from the particle state it is given). */
 int edm_scope_process(EdmEngine* eng, void* stream);
 
 /* Load a host photon batch (PhotonBatch fields, photophysics.py:184-211) of
