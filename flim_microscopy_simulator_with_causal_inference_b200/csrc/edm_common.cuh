@@ -192,6 +192,17 @@ __device__ __forceinline__ void atomic_add_i64(int64_t* p, long long v) {
 
 __device__ __forceinline__ void set_status(uint32_t* st, uint32_t bit) { atomicOr(st, bit); }
 
+// First statement of every kernel of the BD step's chain.  Launched as a
+// programmatic dependent of the kernel before it on the stream, a kernel's
+// blocks may be resident before that kernel has finished; griddepcontrol.wait
+// holds them until it has completed and its writes are visible (so each
+// kernel's completion implies its predecessor's, down the chain), then
+// launch_dependents lets the next kernel of the chain be scheduled.  Launched
+// without the attribute, both are no-ops.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;\n\tgriddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __device__ __forceinline__ int clampi(int v, int n) {
   v = v >= n ? n - 1 : v;
   return v < 0 ? 0 : v;

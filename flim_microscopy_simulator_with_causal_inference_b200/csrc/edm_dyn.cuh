@@ -520,6 +520,7 @@ __global__ void k_scan_reduce(const int32_t* __restrict__ cnt, int64_t n, int32_
 }
 
 __global__ void k_scan_bsum(int32_t* __restrict__ bsum, int nb) {
+  pdl_enter();
   int carry = 0;
   for (int off = 0; off < nb; off += blockDim.x) {
     const int i = off + threadIdx.x;
@@ -533,6 +534,7 @@ __global__ void k_scan_bsum(int32_t* __restrict__ bsum, int nb) {
 
 __global__ void k_scan_down(int32_t* __restrict__ cnt, int64_t n, const int32_t* __restrict__ bsum,
                             int32_t* __restrict__ start, int32_t* __restrict__ cursor) {
+  pdl_enter();
   const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
   const int4 c = load4(cnt, base, n);
   int total;
@@ -549,6 +551,7 @@ __global__ void k_scan_down(int32_t* __restrict__ cnt, int64_t n, const int32_t*
 template <bool F64, int BS>
 __global__ void __launch_bounds__(BS) k_scatter(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk,
                                                     DevState st) {
+  pdl_enter();
   const Tile t = tile_of(blk);
   const EdmDynParams& p = P[t.r];
   if (t.s >= p.particle_offset + p.n_particles) return;
@@ -734,6 +737,7 @@ __device__ __forceinline__ void dfield(const EdmDynParams& p, int sp, double x, 
 template <bool F64, int BS, int MINB>
 __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk,
                                                  DevState st) {
+  pdl_enter();
   const Tile t = tile_of(blk);
   const EdmDynParams& p = P[t.r];
   const int64_t s = t.s;
@@ -1033,6 +1037,7 @@ __device__ __forceinline__ void flush_contacts(const DevState& st, const CatList
 template <bool F64, int MINB>
 __global__ void __launch_bounds__(kBlock, MINB) k_contacts(const EdmDynParams* __restrict__ P, DevState st, Match m,
                                                      CatLists L) {
+  pdl_enter();
   __shared__ int2 buf[kContactSmem];
   __shared__ int nbuf[EDM_MAX_CAT], base[EDM_MAX_CAT];
   const ContactStage S{buf, nbuf, L.n_cat > 0 ? kContactSmem / L.n_cat : kContactSmem};
@@ -1092,6 +1097,7 @@ __device__ __forceinline__ void contact_column_task(const EdmDynParams* __restri
 template <bool F64, int MINB>
 __global__ void __launch_bounds__(kBlock, MINB) k_contacts_cols(const EdmDynParams* __restrict__ P, DevState st,
                                                               Match m, CatLists L) {
+  pdl_enter();
   __shared__ int2 buf[kContactSmem];
   __shared__ int nbuf[EDM_MAX_CAT], base[EDM_MAX_CAT];
   __shared__ int32_t list[kBlock / 32][kSweepChunk];
@@ -1181,6 +1187,7 @@ __device__ __forceinline__ int block_compact(const DevState& st, const Match& m,
 // kBlock * 16 slots and appends them with one atomic (launch with
 // ceil(n_slots / (16 kBlock)) blocks of kBlock).
 __global__ void __launch_bounds__(kBlock) k_sweep_list(DevState st, Match m) {
+  pdl_enter();
   __shared__ int32_t list[kBlock * 16];
   __shared__ int woff[kBlock / 32 + 1];
   __shared__ int at;
@@ -1195,6 +1202,7 @@ __global__ void __launch_bounds__(kBlock) k_sweep_list(DevState st, Match m) {
 template <bool F64, int MINB>
 __global__ void __launch_bounds__(kBlock, MINB) k_contacts_list(const EdmDynParams* __restrict__ P, DevState st,
                                                               CatLists L) {
+  pdl_enter();
   __shared__ int2 buf[kContactSmem];
   __shared__ int nbuf[EDM_MAX_CAT], base[EDM_MAX_CAT];
   const ContactStage S{buf, nbuf, L.n_cat > 0 ? kContactSmem / L.n_cat : kContactSmem};
@@ -1217,6 +1225,7 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contacts_list(const EdmDynPara
 template <bool F64, int MINB, int SPT>
 __global__ void __launch_bounds__(kBlock, MINB) k_contacts_block(const EdmDynParams* __restrict__ P, DevState st,
                                                                Match m, CatLists L) {
+  pdl_enter();
   __shared__ int2 buf[kContactSmem];
   __shared__ int nbuf[EDM_MAX_CAT], base[EDM_MAX_CAT];
   __shared__ int32_t list[kBlock * SPT];
@@ -1279,6 +1288,7 @@ __device__ __forceinline__ void late_contacts(const EdmDynParams& p, const Geo& 
 template <bool F64>
 __global__ void __launch_bounds__(kBlock, 4) k_catalytic(const EdmDynParams* __restrict__ P, DevState st, int cidx,
                                                        uint32_t late) {
+  pdl_enter();
   const int n = st.contact_count[cidx];
   const int lim = (int64_t)n < st.contact_cap ? n : (int)st.contact_cap;
   const int2* list = st.contacts + (int64_t)cidx * st.contact_cap;
@@ -1351,6 +1361,7 @@ __device__ __forceinline__ uint32_t draw_passes(const DevState& st, const DrawPl
 
 __global__ void __launch_bounds__(kBlock, 8) k_pass_draws(const EdmDynParams* __restrict__ P, DevState st,
                                                        const DrawPlan* __restrict__ D, Match any) {
+  pdl_enter();
   sweep4(st, any, [&](int r, int64_t s) {
     const uint8_t f = st.flags[s];
     const int sp = fl_species(f);
@@ -1373,6 +1384,7 @@ template <bool F64>
 __global__ void k_recruit_apply(const EdmDynParams* __restrict__ P, int n_rep, DevState st, int e,
                                 const DrawPlan* __restrict__ D,
                                 uint32_t after) {
+  pdl_enter();
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n_rep) return;
   const EdmDynParams& p = P[r];
@@ -1544,6 +1556,7 @@ template <bool F64>
 __global__ void __launch_bounds__(kBlock) k_particle_passes(const EdmDynParams* __restrict__ P, DevState st,
                                                             const PassGroup* __restrict__ G,
                                                             const DrawPlan* __restrict__ D) {
+  pdl_enter();
   const PassGroup& sg = *G;
   const int n = *st.pl_count;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
@@ -1580,6 +1593,7 @@ __global__ void __launch_bounds__(kBlock) k_particle_passes(const EdmDynParams* 
 template <bool F64>
 __global__ void __launch_bounds__(kBlock) k_bind_candidates(const EdmDynParams* __restrict__ P, DevState st,
                                                             Match m, int b) {
+  pdl_enter();
   sweep4(st, m, [&](int r, int64_t s) {
     const EdmDynParams& p = P[r];
     const EdmBind& B = p.bind[b];
@@ -1627,6 +1641,7 @@ __global__ void __launch_bounds__(kBlock) k_bind_candidates(const EdmDynParams* 
 // Sequential greedy application in pair order, re-checking the live state.
 template <bool F64>
 __global__ void k_bind_apply(const EdmDynParams* __restrict__ P, int n_rep, DevState st, int b) {
+  pdl_enter();
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n_rep) return;
   const EdmDynParams& p = P[r];
@@ -1679,6 +1694,7 @@ __global__ void k_bind_apply(const EdmDynParams* __restrict__ P, int n_rep, DevS
 template <bool F64>
 __global__ void __launch_bounds__(kBlock) k_dissociate(const EdmDynParams* __restrict__ P, DevState st, Match m,
                                                        int b) {
+  pdl_enter();
   sweep4(st, m, [&](int r, int64_t s) {
     const EdmDynParams& p = P[r];
     const EdmBind& B = p.bind[b];
@@ -1718,6 +1734,7 @@ __global__ void __launch_bounds__(kBlock) k_dissociate(const EdmDynParams* __res
 // replica.
 __global__ void k_adapt(const EdmDynParams* __restrict__ P, const int32_t* __restrict__ cnt,
                         double* __restrict__ w) {
+  pdl_enter();
   const EdmDynParams& p = P[blockIdx.y];
   if (p.adapt_grid < 0) return;
   const EdmGrid& A = p.grid[p.adapt_grid];
@@ -1734,6 +1751,7 @@ __global__ void k_adapt(const EdmDynParams* __restrict__ P, const int32_t* __res
 // (dynamics.py:2356-2371).
 __global__ void k_local_cdf(const EdmDynParams* __restrict__ P, const int32_t* __restrict__ cnt,
                             double* __restrict__ cdf_all, int e) {
+  pdl_enter();
   const EdmDynParams& p = P[blockIdx.x];
   const EdmExch& X = p.exch[e];
   if (!X.local_recruit || X.rule_on < 0) return;
@@ -1762,6 +1780,7 @@ __global__ void k_local_cdf(const EdmDynParams* __restrict__ P, const int32_t* _
 }
 
 __global__ void k_grid_merge(int32_t* __restrict__ cnt, int32_t* __restrict__ delta, int64_t n) {
+  pdl_enter();
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const int d = delta[i];
     if (d) {
@@ -1771,6 +1790,9 @@ __global__ void k_grid_merge(int32_t* __restrict__ cnt, int32_t* __restrict__ de
   }
 }
 
-__global__ void k_step_inc(int64_t* step) { *step += 1; }
+__global__ void k_step_inc(int64_t* step) {
+  pdl_enter();
+  *step += 1;
+}
 
 }  // namespace edm

@@ -8,6 +8,7 @@
 // captured into CUDA graphs (the BD step index lives in device memory, so a
 // captured chunk replays with advancing keys).
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -558,15 +559,45 @@ struct EdmEngine {
     if (tune_kernel == kernel) cudaEventRecord(tune_ev[k], s);
   }
 
+  // Launches of the BD step's chain on its stream.  When the operation
+  // before it on the stream is a kernel of the chain (pdl_chain), the kernel
+  // goes as a programmatic dependent of that kernel: its blocks are scheduled
+  // while the predecessor drains and wait in pdl_enter() for its completion,
+  // so the launch latency between the two overlaps the predecessor's tail.
+  // Anything else on the stream (an event wait, a record, a copy) ends the
+  // chain: the next kernel goes with the ordinary full dependency.  Off
+  // while profiling or tuning, whose event records sit between the kernels,
+  // and with EDM_PDL=0 in the environment at engine creation, and on the
+  // default streams.
+  bool pdl_on = true;
+  bool pdl_chain = false;
+  template <typename... K, typename... A>
+  void go(void (*kernel)(K...), dim3 grid, int block, cudaStream_t s, A&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    // created streams only (not the legacy or per-thread default stream)
+    const bool created = reinterpret_cast<uintptr_t>(s) > 2;
+    cfg.numAttrs = (pdl_on && pdl_chain && created && !prof && !pass_prof && tune_kernel < 0) ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+    pdl_chain = true;
+  }
+
   template <bool F64>
   void launch_scatter(const DevState& st, cudaStream_t s) {
     const LaunchShape sh = kShapes[TK_SCATTER][shape[TK_SCATTER]];
     const int t = tile_index(sh.block);
     if (npblk_bs[t] == 0) return;
     switch (sh.block) {
-      case 128: k_scatter<F64, 128><<<npblk_bs[t], 128, 0, s>>>(dp, pblk_bs[t], st); break;
-      case 512: k_scatter<F64, 512><<<npblk_bs[t], 512, 0, s>>>(dp, pblk_bs[t], st); break;
-      default: k_scatter<F64, 256><<<npblk_bs[t], 256, 0, s>>>(dp, pblk_bs[t], st); break;
+      case 128: go(k_scatter<F64, 128>, npblk_bs[t], 128, s, dp, pblk_bs[t], st); break;
+      case 512: go(k_scatter<F64, 512>, npblk_bs[t], 512, s, dp, pblk_bs[t], st); break;
+      default: go(k_scatter<F64, 256>, npblk_bs[t], 256, s, dp, pblk_bs[t], st); break;
     }
   }
 
@@ -578,14 +609,14 @@ struct EdmEngine {
     const int n = npblk_bs[t];
     const int2* b = pblk_bs[t];
     switch (v) {  // the rows of kShapes[TK_MOVE]
-      case 1: k_move<F64, 256, 4><<<n, 256, 0, s>>>(dp, b, st); break;
-      case 2: k_move<F64, 128, 8><<<n, 128, 0, s>>>(dp, b, st); break;
-      case 3: k_move<F64, 128, 10><<<n, 128, 0, s>>>(dp, b, st); break;
-      case 4: k_move<F64, 128, 12><<<n, 128, 0, s>>>(dp, b, st); break;
-      case 5: k_move<F64, 128, 16><<<n, 128, 0, s>>>(dp, b, st); break;
-      case 6: k_move<F64, 256, 6><<<n, 256, 0, s>>>(dp, b, st); break;
-      case 7: k_move<F64, 256, 8><<<n, 256, 0, s>>>(dp, b, st); break;
-      default: k_move<F64, 256, 3><<<n, 256, 0, s>>>(dp, b, st); break;
+      case 1: go(k_move<F64, 256, 4>, n, 256, s, dp, b, st); break;
+      case 2: go(k_move<F64, 128, 8>, n, 128, s, dp, b, st); break;
+      case 3: go(k_move<F64, 128, 10>, n, 128, s, dp, b, st); break;
+      case 4: go(k_move<F64, 128, 12>, n, 128, s, dp, b, st); break;
+      case 5: go(k_move<F64, 128, 16>, n, 128, s, dp, b, st); break;
+      case 6: go(k_move<F64, 256, 6>, n, 256, s, dp, b, st); break;
+      case 7: go(k_move<F64, 256, 8>, n, 256, s, dp, b, st); break;
+      default: go(k_move<F64, 256, 3>, n, 256, s, dp, b, st); break;
     }
   }
 
@@ -594,18 +625,18 @@ struct EdmEngine {
     const int grid16 = (int)((N + 16 * kBlock - 1) / (16 * kBlock));  // 16 slots per thread
     if (grid16 == 0) return;
     switch (shape[TK_CONTACTS]) {  // the rows of kShapes[TK_CONTACTS]
-      case 1: k_contacts_cols<F64, 6><<<grid, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
-      case 2: k_contacts_cols<F64, 4><<<grid, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
-      case 3: k_contacts_block<F64, 6, 16><<<grid16, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
-      case 4: k_contacts_block<F64, 4, 16><<<grid16, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
-      case 5: k_contacts_block<F64, 6, 4><<<grid, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
+      case 1: go(k_contacts_cols<F64, 6>, grid, kBlock, s, dp, st, m, cat_lists); break;
+      case 2: go(k_contacts_cols<F64, 4>, grid, kBlock, s, dp, st, m, cat_lists); break;
+      case 3: go(k_contacts_block<F64, 6, 16>, grid16, kBlock, s, dp, st, m, cat_lists); break;
+      case 4: go(k_contacts_block<F64, 4, 16>, grid16, kBlock, s, dp, st, m, cat_lists); break;
+      case 5: go(k_contacts_block<F64, 6, 4>, grid, kBlock, s, dp, st, m, cat_lists); break;
       case 6:
       case 7:
-        k_sweep_list<<<grid16, kBlock, 0, s>>>(st, m);
-        if (shape[TK_CONTACTS] == 6) k_contacts_list<F64, 6><<<148 * 6, kBlock, 0, s>>>(dp, st, cat_lists);
-        else k_contacts_list<F64, 8><<<148 * 8, kBlock, 0, s>>>(dp, st, cat_lists);
+        go(k_sweep_list, grid16, kBlock, s, st, m);
+        if (shape[TK_CONTACTS] == 6) go(k_contacts_list<F64, 6>, 148 * 6, kBlock, s, dp, st, cat_lists);
+        else go(k_contacts_list<F64, 8>, 148 * 8, kBlock, s, dp, st, cat_lists);
         break;
-      default: k_contacts<F64, 6><<<grid, kBlock, 0, s>>>(dp, st, m, cat_lists); break;
+      default: go(k_contacts<F64, 6>, grid, kBlock, s, dp, st, m, cat_lists); break;
     }
   }
 
@@ -620,12 +651,13 @@ struct EdmEngine {
     z.p[3] = contact_count, z.n[3] = contact_count ? EDM_MAX_CAT : 0;
     z.p[4] = pl_count, z.n[4] = pl_count ? 1 : 0;
     z.p[5] = sw_count, z.n[5] = sw_count ? 1 : 0;
-    k_scan_reduce<<<nbs, kScanThreads, 0, s>>>(cnt, n_cells, bsum, z);
-    k_scan_bsum<<<1, 1024, 0, s>>>(bsum, nbs);
+    k_scan_reduce<<<nbs, kScanThreads, 0, s>>>(cnt, n_cells, bsum, z);  // starts the chain
+    pdl_chain = true;
+    go(k_scan_bsum, 1, 1024, s, bsum, nbs);
     // the previous step's photon pass reads the slots and positions the sort
     // rewrites, and with proximity FRET the bucket starts
     if (phot_uses_cells) join_photons(s);
-    k_scan_down<<<nbs, kScanThreads, 0, s>>>(cnt, n_cells, bsum, cell_start, cursor);
+    go(k_scan_down, nbs, kScanThreads, s, cnt, n_cells, bsum, cell_start, cursor);
     join_photons(s);
     mark(1, s);
     cur ^= 1;
@@ -647,18 +679,16 @@ struct EdmEngine {
       const Pass& ps = passes[i];
       if (pass_prof) cudaEventRecord(pass_prof[i], s);
       switch (ps.kind) {
-        case P_BIND_CAND: k_bind_candidates<F64><<<sgrid, kBlock, 0, s>>>(dp, st, ps.match, ps.index); break;
-        case P_BIND_APPLY: k_bind_apply<F64><<<rb, 128, 0, s>>>(dp, R, st, ps.index); break;
-        case P_DISSOC: k_dissociate<F64><<<sgrid, kBlock, 0, s>>>(dp, st, ps.match, ps.index); break;
+        case P_BIND_CAND: go(k_bind_candidates<F64>, sgrid, kBlock, s, dp, st, ps.match, ps.index); break;
+        case P_BIND_APPLY: go(k_bind_apply<F64>, rb, 128, s, dp, R, st, ps.index); break;
+        case P_DISSOC: go(k_dissociate<F64>, sgrid, kBlock, s, dp, st, ps.match, ps.index); break;
         case P_CONTACTS:
           tune_mark(TK_CONTACTS, 0, s);
           launch_contacts<F64>(st, ps.match, sgrid, s);
           tune_mark(TK_CONTACTS, 1, s);
           break;
-        case P_CAT: k_catalytic<F64><<<cgrid, kBlock, 0, s>>>(dp, st, ps.index, cat_late[ps.index]); break;
-        case P_REC_APPLY:
-          k_recruit_apply<F64><<<rb, 128, 0, s>>>(dp, R, st, ps.index, d_draw, rec_after[ps.index]);
-          break;
+        case P_CAT: go(k_catalytic<F64>, cgrid, kBlock, s, dp, st, ps.index, cat_late[ps.index]); break;
+        case P_REC_APPLY: go(k_recruit_apply<F64>, rb, 128, s, dp, R, st, ps.index, d_draw, rec_after[ps.index]); break;
         case P_DRAWS: {
           // beside the following passes on the side stream (not while timing passes one by one)
           const bool fork = draws_early && !pass_prof && side_stream;
@@ -667,8 +697,10 @@ struct EdmEngine {
             cudaEventRecord(ev_fork, s);
             cudaStreamWaitEvent(side_stream, ev_fork, 0);
             ds = side_stream;
+            pdl_chain = false;
           }
-          k_pass_draws<<<sgrid, kBlock, 0, ds>>>(dp, st, d_draw, draw.any);
+          if (fork) k_pass_draws<<<sgrid, kBlock, 0, ds>>>(dp, st, d_draw, draw.any);
+          else go(k_pass_draws, sgrid, kBlock, s, dp, st, d_draw, draw.any);
           if (fork) {
             cudaEventRecord(ev_join, side_stream);
             joined = false;
@@ -679,19 +711,20 @@ struct EdmEngine {
           if (!joined) {
             cudaStreamWaitEvent(s, ev_join, 0);
             joined = true;
+            pdl_chain = false;
           }
-          k_particle_passes<F64><<<148, kBlock, 0, s>>>(dp, st, d_groups + ps.index, d_draw);
+          go(k_particle_passes<F64>, 148, kBlock, s, dp, st, d_groups + ps.index, d_draw);
           break;
-        case P_ADAPT: k_adapt<<<dim3(4, R), 256, 0, s>>>(dp, grid_cnt, adapt_w); break;
-        case P_LOCAL_CDF: k_local_cdf<<<R, 256, 0, s>>>(dp, grid_cnt, local_cdf, ps.index); break;
+        case P_ADAPT: go(k_adapt, dim3(4, R), 256, s, dp, grid_cnt, adapt_w); break;
+        case P_LOCAL_CDF: go(k_local_cdf, R, 256, s, dp, grid_cnt, local_cdf, ps.index); break;
         case P_REC_CAND:
         case P_DETACH:
         case P_CONV: break;  // fused into P_GROUP passes
-        case P_MERGE: k_grid_merge<<<gm > 0 ? gm : 1, 256, 0, s>>>(grid_cnt, grid_delta, n_grid); break;
+        case P_MERGE: go(k_grid_merge, gm > 0 ? gm : 1, 256, s, grid_cnt, grid_delta, n_grid); break;
       }
     }
     if (pass_prof) cudaEventRecord(pass_prof[passes.size()], s);
-    k_step_inc<<<1, 1, 0, s>>>(d_step);
+    go(k_step_inc, 1, 1, s, d_step);
     cells_valid = true;
     mark(4, s);
   }
@@ -775,12 +808,14 @@ struct EdmEngine {
     if (!phot_pending) return;
     cudaStreamWaitEvent(s, ev_phot_join, 0);
     phot_pending = false;
+    pdl_chain = false;
   }
   void join_beside(cudaStream_t s) {
     join_photons(s);
     if (!scope_pending) return;
     cudaStreamWaitEvent(s, ev_scope_join, 0);
     scope_pending = false;
+    pdl_chain = false;
   }
 
   // Census of the state into `base` (ring of `cap` steps, or one block when
@@ -919,6 +954,7 @@ int edm_create(const EdmDynParams* dyn, const EdmPhotParams* phot, const EdmScop
   E->precision = precision;
   E->f64 = precision == 64;
   E->R = n_replicas;
+  if (const char* pdl = std::getenv("EDM_PDL")) E->pdl_on = pdl[0] != '0';
   E->hdp.assign(dyn, dyn + n_replicas);
   E->has_phot = phot != nullptr;
   E->has_scope = scope != nullptr && phot != nullptr;
