@@ -579,9 +579,12 @@ __global__ void __launch_bounds__(BS) k_scatter(const EdmDynParams* __restrict__
 // =============================================================================
 
 // Enumerate the pair-force terms of slot s; pass `emit(key, fx, fy)`.
+constexpr int kForceCand = 2;  // float32 force candidates listed per sweep
+
 template <bool F64, typename Emit>
 __device__ __forceinline__ void for_each_force_term(const EdmDynParams& p, const Geo& g, const DevState& st,
-                                                    int64_t s, int sp, int id, Emit emit) {
+                                                    int64_t s, int sp, int id, Emit emit, int2* cand = nullptr,
+                                                    int cand_stride = 0) {
   double xi = 0, yi = 0;
   float2 oi = make_float2(0.f, 0.f);
   if constexpr (F64) {
@@ -678,7 +681,32 @@ __device__ __forceinline__ void for_each_force_term(const EdmDynParams& p, const
       }
     }
   };
-  for_neighbour_slots_box(g, st, c_pre, dxlo, dxhi, dylo, dyhi, term);
+  if constexpr (F64) {
+    for_neighbour_slots_box(g, st, c_pre, dxlo, dxhi, dylo, dyhi, term);
+  } else {
+    // The sweep only lists the neighbours that pass the float32 range test
+    // (rarely any) in cand[0], cand[cand_stride], ...; their float64
+    // separation and force follow after it, so the sweep's loop does not
+    // hold the float64 pair code's registers.  More than kForceCand of them
+    // take further sweeps, each listing the next kForceCand in sweep order.
+    for (int done = 0;; done += kForceCand) {
+      int found = 0, kept = 0;
+      for_neighbour_slots_box(g, st, c_pre, dxlo, dxhi, dylo, dyhi, [&](int j, int ordinal, int dcx, int dcy) {
+        if (j == s) return;
+        const float2 oj = ((const float2*)st.pos_pre)[j];
+        const float fdx = __fmaf_rn(-(float)dcx, g.sxf, oi.x - oj.x);
+        const float fdy = __fmaf_rn(-(float)dcy, g.syf, oi.y - oj.y);
+        if (!(__fmaf_rn(fdx, fdx, fdy * fdy) < range_sqf)) return;
+        const int rank = found++;
+        if (rank >= done && rank < done + kForceCand) cand[(kept++) * cand_stride] = make_int2(j, ordinal);
+      });
+      for (int k = 0; k < kept; ++k) {
+        const int2 e = cand[k * cand_stride];
+        term(e.x, e.y, e.y / 3 - 1, e.y % 3 - 1);
+      }
+      if (found <= done + kForceCand) break;
+    }
+  }
 }
 
 // D(x) and grad D at an absolute position (dynamics.py:440-519; sine-x field).
@@ -732,6 +760,13 @@ __device__ __forceinline__ void dfield(const EdmDynParams& p, int sp, double x, 
   }
 }
 
+// dfield out of line, for the float32 move: most systems have no D(x) field,
+// and the field's float64 code would otherwise share the move's registers.
+__device__ __noinline__ void dfield_call(const EdmDynParams& p, int sp, double x, double y, double& D, double& gx,
+                                         double& gy) {
+  dfield(p, sp, x, y, D, gx, gy);
+}
+
 // BS threads per block over tiles of BS slots; MINB resident blocks per SM
 // requested from the register allocator (1 = no constraint).
 template <bool F64, int BS, int MINB>
@@ -768,6 +803,7 @@ __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restric
   double Fx = 0.0, Fy = 0.0;
   long long qx = 0, qy = 0;
   int nterms = 0;
+  __shared__ int2 cand_smem[F64 ? 1 : kForceCand * BS];
   for_each_force_term<F64>(p, g, st, s, sp, id, [&](uint64_t, double fx, double fy) {
     ++nterms;
     if constexpr (F64) {
@@ -777,7 +813,7 @@ __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restric
       qx += __double2ll_rn(fx * 0x1p20);
       qy += __double2ll_rn(fy * 0x1p20);
     }
-  });
+  }, cand_smem + threadIdx.x, BS);
   if constexpr (F64) {
     if (nterms > 2) {
       Fx = 0.0;
@@ -809,7 +845,14 @@ __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restric
   // the float32 path needs the absolute position here only for a D(x) field
   if (F64 || p.dfield != EDM_DFIELD_NONE) abs_pos<F64>(st.pos_pre, st.lo_pre, st.cell_pre, s, g, x, y);
   double Di, gDx, gDy;
-  dfield(p, sp, x, y, Di, gDx, gDy);
+  if constexpr (F64) {
+    dfield(p, sp, x, y, Di, gDx, gDy);
+  } else if (p.dfield == EDM_DFIELD_NONE) {
+    Di = p.D_base[sp];
+    gDx = gDy = 0.0;
+  } else {
+    dfield_call(p, sp, x, y, Di, gDx, gDy);
+  }
   const double dt = p.dt;
   int newc;
   if constexpr (F64) {
