@@ -548,30 +548,54 @@ __global__ void k_scan_down(int32_t* __restrict__ cnt, int64_t n, const int32_t*
   if (n == 0 && blockIdx.x == 0 && threadIdx.x == 0) start[0] = 0;
 }
 
-template <bool F64, int BS>
+template <bool F64, int BS, int SPT>
 __global__ void __launch_bounds__(BS) k_scatter(const EdmDynParams* __restrict__ P, const int2* __restrict__ blk,
-                                                    DevState st) {
+                                                    int ntiles, DevState st) {
   pdl_enter();
-  const Tile t = tile_of(blk);
-  const EdmDynParams& p = P[t.r];
-  if (t.s >= p.particle_offset + p.n_particles) return;
-  const int c = st.cell_post[t.s];
-  const uint8_t f = st.flags_old[t.s];
-  // alive particles mostly have a cell to themselves: a plain atomic; the
-  // non-alive ones all share their replica's last bucket: aggregated per warp
-  const int d = fl_alive(f) ? atomicAdd(&st.cell_cursor[p.cell_offset + c], 1)
-                            : atomic_inc_aggregated(&st.cell_cursor[p.cell_offset + p.nx * p.ny]);
-  if constexpr (F64) {
-    ((double2*)st.pos_pre)[d] = ((const double2*)st.pos_post)[t.s];
-  } else {
-    ((float2*)st.pos_pre)[d] = ((const float2*)st.pos_post)[t.s];
-    st.lo_pre[d] = st.lo_post[t.s];
+  // SPT tiles per block (blockIdx.x * SPT + k): each thread reads its slots'
+  // buckets and takes all their cursor positions before the first dependent
+  // store, so SPT atomics are in flight per thread
+  int64_t src[SPT], bkt[SPT];
+  uint8_t fl[SPT];
+  int cl[SPT], dst[SPT];
+#pragma unroll
+  for (int k = 0; k < SPT; ++k) {
+    src[k] = -1;
+    const int tile = (int)blockIdx.x * SPT + k;
+    if (tile >= ntiles) continue;
+    const int2 b = blk[tile];
+    const EdmDynParams& p = P[b.x];
+    const int64_t s = (int64_t)(uint32_t)b.y + threadIdx.x;
+    if (s >= p.particle_offset + p.n_particles) continue;
+    src[k] = s;
+    cl[k] = st.cell_post[s];
+    fl[k] = st.flags_old[s];
+    bkt[k] = p.cell_offset + (fl_alive(fl[k]) ? cl[k] : p.nx * p.ny);
   }
-  st.cell_pre[d] = c;
-  st.flags[d] = f;
-  const int id = st.ids_old[t.s];
-  st.ids[d] = id;
-  st.slot_of_id[id] = d;
+#pragma unroll
+  for (int k = 0; k < SPT; ++k) {
+    if (src[k] < 0) continue;
+    // alive particles mostly have a cell to themselves: a plain atomic; the
+    // non-alive ones all share their replica's last bucket: aggregated per warp
+    dst[k] = fl_alive(fl[k]) ? atomicAdd(&st.cell_cursor[bkt[k]], 1) : atomic_inc_aggregated(&st.cell_cursor[bkt[k]]);
+  }
+#pragma unroll
+  for (int k = 0; k < SPT; ++k) {
+    if (src[k] < 0) continue;
+    const int64_t s = src[k];
+    const int d = dst[k];
+    if constexpr (F64) {
+      ((double2*)st.pos_pre)[d] = ((const double2*)st.pos_post)[s];
+    } else {
+      ((float2*)st.pos_pre)[d] = ((const float2*)st.pos_post)[s];
+      st.lo_pre[d] = st.lo_post[s];
+    }
+    st.cell_pre[d] = cl[k];
+    st.flags[d] = fl[k];
+    const int id = st.ids_old[s];
+    st.ids[d] = id;
+    st.slot_of_id[id] = d;
+  }
 }
 
 // =============================================================================
@@ -792,8 +816,14 @@ __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restric
     return;
   }
   const int sp = fl_species(f);
-  const int id = st.ids[s] - (int)g.poff;
-  const int64_t step = *st.d_step;
+  // the float32 path reads its id and the step index after the force sweep,
+  // which needs neither, so that they hold no registers during it
+  int id = 0;
+  int64_t step = 0;
+  if constexpr (F64) {
+    id = st.ids[s] - (int)g.poff;
+    step = *st.d_step;
+  }
 
   // Pair forces.  The float64 path sums them in the reference's accumulation
   // order (a sum of two terms is the same either way, so only three or more
@@ -881,6 +911,8 @@ __global__ void __launch_bounds__(BS, MINB) k_move(const EdmDynParams* __restric
     ((double2*)st.pos_post)[s] = make_double2(x, y);
     newc = cell_index(x, g.sx, g.nx) * g.ny + cell_index(y, g.sy, g.ny);
   } else {
+    id = st.ids[s] - (int)g.poff;
+    step = *st.d_step;
     float z0, z1;
     normal2_f32(p.seed, step, EDM_S_BD_NORMAL, (uint64_t)id, z0, z1);
     const float Dif = (float)Di, dtf = (float)dt;

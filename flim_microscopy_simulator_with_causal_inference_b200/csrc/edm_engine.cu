@@ -77,7 +77,8 @@ struct LaunchShape {
 enum TunedKernel { TK_SCATTER = 0, TK_MOVE = 1, TK_CONTACTS = 2, TK_COUNT = 3 };
 constexpr int kMaxShapes = 8;
 constexpr LaunchShape kShapes[TK_COUNT][kMaxShapes] = {
-    {{256, 1}, {128, 1}, {512, 1}},                                // k_scatter
+    // k_scatter: one slot per thread, then (3-4) two
+    {{256, 1}, {128, 1}, {512, 1}, {128, 1}, {256, 1}},
     // k_move: the second number bounds its registers (80 at 256 x 3 down to 32
     // at 128 x 16, with spills below 64): occupancy pays more than the spills
     {{256, 3}, {256, 4}, {128, 8}, {128, 10}, {128, 12}, {128, 16}, {256, 6}, {256, 8}},
@@ -86,7 +87,7 @@ constexpr LaunchShape kShapes[TK_COUNT][kMaxShapes] = {
     // thread); 6-7 over a global sweeper list (k_sweep_list), one wave
     {{256, 6}, {256, 6}, {256, 4}, {256, 6}, {256, 4}, {256, 6}, {256, 6}, {256, 8}},
 };
-constexpr int kNumShapes[TK_COUNT] = {3, 8, 8};
+constexpr int kNumShapes[TK_COUNT] = {5, 8, 8};
 const char* const kTunedNames[TK_COUNT] = {"k_scatter", "k_move", "k_contacts"};
 constexpr int kTileSizes[3] = {128, 256, 512};
 int tile_index(int bs) { return bs == 128 ? 0 : (bs == 256 ? 1 : 2); }
@@ -594,10 +595,14 @@ struct EdmEngine {
     const LaunchShape sh = kShapes[TK_SCATTER][shape[TK_SCATTER]];
     const int t = tile_index(sh.block);
     if (npblk_bs[t] == 0) return;
-    switch (sh.block) {
-      case 128: go(k_scatter<F64, 128>, npblk_bs[t], 128, s, dp, pblk_bs[t], st); break;
-      case 512: go(k_scatter<F64, 512>, npblk_bs[t], 512, s, dp, pblk_bs[t], st); break;
-      default: go(k_scatter<F64, 256>, npblk_bs[t], 256, s, dp, pblk_bs[t], st); break;
+    const int nt = npblk_bs[t];
+    const int2* b = pblk_bs[t];
+    switch (shape[TK_SCATTER]) {  // the rows of kShapes[TK_SCATTER]
+      case 1: go(k_scatter<F64, 128, 1>, nt, 128, s, dp, b, nt, st); break;
+      case 2: go(k_scatter<F64, 512, 1>, nt, 512, s, dp, b, nt, st); break;
+      case 3: go(k_scatter<F64, 128, 2>, (nt + 1) / 2, 128, s, dp, b, nt, st); break;
+      case 4: go(k_scatter<F64, 256, 2>, (nt + 1) / 2, 256, s, dp, b, nt, st); break;
+      default: go(k_scatter<F64, 256, 1>, nt, 256, s, dp, b, nt, st); break;
     }
   }
 

@@ -429,7 +429,8 @@ int edm_ground_truth(EdmEngine* eng, double* fret_E, double* tau_DA,
  * of the same kind, unless retune != 0.  Drops the engine's captured graphs. */
 int edm_autotune(EdmEngine* eng, int32_t steps_per_shape, int32_t retune, void* stream);
 /* The launch shape in use per tuned kernel: shapes[k][4] = (threads per block,
- * minimum blocks per SM, candidates, chosen candidate; k_contacts candidate 0
+ * minimum blocks per SM, candidates, chosen candidate; k_scatter candidates
+ * 3-4 give a thread two slots, the others one; k_contacts candidate 0
  * gives a thread a whole sweeper, 1-2 give each lane one neighbour column of
  * a sweeper within a warp, 3-5 within a block, 6-7 over a global sweeper
  * list), ms[k][2] = (time of the default shape, time of the chosen shape) from
