@@ -42,8 +42,9 @@ def test_autotuned_engine_matches_default_shapes_bitwise():
 @pytest.mark.parametrize("precision", [32, 64])
 def test_every_scatter_and_move_shape_gives_the_same_run(precision):
     """The order in which k_scatter's cursor atomics place the slots of one
-    bucket differs from shape to shape (one or two slots per thread, block
-    sizes); nothing downstream depends on it.  Fresh ensembles of jittered
+    bucket, and the contact search's order of appends, differ from shape to
+    shape (one or two slots per thread, block sizes, the contact search's
+    forms); nothing downstream depends on them.  Fresh ensembles of jittered
     replicas, stepped through graph chunks with photons at each fixed shape,
     end with the same state, counters and stacks bit for bit."""
     import torch
@@ -51,11 +52,12 @@ def test_every_scatter_and_move_shape_gives_the_same_run(precision):
     from flim_microscopy_simulator_with_causal_inference_b200.batch import Ensemble
     raws = W.ensemble_replicas(6, seed=17, n_min=600, n_max=2000)
     ref = None
-    for scatter, move in ((0, 0), (1, 5), (2, 2), (3, 5), (4, 7)):
+    for scatter, move, contacts in ((0, 0, 0), (1, 5, 7), (2, 2, 3), (3, 5, 6), (4, 7, 1)):
         ens = Ensemble(raws, precision=precision, photons=True, device=0)
         eng = ens.engine
-        got = eng.set_launch_shapes([scatter, move, -1])
+        got = eng.set_launch_shapes([scatter, move, contacts])
         assert got["k_scatter"]["candidate"] == scatter and got["k_move"]["candidate"] == move
+        assert got["k_contacts"]["candidate"] == contacts
         s = torch.cuda.Stream()
         eng.pipeline_steps(60, True, 30, stream=s)
         s.synchronize()

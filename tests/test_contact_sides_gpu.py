@@ -57,3 +57,23 @@ def test_float32_sides_agree():
     for key in a:
         assert np.array_equal(a[key], b[key]), key
     assert np.array_equal(ca, cb)
+
+
+@pytest.mark.parametrize("case", ["rich_small", "binding_regions", "adaptive_local"])
+@pytest.mark.parametrize("shape", [1, 3, 6, 7])
+def test_contact_search_forms_match_the_oracle(case, shape):
+    """The contact search by (sweeper, neighbour column) within a warp (1),
+    balanced over the block (3) and over the global sweeper list (6, 7): the
+    float64 path reproduces the oracle bit for bit with each."""
+    P = Pair(cases.get(case), precision=64, photons=False)
+    assert P.eng.set_launch_shapes([-1, -1, shape])["k_contacts"]["candidate"] == shape
+    for t in range(40):
+        P.eng.dynamics_step(1)
+        P.orc.dynamics_step()
+        P.orc.step_index += 1
+        if t % 10 == 9:
+            compare_state(P.gpu_state(), P.orc, F64_TOL)
+    g = P.eng.counters()[0]
+    assert np.array_equal(g[:6], P.orc.counters[:6]), (g[:6], P.orc.counters[:6])
+    assert P.orc.counters[2] > 0, "no catalytic events: the test would not exercise the contact lists"
+    assert P.eng.status() == 0
